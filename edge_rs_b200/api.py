@@ -1,0 +1,162 @@
+"""Python mirror of edge-rs's NEBULA interface for the B200 path.
+
+`nebula_sparse_cuda` takes what `nebula_sparse` takes (src/sc/nebula.rs:434-445:
+gene-major CSR counts, contiguous subject ids, a design with an intercept of
+up to 8 columns, optional positive offsets, NebulaParams) and returns the same
+NebulaFit (nebula.rs:301-344). It calls the C-ABI of libnebula_b200.so; there
+is no CPU fallback. Errors raise NebulaError carrying the EdgeErrors variant.
+"""
+import ctypes
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from . import _ffi
+
+
+class NebulaError(RuntimeError):
+    """An EdgeErrors value returned through the C-ABI."""
+
+    def __init__(self, code, message):
+        self.code = int(code)
+        self.variant = _ffi.STATUS_NAMES.get(self.code, f"code {code}")
+        super().__init__(f"{self.variant}: {message}")
+
+
+@dataclass
+class NebulaParams:
+    """NebulaParams (nebula.rs:207-258); defaults are the R package's."""
+    min: tuple = (1e-4, 1e-4)
+    max: tuple = (10.0, 1000.0)
+    method: str = "LN"
+    cutoff_cell: float = 20.0
+    kappa: float = 800.0
+    cpc: float = 0.005
+    mincp: int = 5
+    min_subjects: int = 0
+    reml: bool = False
+    eps: float = 1e-6
+
+    def to_c(self):
+        method = {"LN": _ffi.NB_METHOD_LN, "HL": _ffi.NB_METHOD_HL}[self.method.upper()]
+        return _ffi.NbParams(float(self.min[0]), float(self.min[1]), float(self.max[0]),
+                             float(self.max[1]), method, float(self.cutoff_cell), float(self.kappa),
+                             float(self.cpc), int(self.mincp), int(self.min_subjects),
+                             int(bool(self.reml)), float(self.eps))
+
+
+@dataclass
+class NebulaFit:
+    """NebulaFit (nebula.rs:301-344); covariance packed upper column-major."""
+    coefficients: np.ndarray
+    covariance: np.ndarray
+    se: np.ndarray
+    subject_overdispersion: np.ndarray
+    cell_overdispersion: np.ndarray
+    convergence: np.ndarray
+    sigma_at_bound: np.ndarray
+    gene_index: np.ndarray
+    n_coef: int
+    stats: dict = field(default_factory=dict)
+
+
+def _as_csr(counts):
+    """(indptr, indices, data, shape) from a scipy CSR matrix or a 4-tuple."""
+    if hasattr(counts, "indptr") and hasattr(counts, "indices"):
+        fmt = _ffi.NB_CSR if getattr(counts, "format", "csr") == "csr" else _ffi.NB_CSC
+        return _ffi.CsrArrays(counts.indptr, counts.indices, counts.data, counts.shape, fmt)
+    indptr, indices, data, shape = counts
+    return _ffi.CsrArrays(indptr, indices, data, shape)
+
+
+def fit_from_arrays(f, n_coef, stats=None):
+    n = int(f.struct.n_kept)
+    packed = n_coef * (n_coef + 1) // 2
+    return NebulaFit(
+        coefficients=f.coefficients[: n * n_coef].reshape(n, n_coef).copy(),
+        covariance=f.covariance[: n * packed].reshape(n, packed).copy(),
+        se=f.se[: n * n_coef].reshape(n, n_coef).copy(),
+        subject_overdispersion=f.subject[:n].copy(),
+        cell_overdispersion=f.cell[:n].copy(),
+        convergence=f.convergence[:n].copy(),
+        sigma_at_bound=f.at_bound[:n].astype(bool),
+        gene_index=f.gene_index[:n].astype(np.int64),
+        n_coef=int(f.struct.n_coef),
+        stats=stats or {},
+    )
+
+
+def call_nebula(fn, counts, subject_id, design, n_coef, offset, params, extra_args=(), options=None,
+                want_stats=False):
+    """Marshals the arguments of a nebula_sparse-shaped C entry point."""
+    csr = _as_csr(counts)
+    n_genes, n_cells = int(csr.struct.n_genes), int(csr.struct.n_cells)
+    subject = np.ascontiguousarray(subject_id, dtype=np.uint64)
+    design = np.ascontiguousarray(design, dtype=np.float64).reshape(-1)
+    off = None if offset is None else np.ascontiguousarray(offset, dtype=np.float64)
+    if subject.size != n_cells:
+        raise NebulaError(2, f"subject_id has {subject.size} entries, expected {n_cells}")
+    if design.size != n_cells * n_coef:
+        raise NebulaError(3, f"design has {design.size} values, expected {n_cells * n_coef}")
+    if off is not None and off.size != n_cells:
+        raise NebulaError(2, f"offset has {off.size} entries, expected {n_cells}")
+    p = (params or NebulaParams()).to_c()
+    out = _ffi.FitArrays(n_genes, n_coef)
+    err = ctypes.create_string_buffer(512)
+    stats = _ffi.NbStats()
+    args = [ctypes.byref(csr.struct), _ffi.ptr(subject, ctypes.c_uint64), _ffi.ptr(design, ctypes.c_double),
+            ctypes.c_uint32(n_coef), _ffi.ptr(off, ctypes.c_double), ctypes.byref(p)]
+    if options is not None:
+        args.append(ctypes.byref(options))
+    args += list(extra_args)
+    args.append(ctypes.byref(out.struct))
+    if want_stats:
+        args.append(ctypes.byref(stats))
+    args += [err, ctypes.c_size_t(len(err))]
+    rc = fn(*args)
+    if rc != 0:
+        raise NebulaError(rc, err.value.decode(errors="replace"))
+    return fit_from_arrays(out, n_coef, stats.as_dict() if want_stats else None)
+
+
+def nebula_sparse_cuda(counts, subject_id, design, n_coef, offset=None, params: Optional[NebulaParams] = None,
+                       warm_start=False, device=-1, host_threads=0, audit_percent=5):
+    """Fits NEBULA per gene with every inner penalised fit on the GPU."""
+    lib = _ffi.product_library()
+    opts = _ffi.NbOptions(int(device), int(bool(warm_start)), int(host_threads), int(audit_percent), None)
+    return call_nebula(lib.nebula_sparse_cuda_ex, counts, subject_id, design, n_coef, offset, params,
+                       options=opts, want_stats=True)
+
+
+@dataclass
+class ScTestResult:
+    """glm_sc_test's output (src/sc/test.rs:69-82) plus log p-values."""
+    log_fc: np.ndarray
+    se: np.ndarray
+    z: np.ndarray
+    p_value: np.ndarray
+    log_p_value: np.ndarray
+    fdr: np.ndarray
+
+
+def glm_sc_test(coefficients, covariance, coef=None, contrast=None):
+    """Wald test of one coefficient or a contrast per gene (src/sc/test.rs:96-200)."""
+    lib = _ffi.product_library()
+    beta = np.ascontiguousarray(coefficients, dtype=np.float64)
+    n_genes, n_coef = beta.shape
+    cov = np.ascontiguousarray(covariance, dtype=np.float64)
+    if contrast is None:
+        if coef is None or not 0 <= coef < n_coef:
+            raise NebulaError(13, f"coefficient {coef} is out of range for {n_coef}")
+        contrast = np.zeros(n_coef)
+        contrast[coef] = 1.0
+    c = np.ascontiguousarray(contrast, dtype=np.float64)
+    outs = [np.zeros(n_genes) for _ in range(6)]
+    err = ctypes.create_string_buffer(256)
+    rc = lib.nb_glm_sc_test(_ffi.ptr(beta, ctypes.c_double), _ffi.ptr(cov, ctypes.c_double), n_genes, n_coef,
+                            _ffi.ptr(c, ctypes.c_double), *[_ffi.ptr(o, ctypes.c_double) for o in outs],
+                            err, len(err))
+    if rc != 0:
+        raise NebulaError(rc, err.value.decode(errors="replace"))
+    return ScTestResult(*outs)

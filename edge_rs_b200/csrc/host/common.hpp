@@ -1,0 +1,125 @@
+// Host-side types shared by the device driver and the CPU oracle: the
+// per-run inputs every gene reads (nebula.rs:676-710 `Shared`), one gene's
+// positive counts (ptmg.rs:1652-1664 `GeneCounts`), stage one's plan
+// (nebula.rs:745-773 `GenePlan`), one gene's outcome (nebula.rs:713-726) and
+// the error convention (src/errors.rs mapped to nb_status codes).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "nebula_cuda.h"
+
+namespace nebula {
+
+// An EdgeErrors value: the nb_status code and its message.
+struct NbError {
+  int32_t code;
+  std::string message;
+};
+[[noreturn]] void fail(int32_t code, const std::string& message);
+
+// NebulaParams (nebula.rs:207-258).
+struct Params {
+  double min0 = 1e-4, min1 = 1e-4, max0 = 10.0, max1 = 1000.0;
+  int method = NB_METHOD_LN;
+  double cutoff_cell = 20.0, kappa = 800.0, cpc = 0.005;
+  uint64_t mincp = 5, min_subjects = 0;
+  bool reml = false;
+  double eps = 1e-6;
+  static Params from(const nb_params* p);
+  void validate() const;  // nebula.rs:266-289
+};
+
+// Everything the per-gene fit reads but never writes (nebula.rs:676-710).
+struct Shared {
+  std::vector<double> design;  // centred and scaled, row-major n_cells x n_coef
+  std::vector<double> log_offset;
+  std::vector<uint64_t> fid;   // subject boundaries, n_subjects + 1
+  std::vector<double> sds;     // column standard deviations (centre_design)
+  size_t n_cells = 0;
+  int n_coef = 0;
+  int n_subjects = 0;
+  int intercept = 0;
+  double log_mean_offset = 0.0;
+  double cells_per_subject = 0.0;
+  double cv2 = 0.0;
+  std::vector<int> cell_columns;
+  int method = NB_METHOD_LN;  // after the cells-per-subject override
+  Params params;
+};
+
+// The gene-major count matrix as the caller handed it over.
+struct CsrView {
+  uint64_t n_genes, n_cells, nnz;
+  const uint32_t* indptr;
+  const uint32_t* indices;
+  const double* data;
+};
+
+// Validation, offsets, centred design, subject totals and the expression
+// filter of nebula_sparse_with (nebula.rs:512-657).
+struct Prepared {
+  Shared shared;
+  CsrView counts{};
+  std::vector<double> totals;  // gene-major n_genes x n_subjects (cumsum_y)
+  std::vector<size_t> kept;    // genes that passed the filter
+};
+Prepared prepare(const nb_csr* counts, const uint64_t* subject_id, const double* design,
+                 uint32_t n_coef, const double* offset, const nb_params* params);
+
+// One gene's positive counts (positive_indices, ptmg.rs:1681-1728).
+struct GeneCounts {
+  std::vector<uint32_t> cells;
+  std::vector<double> counts;
+  double mean_count = 0.0;
+  size_t n_one = 0, n_two = 0;
+};
+GeneCounts positive_indices(const CsrView& csr, size_t gene);
+
+// Stage one's decision for one gene (nebula.rs:745-773).
+enum class Refit { None, Both, SubjectOnly };
+struct GenePlan {
+  int ord = 1;
+  double sigma = 0.0, gamma = 0.0;
+  int convergence = 1;
+  std::vector<double> beta_start;
+  Refit refit = Refit::Both;
+};
+
+// One gene's fit on the centred design scale (nebula.rs:713-726).
+struct GeneOutcome {
+  std::vector<double> beta, covariance, se;
+  double subject = 0.0, cell = 0.0;
+  int convergence = 1;
+};
+
+// The four scalars the profile objective reads off an inner fit
+// (nebula.rs:1337-1346 `InnerFit`).
+struct InnerFit {
+  double log_likelihood, log_likelihood_prev, log_det, second_order;
+};
+
+// What a final (stage-three) inner fit hands finish_gene.
+struct FinalFit {
+  std::vector<double> beta, information;
+  double log_likelihood = 0.0;
+  int iterations = 0, backtracks = 0;
+};
+
+constexpr int kConvSuccess = 1;
+constexpr int kConvCriticalPoint = -10;
+constexpr int kConvMaxIter = -20;
+constexpr int kConvSingular = -25;
+constexpr int kConvNotFinite = -30;
+constexpr int kConvStalled = -40;
+constexpr int kConvOuterFailed = -50;
+constexpr int kConvAtBound = -60;
+constexpr int kPmlMaxIter = 50;       // pml.rs:52
+constexpr int kPmlMaxBacktrack = 10;  // pml.rs:57
+
+inline size_t packed_len(int n) { return static_cast<size_t>(n) * (n + 1) / 2; }
+
+}  // namespace nebula

@@ -1,0 +1,164 @@
+/*
+ * nebula_cuda.h — C-ABI of the B200 NEBULA-HL stage-two path.
+ *
+ * The drop-in entry point is nebula_sparse_cuda(): same inputs and the same
+ * NebulaFit as edge-rs's
+ *   nebula_sparse<T: EdgeFloat>(counts: &CompressedSparse<f64>,
+ *       subject_id: &[usize], design: &[T], n_coef: usize,
+ *       offset: Option<&[T]>, params: Option<NebulaParams>)
+ *       -> Result<NebulaFit, EdgeErrors>            (src/sc/nebula.rs:434-445)
+ * and its device twin nebula_sparse_gpu (src/gpu/stage_two.rs:233-265).
+ * Plain pointers and sizes only; the caller owns every buffer.
+ *
+ * Every function returns NB_OK (0) or one NB_ERR_* code; the codes map 1:1
+ * onto the EdgeErrors variants this path can raise (src/errors.rs), and `err`
+ * (may be NULL) receives the message.
+ */
+#ifndef NEBULA_CUDA_H
+#define NEBULA_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes (src/errors.rs variant in brackets). */
+enum nb_status {
+  NB_OK = 0,
+  NB_ERR_EMPTY_COUNTS = 1,            /* EmptyCounts */
+  NB_ERR_LENGTH_MISMATCH = 2,         /* LengthMismatch */
+  NB_ERR_SHAPE_MISMATCH = 3,          /* ShapeMismatch */
+  NB_ERR_INVALID_ARGUMENT = 4,        /* InvalidArgument */
+  NB_ERR_MUST_BE_POSITIVE = 5,        /* MustBePositive */
+  NB_ERR_MALFORMED_SPARSE = 6,        /* MalformedSparse (errors.rs:162) */
+  NB_ERR_NO_GENES_AFTER_FILTERING = 7,/* NoGenesAfterFiltering (errors.rs:169) */
+  NB_ERR_INVALID_DISPERSION = 8,      /* InvalidDispersion (errors.rs:183) */
+  NB_ERR_SUBJECTS_NOT_CONTIGUOUS = 9, /* SubjectsNotContiguous (errors.rs:196) */
+  NB_ERR_MISSING_INTERCEPT = 10,      /* MissingIntercept (errors.rs:203) */
+  NB_ERR_TOO_FEW_SUBJECTS = 11,       /* TooFewSubjects (errors.rs:207) */
+  NB_ERR_INVALID_BOUNDS = 12,         /* InvalidBounds */
+  NB_ERR_COEF_OUT_OF_RANGE = 13,      /* CoefOutOfRange */
+  NB_ERR_GPU = 14,                    /* Gpu(String) (errors.rs:223) */
+  NB_ERR_UNSUPPORTED = 15             /* what the device path refuses, as the
+                                         reference's does: reml
+                                         (stage_two.rs:242-246) and more than
+                                         8 columns (pml_kernel.rs:1208-1212) */
+};
+
+/* CompressedSparse<f64> (src/utils/sparse.rs:58-69): u32 indptr/indices,
+ * f64 data, a format flag and the (n_genes, n_cells) shape. */
+typedef struct nb_csr {
+  uint64_t n_genes;
+  uint64_t n_cells;
+  uint64_t nnz;
+  const uint32_t* indptr;  /* n_genes + 1 */
+  const uint32_t* indices; /* nnz, cell of each stored value */
+  const double* data;      /* nnz, finite and >= 0; zeros may be stored */
+  int32_t format;          /* NB_CSR (gene-major) or NB_CSC */
+} nb_csr;
+
+enum nb_format { NB_CSR = 0, NB_CSC = 1 };
+enum nb_method { NB_METHOD_LN = 0, NB_METHOD_HL = 1 };
+
+/* NebulaParams (src/sc/nebula.rs:207-258). nb_params_default() fills R's
+ * defaults: min (1e-4, 1e-4), max (10, 1000), method LN, cutoff_cell 20,
+ * kappa 800, cpc 0.005, mincp 5, min_subjects 0, reml off, eps 1e-6. */
+typedef struct nb_params {
+  double min_subject, min_cell; /* min.0, min.1 */
+  double max_subject, max_cell; /* max.0, max.1 */
+  int32_t method;               /* nb_method */
+  double cutoff_cell;
+  double kappa;
+  double cpc;
+  uint64_t mincp;
+  uint64_t min_subjects;
+  int32_t reml;
+  double eps;
+} nb_params;
+
+/* NebulaFit (src/sc/nebula.rs:301-344). Caller-allocated for n_genes rows;
+ * the callee fills the first n_kept rows and writes n_kept and n_coef.
+ * covariance is packed upper, column-major: (i <= j) at j(j+1)/2 + i. */
+typedef struct nb_fit {
+  double* coefficients;           /* n_genes * n_coef */
+  double* covariance;             /* n_genes * n_coef(n_coef+1)/2 */
+  double* se;                     /* n_genes * n_coef */
+  double* subject_overdispersion; /* n_genes */
+  double* cell_overdispersion;    /* n_genes */
+  int32_t* convergence;           /* n_genes */
+  uint8_t* sigma_at_bound;        /* n_genes */
+  uint64_t* gene_index;           /* n_genes */
+  uint64_t n_kept;
+  uint64_t n_coef;
+} nb_fit;
+
+/* How stage two is started and batched. Zero-initialised = the plain
+ * cold-start method the reference runs. */
+typedef struct nb_options {
+  int32_t device;        /* CUDA ordinal; -1 = current device */
+  int32_t warm_start;    /* 1: learned warm start + plain finish (see below) */
+  int32_t host_threads;  /* stage-one host threads; 0 = all cores */
+  int32_t audit_percent; /* warm start only: share of genes refit cold */
+  const float* mlp_weights; /* warm start only: nb_mlp_* layout; NULL = built-in */
+} nb_options;
+
+/* Counters of one call (timings in milliseconds of host wall clock, device
+ * times from CUDA events on the launching stream). */
+typedef struct nb_stats {
+  uint64_t rounds;          /* batched stage-two launches */
+  uint64_t requests;        /* inner fits run on the device */
+  uint64_t sweeps;          /* cell passes run on the device */
+  uint64_t cell_visits;     /* dense + sparse cell visits on the device */
+  uint64_t gpu_launches;    /* kernels launched */
+  double ms_total, ms_prepare, ms_stage_one, ms_stage_two, ms_stage_three;
+  double ms_device;         /* sum of device time of the stage-two fit kernel */
+  uint64_t audited, refit_cold;
+} nb_stats;
+
+void nb_params_default(nb_params* params);
+
+/* Drop-in for nebula_sparse (src/sc/nebula.rs:434-445) with every inner
+ * penalised fit on the GPU. Returns NB_OK or an NB_ERR_* code. */
+int32_t nebula_sparse_cuda(const nb_csr* counts, const uint64_t* subject_id,
+                           const double* design, uint32_t n_coef,
+                           const double* offset_or_null,
+                           const nb_params* params_or_null, nb_fit* out,
+                           char* err, size_t err_len);
+
+/* nebula_sparse_cuda with options and counters (either may be NULL). */
+int32_t nebula_sparse_cuda_ex(const nb_csr* counts, const uint64_t* subject_id,
+                              const double* design, uint32_t n_coef,
+                              const double* offset_or_null,
+                              const nb_params* params_or_null,
+                              const nb_options* options, nb_fit* out,
+                              nb_stats* stats, char* err, size_t err_len);
+
+/* glm_sc_test (src/sc/test.rs:96-200): Wald test of the contrast c per gene,
+ * z = c'beta / sqrt(c'Vc), p = chisq_sf(z^2, 1), BH FDR. log_p_value keeps
+ * the tail in log space where p underflows. Any output may be NULL. */
+int32_t nb_glm_sc_test(const double* coefficients, const double* covariance,
+                       uint64_t n_genes, uint64_t n_coef, const double* contrast,
+                       double* log_fc, double* se, double* z, double* p_value,
+                       double* log_p_value, double* fdr, char* err,
+                       size_t err_len);
+
+/* Reverse-communication BOBYQA as NLopt 2.7.1 runs it
+ * (src/numeric/bobyqa.rs:141-560 BobyqaStepper::{new, ask, tell, result}). */
+typedef struct nb_bobyqa nb_bobyqa;
+nb_bobyqa* nb_bobyqa_new(const double* x0, const double* lower,
+                         const double* upper, uint32_t n, double xtol_rel,
+                         uint32_t maxeval);
+int32_t nb_bobyqa_ask(const nb_bobyqa* h, double* x); /* 1: x pending */
+void nb_bobyqa_tell(nb_bobyqa* h, double value);
+/* returns the NLopt status: 4 xtol, 5 maxeval, 1 success, -4 roundoff */
+int32_t nb_bobyqa_result(const nb_bobyqa* h, double* x, double* f,
+                         uint32_t* evaluations);
+void nb_bobyqa_free(nb_bobyqa* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NEBULA_CUDA_H */

@@ -1,0 +1,59 @@
+// ORACLE — test infrastructure only. C-ABI the tests and the CPU-baseline leg
+// of bench.py load with ctypes. Never linked by the product library.
+#include <cstdint>
+
+#include "pml_cpu.hpp"
+
+#define ORACLE_API extern "C" __attribute__((visibility("default")))
+
+// scalars_out: log_likelihood, log_likelihood_prev, log_det, second_order
+// ints_out: convergence, iterations, backtracks, sweeps
+ORACLE_API int32_t oracle_opt_pml(const double* design, const double* offset, uint64_t n_cells,
+                                  uint32_t n_beta, const double* counts, const uint32_t* cells,
+                                  uint64_t n_pos, const uint64_t* subject_start, uint32_t k,
+                                  const double* subject_total, const double* beta_init,
+                                  const double* log_w_init, double subject, double cell,
+                                  int32_t reml, double eps, int32_t ord, int32_t max_iter,
+                                  int32_t prior_lognormal, double* beta_out, double* log_w_out,
+                                  double* information_out, double* scalars_out,
+                                  int32_t* ints_out) {
+  oracle::PmlData d{design, offset, n_cells, static_cast<int>(n_beta), counts, cells, n_pos,
+                    subject_start, static_cast<int>(k), subject_total};
+  oracle::PmlParams p;
+  p.reml = reml != 0;
+  p.eps = eps;
+  p.ord = ord;
+  p.max_iter = max_iter;
+  oracle::PmlResult r;
+  if (!oracle::opt_pml(d, beta_init, log_w_init, subject, cell, p,
+                       prior_lognormal ? oracle::Prior::LogNormal : oracle::Prior::Gamma, &r))
+    return 4;
+  for (uint32_t j = 0; j < n_beta; ++j) beta_out[j] = r.beta[j];
+  for (uint32_t s = 0; s < k; ++s) log_w_out[s] = r.log_w[s];
+  for (uint32_t j = 0; j < n_beta * n_beta; ++j) information_out[j] = r.information[j];
+  scalars_out[0] = r.log_likelihood;
+  scalars_out[1] = r.log_likelihood_prev;
+  scalars_out[2] = r.log_det;
+  scalars_out[3] = r.second_order;
+  ints_out[0] = r.convergence;
+  ints_out[1] = r.iterations;
+  ints_out[2] = r.backtracks;
+  ints_out[3] = r.sweeps;
+  return 0;
+}
+
+ORACLE_API double oracle_pml_objective_gradient(const double* design, const double* offset,
+                                                uint64_t n_cells, uint32_t n_beta,
+                                                const double* counts, const uint32_t* cells,
+                                                uint64_t n_pos, const uint64_t* subject_start,
+                                                uint32_t k, const double* subject_total,
+                                                const double* beta, const double* log_w,
+                                                double subject, double cell, double* gradient) {
+  oracle::PmlData d{design, offset, n_cells, static_cast<int>(n_beta), counts, cells, n_pos,
+                    subject_start, static_cast<int>(k), subject_total};
+  return oracle::pml_objective_gradient(d, beta, log_w, subject, cell, gradient);
+}
+
+ORACLE_API double oracle_min_eigenvalue(const double* a, uint32_t n) {
+  return oracle::min_eigenvalue(a, static_cast<int>(n));
+}
