@@ -1,0 +1,74 @@
+// Layout shared by the host driver and the batched inner-fit kernel.
+//
+// The kernel runs the reference's penalised NB-gamma inner fit (opt_pml,
+// src/sc/pml.rs:1614-1800) for a batch of requests, one (gene, sigma, gamma)
+// point each, in FP64 throughout: the profile objective the stage-two search
+// compares must agree with the CPU path to ~1e-12 so that BOBYQA, whose
+// resolution is ~1e-6, retraces the same points.
+#pragma once
+
+#include <cstdint>
+
+namespace nebula {
+namespace device {
+
+constexpr int kMaxCoef = 8;        // the device path's width cap (pml_kernel.rs:1208-1212)
+constexpr int kThreads = 256;      // threads per fit CTA
+constexpr int kWarps = kThreads / 32;
+
+// One inner fit to run.
+struct alignas(16) FitRequest {
+  int32_t gene;       // row of the resident CSR (kept genes, in kept order)
+  int32_t ord;        // Laplace order (1, 2 or 3)
+  int32_t reml;       // add log|det(information)| to the log-determinant
+  int32_t pad;
+  double subject;     // nebula's sigma[0] = log(1 + sigma^2)
+  double cell;        // NB size gamma
+  double beta[kMaxCoef];  // starting fixed effects (log_w starts at zero)
+};
+
+// What one inner fit hands back (PmlResult, pml.rs:288-326).
+struct alignas(16) FitResult {
+  double log_likelihood, log_likelihood_prev, log_det, second_order;
+  double beta[kMaxCoef];
+  double information[kMaxCoef * kMaxCoef];
+  int32_t iterations, backtracks, sweeps, status;  // status 0 ok, 1 rejected arguments
+};
+
+// Resident per-call data, device pointers.
+struct GeneData {
+  const double* design;      // n_cells x n_coef, centred, row-major
+  const double* log_offset;  // n_cells
+  const uint32_t* fid;       // n_subjects + 1
+  const uint64_t* gene_ptr;  // n_genes + 1 into cells/counts
+  const uint32_t* cells;     // positive entries' cells, increasing per gene
+  const double* counts;      // positive counts
+  const uint64_t* runs;      // n_genes x (n_subjects + 1): first positive entry of each subject
+  const double* totals;      // n_genes x n_subjects count totals
+  const uint32_t* warp_cells;  // kWarps + 1 boundaries of the dense pass's warp ranges
+  int32_t n_cells;
+  int32_t n_subjects;
+  int32_t n_coef;
+};
+
+struct FitControl {
+  double eps;
+  int32_t max_iter;
+  int32_t max_backtrack;
+};
+
+// Shared-memory bytes one fit CTA needs for n_subjects and n_coef.
+size_t fit_smem_bytes(int n_subjects, int n_coef);
+
+// Launches the persistent fit kernel over *n_requests (read on the device)
+// requests; `counter` must be zeroed before each launch (work queue).
+// `grid` CTAs loop over the queue. Returns cudaError_t as int.
+int launch_fit(const GeneData& data, const FitControl& ctl, const FitRequest* requests,
+               FitResult* results, const int32_t* n_requests, int32_t* counter, int grid,
+               void* stream);
+
+// CTAs per SM the fit kernel can keep resident for this shape.
+int fit_blocks_per_sm(int n_subjects, int n_coef);
+
+}  // namespace device
+}  // namespace nebula

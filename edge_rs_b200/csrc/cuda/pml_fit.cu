@@ -1,0 +1,770 @@
+// Batched penalised NB-gamma inner fit (the reference's opt_pml,
+// src/sc/pml.rs:1614-1800) on sm_100a, FP64 throughout.
+//
+// One persistent CTA per SM slot pulls (gene, sigma, gamma) requests off an
+// atomic work queue and runs the whole Newton loop for each: sweep, Schur
+// complement, pivoted LDL' solve, backtracking, log-determinant and the
+// higher-order Laplace pass.
+//
+// A sweep (pml.rs:1419-1590) splits each subject into a dense part over every
+// cell at a count of zero and a sparse part over the gene's positive counts.
+// Dense pass: the cells are cut into kWarps contiguous ranges, one per warp;
+// lanes stride a range subject by subject, accumulating the per-subject sums
+// in registers, and each (warp, subject) piece is warp-reduced into its own
+// shared-memory slot (slot index subject + warp is unique because both
+// advance together). Sparse pass: warp w takes the subjects s = w mod kWarps
+// and strides their positive entries. A combine step then sums, per subject
+// and in a fixed order, the slots of the warps that touched it; no atomics,
+// so results are bitwise reproducible run to run.
+//
+// The per-request scalars (Newton state, step sizes, loop flags) live in
+// shared memory and are written by thread 0 between barriers, so every
+// thread of the CTA takes the same branches. Every loop is bounded by
+// max_iter Newton steps of at most max_backtrack + 1 trial sweeps: nothing
+// waits on anything.
+//
+// The arithmetic is that of the FP64 CPU oracle operation for operation: the
+// same exp/log (nbmath.hpp), fused multiply-adds only where written (the
+// file is compiled with -fmad=false), and the same summation tree, so the
+// two agree bit for bit and the stage-two search retraces the same points.
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cstdint>
+
+#include "../host/nbmath.hpp"
+#include "pml_device.cuh"
+
+namespace nebula {
+namespace device {
+namespace {
+
+constexpr double kStepCutoff = 40.0;        // pml.rs:74
+constexpr double kGradientTolerance = 0.01; // pml.rs:67
+
+// Slot layout of one per-subject partial: resid, weight, sum ln t,
+// sum y*eta, sum y ln t, X'd (NB), sum p x (NB), sum p x x' (upper, NB(NB+1)/2).
+enum : int { kResid = 0, kWeight = 1, kSumLog = 2, kLinear = 3, kWlog = 4, kScore = 5 };
+template <int NB>
+struct Dims {
+  static constexpr int T = NB * (NB + 1) / 2;
+  static constexpr int NS = 5 + 2 * NB + T;
+  static constexpr int kFirst = kScore + NB;
+  static constexpr int kSecond = kFirst + NB;
+};
+constexpr int kLaplaceSums = 4;
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  return v;
+}
+
+// Shared-memory carve-up for one CTA (all offsets in doubles).
+template <int NB>
+struct Smem {
+  int K;
+  double* slots_dense;   // (K + kWarps) x NS
+  double* slots_sparse;  // K x NS, per-subject totals after the combine
+  double* sw[2];         // two sweeps: w K, dw K, vw K, vwb K*NB, db NB, vb NB*NB, ll 1
+  double* beta;          // NB
+  double* log_w;         // K
+  double* new_beta;      // NB
+  double* new_log_w;     // K
+  double* step_beta;     // NB
+  double* step_log_w;    // K
+  double* dwvw;          // K
+  double* damp_beta;     // NB
+  double* damp_log_w;    // K
+  double* vw_step;       // K
+  double* vb2;           // NB*NB
+  double* factor;        // NB*NB
+  double* llv;           // K (per-subject log-likelihood terms)
+  double* sc;            // 16 scalars
+  uint32_t* fid;         // K + 1
+  uint32_t* wcells;      // kWarps + 1
+
+  __host__ __device__ static size_t sweep_doubles(int K) { return 3 * K + K * NB + NB + NB * NB + 1; }
+  __host__ __device__ static size_t doubles(int K) {
+    return (size_t)(2 * K + kWarps) * Dims<NB>::NS + 2 * sweep_doubles(K) + 4 * NB + 7 * K +
+           2 * NB * NB + 16;
+  }
+  __host__ __device__ static size_t bytes(int K) { return doubles(K) * 8 + (K + 1 + kWarps + 1) * 4 + 16; }
+
+  __device__ void carve(double* base, int K_) {
+    K = K_;
+    double* p = base;
+    slots_dense = p;
+    p += (K + kWarps) * Dims<NB>::NS;
+    slots_sparse = p;
+    p += K * Dims<NB>::NS;
+    sw[0] = p;
+    p += sweep_doubles(K);
+    sw[1] = p;
+    p += sweep_doubles(K);
+    beta = p; p += NB;
+    log_w = p; p += K;
+    new_beta = p; p += NB;
+    new_log_w = p; p += K;
+    step_beta = p; p += NB;
+    step_log_w = p; p += K;
+    dwvw = p; p += K;
+    damp_beta = p; p += NB;
+    damp_log_w = p; p += K;
+    vw_step = p; p += K;
+    vb2 = p; p += NB * NB;
+    factor = p; p += NB * NB;
+    llv = p; p += K;
+    sc = p; p += 16;
+    fid = reinterpret_cast<uint32_t*>(p);
+    wcells = fid + K + 1;
+  }
+};
+
+// Views into one sweep's storage.
+template <int NB>
+struct SweepView {
+  double *w, *dw, *vw, *vwb, *db, *vb, *ll;
+  __device__ SweepView(double* p, int K) {
+    w = p;
+    dw = p + K;
+    vw = p + 2 * K;
+    vwb = p + 3 * K;
+    db = vwb + K * NB;
+    vb = db + NB;
+    ll = vb + NB * NB;
+  }
+};
+
+// Scalar slots in Smem::sc.
+enum : int {
+  kLl = 0, kLlPrev = 1, kLikdif = 2, kMinStep = 3, kStep = 4, kBacktracks = 5, kStop = 6,
+  kSweeps = 7, kAlpha = 8, kLambda = 9, kGamma = 10, kLogDet = 11, kSecond = 12, kCur = 13
+};
+
+__device__ __forceinline__ int subject_of(const uint32_t* fid, int K, int c) {
+  int lo = 0, hi = K;  // fid[lo] <= c < fid[hi]
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (fid[mid] <= static_cast<uint32_t>(c)) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Per-cell fold (pml.rs:1469-1489) into the register accumulator.
+template <int NB>
+__device__ __forceinline__ void fold(double* acc, const double* x, double d, double p) {
+  acc[kResid] += d;
+  acc[kWeight] += p;
+  int t = 0;
+#pragma unroll
+  for (int a = 0; a < NB; ++a) {
+    acc[kScore + a] = nb_fma(x[a], d, acc[kScore + a]);
+    double pa = p * x[a];
+    acc[Dims<NB>::kFirst + a] += pa;
+#pragma unroll
+    for (int b = a; b < NB; ++b) {
+      acc[Dims<NB>::kSecond + t] = nb_fma(pa, x[b], acc[Dims<NB>::kSecond + t]);
+      ++t;
+    }
+  }
+}
+
+template <int NB>
+__device__ __forceinline__ void load_row(const double* __restrict__ design, int r, double* x) {
+  const double* row = design + static_cast<size_t>(r) * NB;
+#pragma unroll
+  for (int j = 0; j < NB; ++j) x[j] = __ldg(row + j);
+}
+
+template <int NB>
+__device__ __forceinline__ double linear_eta(const double* x, const double* beta, double off) {
+  double eta = off;
+#pragma unroll
+  for (int j = 0; j < NB; ++j) eta = nb_fma(x[j], beta[j], eta);
+  return eta;
+}
+
+template <int NV>
+__device__ __forceinline__ void reduce_to(double* acc, double* slot, int lane) {
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    double s = warp_sum(acc[v]);
+    if (lane == 0) slot[v] = s;
+  }
+}
+
+// One sweep's partial sums into the slots (dense then sparse), then the
+// per-subject combine into slots_sparse. Mode 0: the fit sums of
+// sweep_width; mode 1: the four Laplace sums (pml.rs:1842-1899).
+template <int NB, int MODE>
+__device__ void sweep_sums(const GeneData& d, Smem<NB>& sm, int gene, const double* beta_sm,
+                           const double* log_w, double gamma) {
+  constexpr int NV = MODE == 0 ? Dims<NB>::NS : kLaplaceSums;
+  const int K = sm.K;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double beta[NB];
+#pragma unroll
+  for (int j = 0; j < NB; ++j) beta[j] = beta_sm[j];
+
+  // dense part: every cell at a count of zero
+  const int c_begin = static_cast<int>(sm.wcells[warp]), c_end = static_cast<int>(sm.wcells[warp + 1]);
+  if (c_begin < c_end) {
+    int s = subject_of(sm.fid, K, c_begin);
+    for (int c0 = c_begin; c0 < c_end; ++s) {
+      const int s_end = min(c_end, static_cast<int>(sm.fid[s + 1]));
+      const double lw = log_w[s];
+      double acc[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) acc[v] = 0.0;
+      for (int r = c0 + lane; r < s_end; r += 32) {
+        double x[NB];
+        load_row<NB>(d.design, r, x);
+        double eta = linear_eta<NB>(x, beta, __ldg(d.log_offset + r));
+        double e = nb_exp(eta + lw);
+        double t = e + gamma;
+        if (MODE == 0) {
+          acc[kSumLog] += nb_log(t);
+          double inv = 1.0 / t;
+          double u = e * inv;
+          fold<NB>(acc, x, -gamma * u, (gamma * u) * inv);
+        } else {
+          double p2 = e / (t * t), p3 = p2 / t, p4 = p3 / t, p5 = p4 / t, e2 = e * e;
+          acc[0] += gamma * p2;
+          acc[1] += gamma * (p3 * (gamma - e));
+          acc[2] += gamma * (p4 * (gamma * gamma + e2 - (4.0 * gamma) * e));
+          acc[3] += gamma * (p5 * (gamma * gamma * gamma - (11.0 * gamma * gamma) * e +
+                                   (11.0 * gamma) * e2 - e2 * e));
+        }
+      }
+      reduce_to<NV>(acc, sm.slots_dense + (s + warp) * Dims<NB>::NS, lane);
+      c0 = s_end;
+    }
+  }
+  // sparse part: what the positive counts change
+  const uint64_t* runs = d.runs + static_cast<size_t>(gene) * (K + 1);
+  for (int s = warp; s < K; s += kWarps) {
+    const uint64_t p0 = runs[s], p1 = runs[s + 1];
+    const double lw = log_w[s];
+    double acc[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) acc[v] = 0.0;
+    for (uint64_t p = p0 + lane; p < p1; p += 32) {
+      const int c = static_cast<int>(__ldg(d.cells + p));
+      const double y = __ldg(d.counts + p);
+      double x[NB];
+      load_row<NB>(d.design, c, x);
+      double eta = linear_eta<NB>(x, beta, __ldg(d.log_offset + c));
+      double e = nb_exp(eta + lw);
+      double t = e + gamma;
+      if (MODE == 0) {
+        acc[kLinear] = nb_fma(eta, y, acc[kLinear]);
+        acc[kWlog] = nb_fma(y, nb_log(t), acc[kWlog]);
+        double inv = 1.0 / t;
+        double u = e * inv;
+        fold<NB>(acc, x, y * (1.0 - u), (y * u) * inv);
+      } else {
+        double p2 = e / (t * t), p3 = p2 / t, p4 = p3 / t, p5 = p4 / t, e2 = e * e;
+        acc[0] += y * p2;
+        acc[1] += y * (p3 * (gamma - e));
+        acc[2] += y * (p4 * (gamma * gamma + e2 - (4.0 * gamma) * e));
+        acc[3] += y * (p5 * (gamma * gamma * gamma - (11.0 * gamma * gamma) * e + (11.0 * gamma) * e2 -
+                             e2 * e));
+      }
+    }
+    reduce_to<NV>(acc, sm.slots_sparse + s * Dims<NB>::NS, lane);
+  }
+  __syncthreads();
+  // combine: per subject, the dense pieces in warp order, then the sparse part
+  for (int idx = threadIdx.x; idx < K * NV; idx += blockDim.x) {
+    const int s = idx / NV, v = idx - s * NV;
+    const uint32_t a0 = sm.fid[s], a1 = sm.fid[s + 1];
+    double total = 0.0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+      if (sm.wcells[w] < a1 && sm.wcells[w + 1] > a0) total += sm.slots_dense[(s + w) * Dims<NB>::NS + v];
+    }
+    total += sm.slots_sparse[s * Dims<NB>::NS + v];
+    sm.slots_sparse[s * Dims<NB>::NS + v] = total;
+  }
+  __syncthreads();
+}
+
+// A full sweep into `out` (pml.rs:1564-1589).
+template <int NB>
+__device__ void sweep(const GeneData& d, Smem<NB>& sm, int gene, const double* beta, const double* log_w,
+                      SweepView<NB> out) {
+  const int K = sm.K;
+  const double gamma = sm.sc[kGamma], alpha = sm.sc[kAlpha], lambda = sm.sc[kLambda];
+  sweep_sums<NB, 0>(d, sm, gene, beta, log_w, gamma);
+  const double* tot = d.totals + static_cast<size_t>(gene) * K;
+  const int tid = threadIdx.x;
+  for (int s = tid; s < K; s += blockDim.x) {
+    const double* T = sm.slots_sparse + s * Dims<NB>::NS;
+    const double lw = log_w[s];
+    const double w_s = nb_exp(lw);
+    sm.llv[s] = T[kLinear] + lw * __ldg(tot + s) - gamma * T[kSumLog] - T[kWlog];
+    out.w[s] = w_s;
+    out.dw[s] = T[kResid] + (alpha - lambda * w_s);
+    out.vw[s] = gamma * T[kWeight] + lambda * w_s;
+#pragma unroll
+    for (int a = 0; a < NB; ++a) out.vwb[s * NB + a] = gamma * T[Dims<NB>::kFirst + a];
+  }
+  __syncthreads();
+  // sums over subjects in subject order, as the CPU path adds them
+  if (tid < NB) {
+    double acc = 0.0;
+    for (int s = 0; s < K; ++s) acc += sm.slots_sparse[s * Dims<NB>::NS + kScore + tid];
+    out.db[tid] = acc;
+  } else if (tid < NB + Dims<NB>::T) {
+    const int t = tid - NB;
+    int a = 0, rem = t;
+    while (rem >= NB - a) {
+      rem -= NB - a;
+      ++a;
+    }
+    const int b = a + rem;
+    double acc = 0.0;
+    for (int s = 0; s < K; ++s) acc += gamma * sm.slots_sparse[s * Dims<NB>::NS + Dims<NB>::kSecond + t];
+    out.vb[a * NB + b] = acc;
+    out.vb[b * NB + a] = acc;
+  } else if (tid == 64) {
+    double ll = 0.0, sl = 0.0, sw = 0.0;
+    for (int s = 0; s < K; ++s) ll += sm.llv[s];
+    for (int s = 0; s < K; ++s) sl += log_w[s];
+    for (int s = 0; s < K; ++s) sw += out.w[s];
+    *out.ll = ll + (alpha * sl - lambda * sw);
+  }
+  if (tid == 0) sm.sc[kSweeps] += 1.0;
+  __syncthreads();
+}
+
+// Pivoted LDL' solve, Eigen's LDLT as nebula calls it (pml.rs:1940-2021).
+template <int NB>
+__device__ void ldlt_solve(double* a, double* b) {
+  int perm[NB];
+  double tmp[NB];
+  for (int step = 0; step < NB; ++step) {
+    int pivot = step;
+    double best = fabs(a[step * NB + step]);
+    for (int i = step + 1; i < NB; ++i) {
+      double v = fabs(a[i * NB + i]);
+      if (v > best) {
+        best = v;
+        pivot = i;
+      }
+    }
+    perm[step] = pivot;
+    if (pivot != step) {
+      for (int j = 0; j < step; ++j) {
+        double t = a[step * NB + j];
+        a[step * NB + j] = a[pivot * NB + j];
+        a[pivot * NB + j] = t;
+      }
+      for (int i = pivot + 1; i < NB; ++i) {
+        double t = a[i * NB + step];
+        a[i * NB + step] = a[i * NB + pivot];
+        a[i * NB + pivot] = t;
+      }
+      double t = a[step * NB + step];
+      a[step * NB + step] = a[pivot * NB + pivot];
+      a[pivot * NB + pivot] = t;
+      for (int i = step + 1; i < pivot; ++i) {
+        double u = a[i * NB + step];
+        a[i * NB + step] = a[pivot * NB + i];
+        a[pivot * NB + i] = u;
+      }
+    }
+    if (step > 0) {
+      for (int j = 0; j < step; ++j) tmp[j] = a[j * NB + j] * a[step * NB + j];
+      double acc = 0.0;
+      for (int j = 0; j < step; ++j) acc += a[step * NB + j] * tmp[j];
+      a[step * NB + step] -= acc;
+      for (int i = step + 1; i < NB; ++i) {
+        double acc2 = 0.0;
+        for (int j = 0; j < step; ++j) acc2 += a[i * NB + j] * tmp[j];
+        a[i * NB + step] -= acc2;
+      }
+    }
+    double dd = a[step * NB + step];
+    if (dd != 0.0)
+      for (int i = step + 1; i < NB; ++i) a[i * NB + step] /= dd;
+  }
+  for (int step = 0; step < NB; ++step) {
+    double t = b[step];
+    b[step] = b[perm[step]];
+    b[perm[step]] = t;
+  }
+  for (int i = 0; i < NB; ++i) {
+    double acc = b[i];
+    for (int j = 0; j < i; ++j) acc -= a[i * NB + j] * b[j];
+    b[i] = acc;
+  }
+  for (int i = 0; i < NB; ++i) {
+    double dd = a[i * NB + i];
+    b[i] = fabs(dd) > DBL_MIN ? b[i] / dd : 0.0;
+  }
+  for (int i = NB - 1; i >= 0; --i) {
+    double acc = b[i];
+    for (int j = i + 1; j < NB; ++j) acc -= a[j * NB + i] * b[j];
+    b[i] = acc;
+  }
+  for (int step = NB - 1; step >= 0; --step) {
+    double t = b[step];
+    b[step] = b[perm[step]];
+    b[perm[step]] = t;
+  }
+}
+
+// Determinant by partial-pivot LU, a product as the C++ takes it (pml.rs:2036-2069).
+template <int NB>
+__device__ double determinant(double* a) {
+  double det = 1.0;
+  for (int step = 0; step < NB; ++step) {
+    int pivot = step;
+    double best = fabs(a[step * NB + step]);
+    for (int i = step + 1; i < NB; ++i) {
+      double v = fabs(a[i * NB + step]);
+      if (v > best) {
+        best = v;
+        pivot = i;
+      }
+    }
+    if (pivot != step) {
+      for (int j = 0; j < NB; ++j) {
+        double t = a[step * NB + j];
+        a[step * NB + j] = a[pivot * NB + j];
+        a[pivot * NB + j] = t;
+      }
+      det = -det;
+    }
+    double dd = a[step * NB + step];
+    det *= dd;
+    if (dd == 0.0) return 0.0;
+    for (int i = step + 1; i < NB; ++i) {
+      double f = a[i * NB + step] / dd;
+      a[i * NB + step] = f;
+      for (int j = step + 1; j < NB; ++j) a[i * NB + j] -= f * a[step * NB + j];
+    }
+  }
+  return det;
+}
+
+template <int NB>
+__global__ void __launch_bounds__(kThreads) fit_kernel(GeneData d, FitControl ctl,
+                                                       const FitRequest* __restrict__ requests,
+                                                       FitResult* __restrict__ results,
+                                                       const int32_t* __restrict__ n_requests,
+                                                       int32_t* __restrict__ counter) {
+  extern __shared__ __align__(16) double smem_raw[];
+  Smem<NB> sm;
+  const int K = d.n_subjects;
+  sm.carve(smem_raw, K);
+  const int tid = threadIdx.x;
+  for (int i = tid; i <= K; i += blockDim.x) sm.fid[i] = d.fid[i];
+  if (tid <= kWarps) sm.wcells[tid] = d.warp_cells[tid];
+  __shared__ int next_req;
+  const int total = *n_requests;
+
+  for (;;) {
+    __syncthreads();
+    if (tid == 0) next_req = atomicAdd(counter, 1);
+    __syncthreads();
+    const int q = next_req;
+    if (q >= total) break;
+    const FitRequest req = requests[q];
+    const int gene = req.gene;
+    FitResult* out = results + q;
+
+    // gamma_penalty (pml.rs:432-441) and the argument checks of optimise
+    const double exps = nb_exp(req.subject);
+    const bool bad = !(isfinite(exps) && exps > 1.0) || !(isfinite(req.cell) && req.cell > 0.0);
+    if (bad) {
+      if (tid == 0) {
+        out->status = 1;
+        out->iterations = 0;
+        out->sweeps = 0;
+      }
+      continue;
+    }
+    if (tid == 0) {
+      sm.sc[kAlpha] = 1.0 / (exps - 1.0);
+      sm.sc[kLambda] = 1.0 / (sqrt(exps) * (exps - 1.0));
+      sm.sc[kGamma] = req.cell;
+      sm.sc[kSweeps] = 0.0;
+    }
+    if (tid < NB) sm.beta[tid] = req.beta[tid];
+    for (int s = tid; s < K; s += blockDim.x) sm.log_w[s] = 0.0;
+    __syncthreads();
+
+    int cur = 0;  // index of the current sweep buffer (every thread tracks it identically)
+    sweep<NB>(d, sm, gene, sm.beta, sm.log_w, SweepView<NB>(sm.sw[cur], K));
+    if (tid == 0) {
+      sm.sc[kLl] = *SweepView<NB>(sm.sw[cur], K).ll;
+      sm.sc[kLlPrev] = 0.0;
+      sm.sc[kLikdif] = 0.0;
+      sm.sc[kStep] = 0.0;
+      sm.sc[kBacktracks] = 0.0;
+    }
+    __syncthreads();
+
+    for (;;) {
+      const double step = sm.sc[kStep];
+      const bool go = step == 0.0 || (sm.sc[kLikdif] > ctl.eps && step < static_cast<double>(ctl.max_iter));
+      __syncthreads();
+      if (!go) break;
+      SweepView<NB> c(sm.sw[cur], K);
+      SweepView<NB> tr(sm.sw[cur ^ 1], K);
+      if (tid == 0) sm.sc[kStep] = step + 1.0;
+      // Schur complement of the random-effect block and the step (pml.rs:1660-1710)
+      for (int s = tid; s < K; s += blockDim.x) {
+        sm.vw_step[s] = c.vw[s];
+        sm.dwvw[s] = c.dw[s] / c.vw[s];
+        sm.damp_log_w[s] = 1.0;
+      }
+      if (tid < NB) sm.damp_beta[tid] = 1.0;
+      __syncthreads();
+      if (tid < Dims<NB>::T) {
+        int a = 0, rem = tid;
+        while (rem >= NB - a) {
+          rem -= NB - a;
+          ++a;
+        }
+        const int b = a + rem;
+        double acc = 0.0;
+        for (int s = 0; s < K; ++s) acc += c.vwb[s * NB + a] * c.vwb[s * NB + b] / c.vw[s];
+        const double v = c.vb[a * NB + b] - acc;
+        sm.vb2[a * NB + b] = v;
+        sm.vb2[b * NB + a] = v;
+        sm.factor[a * NB + b] = v;
+        sm.factor[b * NB + a] = v;
+      } else if (tid >= 64 && tid < 64 + NB) {
+        const int j = tid - 64;
+        double acc = 0.0;
+        for (int s = 0; s < K; ++s) acc += c.vwb[s * NB + j] * sm.dwvw[s];
+        sm.step_beta[j] = c.db[j] - acc;
+      }
+      __syncthreads();
+      if (tid == 0) ldlt_solve<NB>(sm.factor, sm.step_beta);
+      __syncthreads();
+      for (int s = tid; s < K; s += blockDim.x) {
+        double acc = 0.0;
+#pragma unroll
+        for (int j = 0; j < NB; ++j) acc += c.vwb[s * NB + j] * sm.step_beta[j];
+        sm.step_log_w[s] = sm.dwvw[s] - acc / c.vw[s];
+        sm.new_log_w[s] = sm.log_w[s] + sm.step_log_w[s];
+      }
+      if (tid < NB) sm.new_beta[tid] = sm.beta[tid] + sm.step_beta[tid];
+      if (tid == 0) sm.sc[kLlPrev] = sm.sc[kLl];
+      __syncthreads();
+      sweep<NB>(d, sm, gene, sm.new_beta, sm.new_log_w, tr);
+      if (tid == 0) {
+        sm.sc[kLl] = *tr.ll;
+        sm.sc[kLikdif] = sm.sc[kLl] - sm.sc[kLlPrev];
+        sm.sc[kBacktracks] = 0.0;
+        sm.sc[kMinStep] = kStepCutoff;
+        sm.sc[kStop] = 0.0;
+      }
+      __syncthreads();
+      // backtracking (pml.rs:1716-1760)
+      for (;;) {
+        const double ll = sm.sc[kLl];
+        const bool again = sm.sc[kLikdif] < 0.0 || isinf(ll);
+        __syncthreads();
+        if (!again) break;
+        if (tid == 0) {
+          const double bt = sm.sc[kBacktracks] + 1.0;
+          sm.sc[kBacktracks] = bt;
+          sm.sc[kMinStep] = sm.sc[kMinStep] / 2.0;
+          if (bt > static_cast<double>(ctl.max_backtrack)) {
+            sm.sc[kLikdif] = 0.0;
+            sm.sc[kLl] = sm.sc[kLlPrev];
+            double gb = 0.0, gw = 0.0;
+            for (int j = 0; j < NB; ++j) gb = fmax(gb, fabs(c.db[j]));
+            for (int s = 0; s < K; ++s) gw = fmax(gw, fabs(c.dw[s]));
+            if (gb > kGradientTolerance || gw > kGradientTolerance) sm.sc[kBacktracks] = bt + 1.0;
+            sm.sc[kStop] = 1.0;
+          }
+        }
+        __syncthreads();
+        if (sm.sc[kStop] != 0.0) break;
+        const double min_step = sm.sc[kMinStep];
+        if (tid < NB) {
+          const double dd = sm.step_beta[tid];
+          if (dd < kStepCutoff && dd > -kStepCutoff) {
+            sm.damp_beta[tid] /= 2.0;
+            sm.new_beta[tid] = sm.beta[tid] + dd * sm.damp_beta[tid];
+          } else if (dd > 0.0) {
+            sm.new_beta[tid] = sm.beta[tid] + min_step;
+          } else {
+            sm.new_beta[tid] = sm.beta[tid] - min_step;
+          }
+        }
+        for (int s = tid; s < K; s += blockDim.x) {
+          const double dd = sm.step_log_w[s];
+          if (dd < kStepCutoff && dd > -kStepCutoff) {
+            sm.damp_log_w[s] /= 2.0;
+            sm.new_log_w[s] = sm.log_w[s] + dd * sm.damp_log_w[s];
+          } else if (dd > 0.0) {
+            sm.new_log_w[s] = sm.log_w[s] + min_step;
+          } else {
+            sm.new_log_w[s] = sm.log_w[s] - min_step;
+          }
+        }
+        __syncthreads();
+        sweep<NB>(d, sm, gene, sm.new_beta, sm.new_log_w, tr);
+        if (tid == 0) {
+          sm.sc[kLl] = *tr.ll;
+          sm.sc[kLikdif] = sm.sc[kLl] - sm.sc[kLlPrev];
+        }
+        __syncthreads();
+      }
+      // accept the trial point as the new iterate
+      if (tid < NB) sm.beta[tid] = sm.new_beta[tid];
+      for (int s = tid; s < K; s += blockDim.x) sm.log_w[s] = sm.new_log_w[s];
+      cur ^= 1;
+      __syncthreads();
+    }
+
+    // log-determinant from the previous iterate's vw (pml.rs:1767-1777)
+    if (tid == 0) {
+      double log_det = 0.0;
+      for (int s = 0; s < K; ++s) log_det += nb_log(fabs(sm.vw_step[s]));
+      if (req.reml) {
+        for (int i = 0; i < NB * NB; ++i) sm.factor[i] = sm.vb2[i];
+        log_det += nb_log(fabs(determinant<NB>(sm.factor)));
+      }
+      sm.sc[kLogDet] = log_det;
+      sm.sc[kSecond] = 0.0;
+    }
+    __syncthreads();
+    // higher-order Laplace correction at the final iterate (pml.rs:1828-1919)
+    if (req.ord > 1) {
+      SweepView<NB> c(sm.sw[cur], K);
+      sweep_sums<NB, 1>(d, sm, gene, sm.beta, sm.log_w, sm.sc[kGamma]);
+      if (tid == 0) {
+        const double gamma = sm.sc[kGamma], lambda = sm.sc[kLambda];
+        const bool high = req.ord > 2;
+        double third_acc = 0.0, fourth_acc = 0.0, fifth_acc = 0.0;
+        for (int s = 0; s < K; ++s) {
+          const double* S = sm.slots_sparse + s * Dims<NB>::NS;
+          const double prior = lambda * c.w[s];
+          const double vw = gamma * S[0] + prior;
+          const double third = gamma * S[1] + prior;
+          third_acc += third * third / (vw * vw * vw);
+          if (high) {
+            const double fourth = gamma * S[2] + prior;
+            const double fifth = gamma * S[3] + prior;
+            const double vs = vw * vw;
+            fourth_acc += fourth / vs;
+            fifth_acc += fifth * third / (vs * vs);
+          }
+        }
+        double second = 5.0 * third_acc / 24.0;
+        if (high) {
+          second -= fourth_acc / 8.0;
+          second += 7.0 * fifth_acc / 48.0;
+        }
+        sm.sc[kSecond] = second;
+        sm.sc[kSweeps] += 1.0;
+      }
+      __syncthreads();
+    }
+    if (tid < NB) out->beta[tid] = sm.beta[tid];
+    for (int i = tid; i < NB * NB; i += blockDim.x) out->information[i] = sm.vb2[i];
+    if (tid == 0) {
+      out->log_likelihood = sm.sc[kLl];
+      out->log_likelihood_prev = sm.sc[kLlPrev];
+      out->log_det = sm.sc[kLogDet];
+      out->second_order = sm.sc[kSecond];
+      out->iterations = static_cast<int32_t>(sm.sc[kStep]);
+      out->backtracks = static_cast<int32_t>(sm.sc[kBacktracks]);
+      out->sweeps = static_cast<int32_t>(sm.sc[kSweeps]);
+      out->status = 0;
+    }
+  }
+}
+
+template <int NB>
+size_t smem_for(int K) {
+  return Smem<NB>::bytes(K);
+}
+
+// Opts the kernel into the dynamic shared memory one CTA needs; the
+// attribute may not exceed the per-block opt-in limit less the kernel's
+// static shared memory.
+template <int NB>
+cudaError_t configure_nb(size_t smem) {
+  return cudaFuncSetAttribute(fit_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              static_cast<int>(smem));
+}
+
+template <int NB>
+int launch_nb(const GeneData& d, const FitControl& ctl, const FitRequest* req, FitResult* res,
+              const int32_t* n_req, int32_t* counter, int grid, cudaStream_t stream) {
+  const size_t smem = Smem<NB>::bytes(d.n_subjects);
+  cudaError_t e = configure_nb<NB>(smem);
+  if (e != cudaSuccess) return e;
+  fit_kernel<NB><<<grid, kThreads, smem, stream>>>(d, ctl, req, res, n_req, counter);
+  return cudaGetLastError();
+}
+
+template <int NB>
+int blocks_nb(int K) {
+  int blocks = 0;
+  const size_t smem = Smem<NB>::bytes(K);
+  if (configure_nb<NB>(smem) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fit_kernel<NB>, kThreads, smem) != cudaSuccess)
+    return 0;
+  return blocks;
+}
+
+}  // namespace
+
+size_t fit_smem_bytes(int n_subjects, int n_coef) {
+  switch (n_coef) {
+    case 1: return smem_for<1>(n_subjects);
+    case 2: return smem_for<2>(n_subjects);
+    case 3: return smem_for<3>(n_subjects);
+    case 4: return smem_for<4>(n_subjects);
+    case 5: return smem_for<5>(n_subjects);
+    case 6: return smem_for<6>(n_subjects);
+    case 7: return smem_for<7>(n_subjects);
+    case 8: return smem_for<8>(n_subjects);
+    default: return 0;
+  }
+}
+
+int fit_blocks_per_sm(int n_subjects, int n_coef) {
+  switch (n_coef) {
+    case 1: return blocks_nb<1>(n_subjects);
+    case 2: return blocks_nb<2>(n_subjects);
+    case 3: return blocks_nb<3>(n_subjects);
+    case 4: return blocks_nb<4>(n_subjects);
+    case 5: return blocks_nb<5>(n_subjects);
+    case 6: return blocks_nb<6>(n_subjects);
+    case 7: return blocks_nb<7>(n_subjects);
+    case 8: return blocks_nb<8>(n_subjects);
+    default: return 0;
+  }
+}
+
+int launch_fit(const GeneData& d, const FitControl& ctl, const FitRequest* req, FitResult* res,
+               const int32_t* n_req, int32_t* counter, int grid, void* stream) {
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  switch (d.n_coef) {
+    case 1: return launch_nb<1>(d, ctl, req, res, n_req, counter, grid, s);
+    case 2: return launch_nb<2>(d, ctl, req, res, n_req, counter, grid, s);
+    case 3: return launch_nb<3>(d, ctl, req, res, n_req, counter, grid, s);
+    case 4: return launch_nb<4>(d, ctl, req, res, n_req, counter, grid, s);
+    case 5: return launch_nb<5>(d, ctl, req, res, n_req, counter, grid, s);
+    case 6: return launch_nb<6>(d, ctl, req, res, n_req, counter, grid, s);
+    case 7: return launch_nb<7>(d, ctl, req, res, n_req, counter, grid, s);
+    case 8: return launch_nb<8>(d, ctl, req, res, n_req, counter, grid, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace device
+}  // namespace nebula

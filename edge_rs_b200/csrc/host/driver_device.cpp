@@ -1,0 +1,493 @@
+// nebula_sparse_cuda: the drop-in for nebula_sparse (src/sc/nebula.rs:434-445)
+// with every penalised inner fit on the GPU.
+//
+// Mirrors the reference's device path (src/gpu/stage_two.rs:281-320 fit_all,
+// :362-544 search_all) but keeps the finish on the device: stage one runs on
+// host threads; stage two advances every gene's search in lockstep, one
+// batched launch per round holding each search's pending point(s); stage
+// three batches the final fit of every gene into one more launch. The host
+// only steps the searches and assembles the objective from the four scalars
+// each device fit returns.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <mutex>
+#include <thread>
+
+#include "../cuda/pml_device.cuh"
+#include "common.hpp"
+#include "driver_device.hpp"
+#include "export.hpp"
+#include "search.hpp"
+#include "stage_one.hpp"
+
+namespace nebula {
+namespace {
+
+using Clock = std::chrono::steady_clock;
+double ms_since(Clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+}
+
+void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) fail(NB_ERR_GPU, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename F>
+void parallel_for(size_t n, int threads, F&& f) {
+  int nt = threads > 0 ? threads : static_cast<int>(std::thread::hardware_concurrency());
+  nt = std::max(1, std::min<int>(nt, static_cast<int>(n)));
+  std::atomic<size_t> next{0};
+  std::mutex err_mu;
+  std::optional<std::pair<size_t, NbError>> first_err;
+  auto worker = [&]() {
+    for (;;) {
+      size_t i = next.fetch_add(1);
+      if (i >= n) return;
+      try {
+        f(i);
+      } catch (const NbError& e) {
+        std::lock_guard<std::mutex> lock(err_mu);
+        if (!first_err || i < first_err->first) first_err = std::make_pair(i, e);
+      }
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nt; ++t) pool.emplace_back(worker);
+  worker();
+  for (auto& th : pool) th.join();
+  if (first_err) throw first_err->second;
+}
+
+template <typename T>
+T* device_copy(const T* host, size_t n, std::vector<void*>* owned) {
+  T* d = nullptr;
+  cuda_check(cudaMalloc(reinterpret_cast<void**>(&d), std::max<size_t>(n, 1) * sizeof(T)), "cudaMalloc");
+  owned->push_back(d);
+  if (n) cuda_check(cudaMemcpy(d, host, n * sizeof(T), cudaMemcpyHostToDevice), "cudaMemcpy H2D");
+  return d;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Resident device copy of one call's inputs, and the per-round launch.
+
+DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& genes, int device) {
+  const Shared& sh = prep.shared;
+  if (device >= 0) cuda_check(cudaSetDevice(device), "cudaSetDevice");
+  cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  const int K = sh.n_subjects;
+  const size_t G = genes.size();
+  std::vector<uint64_t> gene_ptr(G + 1, 0);
+  for (size_t g = 0; g < G; ++g) gene_ptr[g + 1] = gene_ptr[g] + genes[g].cells.size();
+  const size_t nnz = gene_ptr[G];
+  std::vector<uint32_t> cells(nnz);
+  std::vector<double> counts(nnz), totals(G * K);
+  std::vector<uint64_t> runs(G * (K + 1));
+  for (size_t g = 0; g < G; ++g) {
+    const GeneCounts& gc = genes[g];
+    std::copy(gc.cells.begin(), gc.cells.end(), cells.begin() + gene_ptr[g]);
+    std::copy(gc.counts.begin(), gc.counts.end(), counts.begin() + gene_ptr[g]);
+    std::copy(prep.totals.begin() + prep.kept[g] * K, prep.totals.begin() + (prep.kept[g] + 1) * K,
+              totals.begin() + g * K);
+    // positive_runs (pml.rs:1155-1160) as absolute positions
+    for (int s = 0; s <= K; ++s) {
+      uint64_t b = sh.fid[s];
+      auto it = std::lower_bound(gc.cells.begin(), gc.cells.end(), b,
+                                 [](uint32_t c, uint64_t v) { return c < v; });
+      runs[g * (K + 1) + s] = gene_ptr[g] + static_cast<uint64_t>(it - gc.cells.begin());
+    }
+  }
+  std::vector<uint32_t> fid(sh.fid.begin(), sh.fid.end());
+  std::vector<uint32_t> wcells(device::kWarps + 1);
+  for (int w = 0; w <= device::kWarps; ++w)
+    wcells[w] = static_cast<uint32_t>(sh.n_cells * static_cast<size_t>(w) / device::kWarps);
+
+  data_.design = device_copy(sh.design.data(), sh.design.size(), &owned_);
+  data_.log_offset = device_copy(sh.log_offset.data(), sh.log_offset.size(), &owned_);
+  data_.fid = device_copy(fid.data(), fid.size(), &owned_);
+  data_.gene_ptr = device_copy(gene_ptr.data(), gene_ptr.size(), &owned_);
+  data_.cells = device_copy(cells.data(), cells.size(), &owned_);
+  data_.counts = device_copy(counts.data(), counts.size(), &owned_);
+  data_.runs = device_copy(runs.data(), runs.size(), &owned_);
+  data_.totals = device_copy(totals.data(), totals.size(), &owned_);
+  data_.warp_cells = device_copy(wcells.data(), wcells.size(), &owned_);
+  data_.n_cells = static_cast<int32_t>(sh.n_cells);
+  data_.n_subjects = K;
+  data_.n_coef = sh.n_coef;
+  ctl_.eps = sh.params.eps;
+  ctl_.max_iter = kPmlMaxIter;
+  ctl_.max_backtrack = kPmlMaxBacktrack;
+
+  int sms = 0, dev = 0;
+  cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+  cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute");
+  int per_sm = device::fit_blocks_per_sm(K, sh.n_coef);
+  if (per_sm <= 0)
+    fail(NB_ERR_UNSUPPORTED, "the fit kernel cannot be resident with " + std::to_string(K) +
+                                 " subjects and " + std::to_string(sh.n_coef) + " columns");
+  grid_ = per_sm * sms;
+  cuda_check(cudaMalloc(&d_counter_, 2 * sizeof(int32_t)), "cudaMalloc");
+  owned_.push_back(d_counter_);
+  cuda_check(cudaEventCreate(&ev0_), "event");
+  cuda_check(cudaEventCreate(&ev1_), "event");
+}
+
+DeviceFitter::~DeviceFitter() {
+  for (void* p : owned_) cudaFree(p);
+  if (d_req_) cudaFree(d_req_);
+  if (d_res_) cudaFree(d_res_);
+  if (h_req_) cudaFreeHost(h_req_);
+  if (h_res_) cudaFreeHost(h_res_);
+  if (ev0_) cudaEventDestroy(ev0_);
+  if (ev1_) cudaEventDestroy(ev1_);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+void DeviceFitter::reserve(size_t n) {
+  if (n <= capacity_) return;
+  size_t cap = std::max<size_t>(n, capacity_ * 2);
+  if (d_req_) cudaFree(d_req_);
+  if (d_res_) cudaFree(d_res_);
+  if (h_req_) cudaFreeHost(h_req_);
+  if (h_res_) cudaFreeHost(h_res_);
+  cuda_check(cudaMalloc(reinterpret_cast<void**>(&d_req_), cap * sizeof(device::FitRequest)), "cudaMalloc");
+  cuda_check(cudaMalloc(reinterpret_cast<void**>(&d_res_), cap * sizeof(device::FitResult)), "cudaMalloc");
+  cuda_check(cudaMallocHost(reinterpret_cast<void**>(&h_req_), cap * sizeof(device::FitRequest)), "cudaMallocHost");
+  cuda_check(cudaMallocHost(reinterpret_cast<void**>(&h_res_), cap * sizeof(device::FitResult)), "cudaMallocHost");
+  capacity_ = cap;
+}
+
+const device::FitResult* DeviceFitter::run(const std::vector<device::FitRequest>& reqs) {
+  const size_t n = reqs.size();
+  if (n == 0) return nullptr;
+  reserve(n);
+  std::memcpy(h_req_, reqs.data(), n * sizeof(device::FitRequest));
+  int32_t header[2] = {static_cast<int32_t>(n), 0};
+  cuda_check(cudaMemcpyAsync(d_req_, h_req_, n * sizeof(device::FitRequest), cudaMemcpyHostToDevice, stream_),
+             "request copy");
+  cuda_check(cudaMemcpyAsync(d_counter_, header, sizeof(header), cudaMemcpyHostToDevice, stream_), "count copy");
+  cuda_check(cudaEventRecord(ev0_, stream_), "event");
+  int grid = static_cast<int>(std::min<size_t>(grid_, n));
+  cuda_check(static_cast<cudaError_t>(device::launch_fit(data_, ctl_, d_req_, d_res_, d_counter_, d_counter_ + 1,
+                                                          grid, stream_)),
+             "fit kernel launch");
+  cuda_check(cudaEventRecord(ev1_, stream_), "event");
+  cuda_check(cudaMemcpyAsync(h_res_, d_res_, n * sizeof(device::FitResult), cudaMemcpyDeviceToHost, stream_),
+             "result copy");
+  cuda_check(cudaStreamSynchronize(stream_), "fit kernel");
+  float ms = 0.0f;
+  cuda_check(cudaEventElapsedTime(&ms, ev0_, ev1_), "event time");
+  device_ms_ += ms;
+  ++launches_;
+  requests_ += n;
+  for (size_t i = 0; i < n; ++i) {
+    sweeps_ += static_cast<uint64_t>(h_res_[i].sweeps);
+  }
+  return h_res_;
+}
+
+// ---------------------------------------------------------------------------
+
+namespace {
+
+struct GeneTask {
+  GenePlan plan;
+  std::unique_ptr<StageTwoSearch> search;
+  VarianceObjective objective;
+  std::optional<std::optional<std::pair<std::vector<double>, bool>>> refit;
+};
+
+void write_err(char* err, size_t len, const std::string& msg) {
+  if (!err || len == 0) return;
+  size_t n = std::min(len - 1, msg.size());
+  std::memcpy(err, msg.data(), n);
+  err[n] = 0;
+}
+
+}  // namespace
+
+int32_t run_nebula_device(const nb_csr* counts, const uint64_t* subject_id, const double* design,
+                          uint32_t n_coef, const double* offset, const nb_params* params,
+                          const nb_options* options, nb_fit* out, nb_stats* stats, char* err,
+                          size_t err_len) {
+  const auto t_start = Clock::now();
+  try {
+    if (!out) fail(NB_ERR_INVALID_ARGUMENT, "out is null");
+    nb_options opt{};
+    opt.device = -1;
+    opt.audit_percent = 5;
+    if (options) opt = *options;
+    if (n_coef > static_cast<uint32_t>(device::kMaxCoef))
+      fail(NB_ERR_UNSUPPORTED, "the device path takes at most 8 design columns");
+    Prepared prep = prepare(counts, subject_id, design, n_coef, offset, params);
+    const Shared& sh = prep.shared;
+    const size_t G = prep.kept.size();
+    std::vector<GeneCounts> genes(G);
+    for (size_t g = 0; g < G; ++g) genes[g] = positive_indices(prep.counts, prep.kept[g]);
+    const double ms_prepare = ms_since(t_start);
+
+    // stage one on host threads (nebula.rs:812-901)
+    auto t1 = Clock::now();
+    std::vector<GeneTask> tasks(G);
+    parallel_for(G, opt.host_threads, [&](size_t g) {
+      tasks[g].plan = plan_gene(sh, genes[g], &prep.totals[prep.kept[g] * sh.n_subjects]);
+    });
+    const double ms_stage_one = ms_since(t1);
+
+    DeviceFitter fitter(prep, genes, opt.device);
+
+    // stage two: every search in lockstep, one launch per round
+    auto t2 = Clock::now();
+    std::vector<size_t> active;
+    for (size_t g = 0; g < G; ++g) {
+      GeneTask& t = tasks[g];
+      if (t.plan.refit == Refit::None) continue;
+      std::optional<double> fixed_cell;
+      std::vector<double> start;
+      if (t.plan.refit == Refit::Both) {
+        start = {t.plan.sigma, t.plan.gamma};
+      } else {
+        start = {t.plan.sigma};
+        fixed_cell = t.plan.gamma;
+      }
+      std::vector<double> lower, upper;
+      variance_bounds(sh.params, fixed_cell.has_value(), &lower, &upper);
+      t.search = std::make_unique<StageTwoSearch>(start, lower, upper, t.plan.ord);
+      t.objective = VarianceObjective::make(sh, genes[g], fixed_cell);
+      active.push_back(g);
+    }
+    struct Slot {
+      size_t gene;
+      size_t point;
+      double subject, cell;
+      int request;  // index into the batch, -1 when the point is outside the domain
+    };
+    std::vector<device::FitRequest> batch;
+    std::vector<Slot> slots;
+    uint64_t rounds = 0;
+    while (!active.empty()) {
+      batch.clear();
+      slots.clear();
+      for (size_t g : active) {
+        GeneTask& t = tasks[g];
+        const auto& points = t.search->ask();
+        for (size_t p = 0; p < points.size(); ++p) {
+          double subject = 0.0, cell = 0.0;
+          std::vector<double> beta;
+          Slot slot{g, p, 0.0, 0.0, -1};
+          if (t.objective.request(points[p], t.plan.beta_start, &subject, &cell, &beta)) {
+            device::FitRequest r{};
+            r.gene = static_cast<int32_t>(g);
+            r.ord = t.search->order();
+            r.reml = sh.params.reml ? 1 : 0;
+            r.subject = subject;
+            r.cell = cell;
+            for (int j = 0; j < sh.n_coef; ++j) r.beta[j] = beta[j];
+            slot.subject = subject;
+            slot.cell = cell;
+            slot.request = static_cast<int>(batch.size());
+            batch.push_back(r);
+          }
+          slots.push_back(slot);
+        }
+      }
+      const device::FitResult* res = fitter.run(batch);
+      ++rounds;
+      std::vector<double> values;
+      size_t si = 0;
+      std::vector<size_t> still;
+      for (size_t g : active) {
+        GeneTask& t = tasks[g];
+        const size_t n_points = t.search->ask().size();
+        values.assign(n_points, std::numeric_limits<double>::infinity());
+        for (size_t p = 0; p < n_points; ++p, ++si) {
+          const Slot& s = slots[si];
+          if (s.request < 0) continue;
+          const device::FitResult& r = res[s.request];
+          if (r.status != 0) continue;
+          InnerFit fit{r.log_likelihood, r.log_likelihood_prev, r.log_det, r.second_order};
+          values[p] = t.objective.assemble(s.subject, s.cell, fit, t.objective.tail(s.cell));
+        }
+        t.search->tell(values);
+        if (t.search->done()) {
+          t.refit = t.search->result();
+          t.search.reset();
+        } else {
+          still.push_back(g);
+        }
+      }
+      active.swap(still);
+    }
+    const double ms_stage_two = ms_since(t2);
+
+    // stage three: one final fit per gene at order one (nebula.rs:948-967)
+    auto t3 = Clock::now();
+    std::vector<double> sigma(G), gamma(G);
+    std::vector<int> conv(G);
+    batch.clear();
+    for (size_t g = 0; g < G; ++g) {
+      apply_refit(tasks[g].plan, tasks[g].refit, &sigma[g], &gamma[g], &conv[g]);
+      device::FitRequest r{};
+      r.gene = static_cast<int32_t>(g);
+      r.ord = 1;
+      r.reml = sh.params.reml ? 1 : 0;
+      r.subject = sigma[g];
+      r.cell = gamma[g];
+      for (int j = 0; j < sh.n_coef; ++j) r.beta[j] = tasks[g].plan.beta_start[j];
+      r.beta[sh.intercept] -= sigma[g] / 2.0;
+      batch.push_back(r);
+    }
+    const device::FitResult* res = fitter.run(batch);
+    std::vector<GeneOutcome> outcomes(G);
+    for (size_t g = 0; g < G; ++g) {
+      const device::FitResult& r = res[g];
+      if (r.status != 0) fail(NB_ERR_INVALID_ARGUMENT, "opt_pml rejected the final variance components");
+      FinalFit ff;
+      ff.beta.assign(r.beta, r.beta + sh.n_coef);
+      ff.information.resize(static_cast<size_t>(sh.n_coef) * sh.n_coef);
+      for (int a = 0; a < sh.n_coef; ++a)
+        for (int b = 0; b < sh.n_coef; ++b) ff.information[a * sh.n_coef + b] = r.information[a * sh.n_coef + b];
+      ff.log_likelihood = r.log_likelihood;
+      ff.iterations = r.iterations;
+      ff.backtracks = r.backtracks;
+      outcomes[g] = finish_gene(sh, sigma[g], gamma[g], conv[g], ff);
+    }
+    const double ms_stage_three = ms_since(t3);
+    assemble_fit(sh, outcomes, prep.kept, out);
+    if (stats) {
+      *stats = nb_stats{};
+      stats->rounds = rounds;
+      stats->requests = fitter.requests();
+      stats->sweeps = fitter.sweeps();
+      stats->cell_visits = 0;
+      stats->gpu_launches = fitter.launches();
+      stats->ms_prepare = ms_prepare;
+      stats->ms_stage_one = ms_stage_one;
+      stats->ms_stage_two = ms_stage_two;
+      stats->ms_stage_three = ms_stage_three;
+      stats->ms_device = fitter.device_ms();
+      stats->ms_total = ms_since(t_start);
+    }
+    return NB_OK;
+  } catch (const NbError& e) {
+    write_err(err, err_len, e.message);
+    return e.code;
+  }
+}
+
+}  // namespace nebula
+
+NB_API void nb_params_default(nb_params* p) {
+  if (!p) return;
+  nebula::Params d;
+  p->min_subject = d.min0;
+  p->min_cell = d.min1;
+  p->max_subject = d.max0;
+  p->max_cell = d.max1;
+  p->method = d.method;
+  p->cutoff_cell = d.cutoff_cell;
+  p->kappa = d.kappa;
+  p->cpc = d.cpc;
+  p->mincp = d.mincp;
+  p->min_subjects = d.min_subjects;
+  p->reml = d.reml ? 1 : 0;
+  p->eps = d.eps;
+}
+
+NB_API int32_t nebula_sparse_cuda(const nb_csr* counts, const uint64_t* subject_id, const double* design,
+                                  uint32_t n_coef, const double* offset_or_null,
+                                  const nb_params* params_or_null, nb_fit* out, char* err, size_t err_len) {
+  return nebula::run_nebula_device(counts, subject_id, design, n_coef, offset_or_null, params_or_null,
+                                   nullptr, out, nullptr, err, err_len);
+}
+
+NB_API int32_t nebula_sparse_cuda_ex(const nb_csr* counts, const uint64_t* subject_id, const double* design,
+                                     uint32_t n_coef, const double* offset_or_null,
+                                     const nb_params* params_or_null, const nb_options* options, nb_fit* out,
+                                     nb_stats* stats, char* err, size_t err_len) {
+  return nebula::run_nebula_device(counts, subject_id, design, n_coef, offset_or_null, params_or_null, options,
+                                   out, stats, err, err_len);
+}
+
+// opt_pml (src/sc/pml.rs:468-508) for a batch of variance points of one
+// gene, on the device; the batched twin of the reference's device entry
+// (src/gpu/nebula_gpu.rs:466-594 opt_pml_batch). scalars_out per request:
+// log_likelihood, log_likelihood_prev, log_det, second_order; ints_out:
+// status (0 ok, 1 rejected arguments), iterations, backtracks, sweeps.
+NB_API int32_t nb_opt_pml_cuda(const double* design, const double* offset, uint64_t n_cells, uint32_t n_beta,
+                               const double* counts, const uint32_t* cells, uint64_t n_pos,
+                               const uint64_t* subject_start, uint32_t k, const double* subject_total,
+                               uint32_t n_requests, const double* beta_init, const double* subject,
+                               const double* cell, const int32_t* ord, int32_t reml, double eps,
+                               double* beta_out, double* information_out, double* scalars_out,
+                               int32_t* ints_out, char* err, size_t err_len) {
+  using namespace nebula;
+  try {
+    if (n_beta == 0 || n_beta > static_cast<uint32_t>(device::kMaxCoef))
+      fail(NB_ERR_UNSUPPORTED, "the device path takes 1 to 8 design columns");
+    if (k == 0 || n_cells == 0) fail(NB_ERR_MUST_BE_POSITIVE, "need cells and subjects");
+    if (subject_start[0] != 0 || subject_start[k] != n_cells)
+      fail(NB_ERR_INVALID_ARGUMENT, "subject_start must run from 0 to n_cells");
+    for (uint32_t s = 0; s < k; ++s)
+      if (subject_start[s] >= subject_start[s + 1])
+        fail(NB_ERR_SUBJECTS_NOT_CONTIGUOUS, "empty or unordered subject block");
+    for (uint64_t i = 0; i < n_pos; ++i)
+      if (cells[i] >= n_cells || (i > 0 && cells[i] <= cells[i - 1]))
+        fail(NB_ERR_INVALID_ARGUMENT, "Cell indices must be strictly increasing and in range.");
+    Prepared prep;
+    Shared& sh = prep.shared;
+    sh.design.assign(design, design + n_cells * n_beta);
+    sh.log_offset.assign(offset, offset + n_cells);
+    sh.fid.assign(subject_start, subject_start + k + 1);
+    sh.n_cells = n_cells;
+    sh.n_coef = static_cast<int>(n_beta);
+    sh.n_subjects = static_cast<int>(k);
+    sh.params.eps = eps;
+    prep.totals.assign(subject_total, subject_total + k);
+    prep.kept = {0};
+    std::vector<GeneCounts> genes(1);
+    genes[0].cells.assign(cells, cells + n_pos);
+    genes[0].counts.assign(counts, counts + n_pos);
+    DeviceFitter fitter(prep, genes, -1);
+    std::vector<device::FitRequest> reqs(n_requests);
+    for (uint32_t q = 0; q < n_requests; ++q) {
+      device::FitRequest& r = reqs[q];
+      r = device::FitRequest{};
+      r.gene = 0;
+      r.ord = ord ? ord[q] : 1;
+      r.reml = reml;
+      r.subject = subject[q];
+      r.cell = cell[q];
+      for (uint32_t j = 0; j < n_beta; ++j) r.beta[j] = beta_init[q * n_beta + j];
+    }
+    const device::FitResult* res = fitter.run(reqs);
+    for (uint32_t q = 0; q < n_requests; ++q) {
+      const device::FitResult& r = res[q];
+      for (uint32_t j = 0; j < n_beta; ++j) beta_out[q * n_beta + j] = r.beta[j];
+      for (uint32_t j = 0; j < n_beta * n_beta; ++j) information_out[q * n_beta * n_beta + j] = r.information[j];
+      scalars_out[q * 4 + 0] = r.log_likelihood;
+      scalars_out[q * 4 + 1] = r.log_likelihood_prev;
+      scalars_out[q * 4 + 2] = r.log_det;
+      scalars_out[q * 4 + 3] = r.second_order;
+      ints_out[q * 4 + 0] = r.status;
+      ints_out[q * 4 + 1] = r.iterations;
+      ints_out[q * 4 + 2] = r.backtracks;
+      ints_out[q * 4 + 3] = r.sweeps;
+    }
+    return NB_OK;
+  } catch (const NbError& e) {
+    if (err && err_len) {
+      size_t n = std::min(err_len - 1, e.message.size());
+      std::memcpy(err, e.message.data(), n);
+      err[n] = 0;
+    }
+    return e.code;
+  }
+}

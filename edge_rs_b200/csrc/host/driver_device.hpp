@@ -1,0 +1,54 @@
+// The product driver's resident device state and per-round launch.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "../cuda/pml_device.cuh"
+#include "common.hpp"
+
+namespace nebula {
+
+// Owns one call's device copy of the design, offsets and kept genes' counts,
+// and runs batches of inner fits on them.
+class DeviceFitter {
+ public:
+  DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& genes, int device);
+  ~DeviceFitter();
+  DeviceFitter(const DeviceFitter&) = delete;
+  DeviceFitter& operator=(const DeviceFitter&) = delete;
+
+  // Runs one batch; the returned results (pinned host memory) stay valid
+  // until the next call.
+  const device::FitResult* run(const std::vector<device::FitRequest>& reqs);
+
+  double device_ms() const { return device_ms_; }
+  uint64_t launches() const { return launches_; }
+  uint64_t requests() const { return requests_; }
+  uint64_t sweeps() const { return sweeps_; }
+
+ private:
+  void reserve(size_t n);
+  cudaStream_t stream_ = nullptr;
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  device::GeneData data_{};
+  device::FitControl ctl_{};
+  std::vector<void*> owned_;
+  int32_t* d_counter_ = nullptr;  // [0] request count, [1] work-queue counter
+  device::FitRequest* d_req_ = nullptr;
+  device::FitResult* d_res_ = nullptr;
+  device::FitRequest* h_req_ = nullptr;
+  device::FitResult* h_res_ = nullptr;
+  size_t capacity_ = 0;
+  int grid_ = 0;
+  double device_ms_ = 0.0;
+  uint64_t launches_ = 0, requests_ = 0, sweeps_ = 0;
+};
+
+int32_t run_nebula_device(const nb_csr* counts, const uint64_t* subject_id, const double* design,
+                          uint32_t n_coef, const double* offset, const nb_params* params,
+                          const nb_options* options, nb_fit* out, nb_stats* stats, char* err,
+                          size_t err_len);
+
+}  // namespace nebula

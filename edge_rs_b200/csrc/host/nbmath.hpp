@@ -1,0 +1,143 @@
+// exp and log for doubles, compiled identically for the host (g++) and the
+// device (nvcc), so that the CUDA inner fit and its CPU oracle take
+// bit-identical logarithms and exponentials and, with the same summation
+// tree, produce bit-identical sweeps.
+//
+// exp: Cody and Waite's argument reduction x = k ln2 + r with ln2 split in a
+// 32-bit head and a tail, |r| <= ln2 / 2, then the Taylor polynomial of
+// degree 13 in Horner form (truncation below 5e-18 relative), and the scaling
+// by 2^k built from the exponent bits in two factors so that results in the
+// subnormal range round once.
+//
+// log: x = m 2^e with m in [sqrt(1/2), sqrt(2)), f = m - 1, s = f / (2 + f),
+// ln m = 2 atanh(s) = 2s + 2s^3 (1/3 + s^2/5 + ... + s^20/23) with |s| <= 0.1716
+// (truncation below 1e-18), and ln x = e ln2_hi + (e ln2_lo + ln m).
+//
+// Both are within about one ulp of the correctly rounded result (checked
+// against the C library over the ranges the fits use) and handle 0, inf,
+// NaN and subnormals.
+#pragma once
+
+#include <cstdint>
+#include <cstring>
+
+#ifdef __CUDACC__
+#define NB_HD __host__ __device__ __forceinline__
+#else
+#define NB_HD inline
+#include <cmath>
+#endif
+
+namespace nebula {
+
+NB_HD double nb_fma(double a, double b, double c) {
+#ifdef __CUDA_ARCH__
+  return __fma_rn(a, b, c);
+#else
+  return __builtin_fma(a, b, c);
+#endif
+}
+
+NB_HD uint64_t nb_bits(double x) {
+#ifdef __CUDA_ARCH__
+  return static_cast<uint64_t>(__double_as_longlong(x));
+#else
+  uint64_t u;
+  std::memcpy(&u, &x, 8);
+  return u;
+#endif
+}
+
+NB_HD double nb_from_bits(uint64_t u) {
+#ifdef __CUDA_ARCH__
+  return __longlong_as_double(static_cast<long long>(u));
+#else
+  double x;
+  std::memcpy(&x, &u, 8);
+  return x;
+#endif
+}
+
+// 2^k for -1022 <= k <= 1023
+NB_HD double nb_pow2(int k) { return nb_from_bits(static_cast<uint64_t>(k + 1023) << 52); }
+
+NB_HD double nb_rint(double x) {
+  // round to nearest (ties to even) for |x| < 2^51
+  const double shifter = 6755399441055744.0;  // 1.5 * 2^52
+  return (x + shifter) - shifter;
+}
+
+NB_HD double nb_exp(double x) {
+  if (!(x == x)) return x;                      // NaN
+  if (x > 709.782712893384) return 1.0 / 0.0;  // overflow
+  if (x < -745.1332191019412) return 0.0;      // underflow
+  const double log2e = 1.4426950408889634;
+  const double ln2_hi = 6.93147180369123816490e-01;  // ln 2 in 32 bits
+  const double ln2_lo = 1.90821492927058770002e-10;
+  const double k = nb_rint(x * log2e);
+  double r = nb_fma(-k, ln2_hi, x);
+  r = nb_fma(-k, ln2_lo, r);
+  // Taylor coefficients 1/n!, n = 13 .. 2
+  double p = 1.6059043836821613e-10;
+  p = nb_fma(p, r, 2.0876756987868100e-09);
+  p = nb_fma(p, r, 2.5052108385441720e-08);
+  p = nb_fma(p, r, 2.7557319223985893e-07);
+  p = nb_fma(p, r, 2.7557319223985888e-06);
+  p = nb_fma(p, r, 2.4801587301587302e-05);
+  p = nb_fma(p, r, 1.9841269841269841e-04);
+  p = nb_fma(p, r, 1.3888888888888889e-03);
+  p = nb_fma(p, r, 8.3333333333333332e-03);
+  p = nb_fma(p, r, 4.1666666666666664e-02);
+  p = nb_fma(p, r, 1.6666666666666666e-01);
+  p = nb_fma(p, r, 0.5);
+  p = nb_fma(p, r, 1.0);
+  const double er = nb_fma(p, r, 1.0);
+  const int ki = static_cast<int>(k);
+  if (ki >= -1021 && ki <= 1023) return er * nb_pow2(ki);
+  // split the scale so that neither factor leaves the normal range
+  const int k1 = ki / 2;
+  return (er * nb_pow2(k1)) * nb_pow2(ki - k1);
+}
+
+NB_HD double nb_log(double x) {
+  if (!(x == x)) return x;         // NaN
+  if (x < 0.0) return 0.0 / 0.0;   // NaN
+  if (x == 0.0) return -1.0 / 0.0;
+  if (x == 1.0 / 0.0) return x;
+  int e = 0;
+  if (x < 2.2250738585072014e-308) {  // subnormal: scale into the normal range
+    x *= 18014398509481984.0;         // 2^54
+    e = -54;
+  }
+  uint64_t u = nb_bits(x);
+  e += static_cast<int>((u >> 52) & 0x7ff) - 1023;
+  double m = nb_from_bits((u & 0x000fffffffffffffULL) | 0x3ff0000000000000ULL);  // [1, 2)
+  if (m > 1.4142135623730951) {
+    m *= 0.5;
+    e += 1;
+  }
+  const double f = m - 1.0;
+  const double s = f / (2.0 + f);
+  const double z = s * s;
+  // 1/3 + z/5 + ... + z^10/23
+  double q = 1.0 / 23.0;
+  q = nb_fma(q, z, 1.0 / 21.0);
+  q = nb_fma(q, z, 1.0 / 19.0);
+  q = nb_fma(q, z, 1.0 / 17.0);
+  q = nb_fma(q, z, 1.0 / 15.0);
+  q = nb_fma(q, z, 1.0 / 13.0);
+  q = nb_fma(q, z, 1.0 / 11.0);
+  q = nb_fma(q, z, 1.0 / 9.0);
+  q = nb_fma(q, z, 1.0 / 7.0);
+  q = nb_fma(q, z, 1.0 / 5.0);
+  q = nb_fma(q, z, 1.0 / 3.0);
+  // ln m = 2s + 2 s z q, with f - s f kept exact-ish as 2s = f - s f
+  const double two_s = f - s * f;
+  const double lnm = nb_fma(2.0 * s * z, q, two_s);
+  const double ln2_hi = 6.93147180369123816490e-01;
+  const double ln2_lo = 1.90821492927058770002e-10;
+  const double ed = static_cast<double>(e);
+  return nb_fma(ed, ln2_hi, nb_fma(ed, ln2_lo, lnm));
+}
+
+}  // namespace nebula

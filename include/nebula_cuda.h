@@ -135,6 +135,26 @@ int32_t nebula_sparse_cuda_ex(const nb_csr* counts, const uint64_t* subject_id,
                               const nb_options* options, nb_fit* out,
                               nb_stats* stats, char* err, size_t err_len);
 
+/* opt_pml (src/sc/pml.rs:468-508) for a batch of variance points of one
+ * gene on the device (the batched twin of the reference's device entry,
+ * src/gpu/nebula_gpu.rs:466-594). The design is used as given (already
+ * centred), offsets are logs, subject_start has k + 1 boundaries, counts and
+ * cells are the positive entries in increasing cell order. Per request:
+ * beta_init (n_beta), subject (nebula's sigma[0]), cell (NB size), ord.
+ * scalars_out (4 per request): log_likelihood, log_likelihood_prev, log_det,
+ * second_order; ints_out (4 per request): status (0 ok, 1 rejected
+ * arguments), iterations, backtracks, sweeps. */
+int32_t nb_opt_pml_cuda(const double* design, const double* offset,
+                        uint64_t n_cells, uint32_t n_beta, const double* counts,
+                        const uint32_t* cells, uint64_t n_pos,
+                        const uint64_t* subject_start, uint32_t k,
+                        const double* subject_total, uint32_t n_requests,
+                        const double* beta_init, const double* subject,
+                        const double* cell, const int32_t* ord, int32_t reml,
+                        double eps, double* beta_out, double* information_out,
+                        double* scalars_out, int32_t* ints_out, char* err,
+                        size_t err_len);
+
 /* glm_sc_test (src/sc/test.rs:96-200): Wald test of the contrast c per gene,
  * z = c'beta / sqrt(c'Vc), p = chisq_sf(z^2, 1), BH FDR. log_p_value keeps
  * the tail in log space where p underflows. Any output may be NULL. */

@@ -31,14 +31,6 @@ oracle::PmlData pml_view(const Shared& sh, const GeneCounts& gc, const double* t
                          sh.n_subjects, totals};
 }
 
-// VarianceObjective::tail in count order (nebula.rs:1429-1437).
-double tail_in_count_order(const GeneCounts& gc, double cell) {
-  double t = 0.0;
-  for (double y : gc.counts)
-    if (y != 1.0 && y != 2.0) t += ln_gamma(y + cell);
-  return t;
-}
-
 struct GeneStats {
   long evaluations = 0, sweeps = 0;
 };
@@ -80,7 +72,9 @@ GeneOutcome fit_gene_cpu(const Shared& sh, const CsrView& csr, const std::vector
           oracle::PmlResult r;
           if (oracle::opt_pml(data, beta.data(), nullptr, subject, cell, p, oracle::Prior::Gamma, &r)) {
             InnerFit fit{r.log_likelihood, r.log_likelihood_prev, r.log_det, r.second_order};
-            v = objective.assemble(subject, cell, fit, tail_in_count_order(gc, cell));
+            // the lgamma tail over distinct counts (stage_two.rs:746-766), which the
+            // reference pins to the per-count sum of nebula.rs:1429-1437 at 1e-14
+            v = objective.assemble(subject, cell, fit, objective.tail(cell));
             stats->sweeps += r.sweeps;
           }
         }

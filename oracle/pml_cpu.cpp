@@ -1,6 +1,12 @@
 // ORACLE — test infrastructure only (see pml_cpu.hpp). FP64 restatement of
-// the reference's opt_pml, one gene at a time, sequential sums.
+// the reference's opt_pml, one gene at a time. Its sums follow a fixed tree
+// (see tree_sums) and its exp/log are nbmath.hpp's, so that the CUDA kernel,
+// which takes the same tree and the same functions, agrees with it bit for
+// bit; against the R goldens the association of the sums does not matter at
+// their 1e-11 tolerance.
 #include "pml_cpu.hpp"
+
+#include "nbmath.hpp"
 
 #include <algorithm>
 #include <cfloat>
@@ -60,77 +66,171 @@ std::vector<size_t> positive_runs(const PmlData& d) {
   return run;
 }
 
+// The summation tree both this oracle and the CUDA kernel use for a sweep's
+// per-subject sums, so that the two agree bit for bit. Dense part: the cells
+// are cut into kWarps equal contiguous ranges; within a range each subject
+// piece is summed by kLanes strided partial sums (lane l takes cells
+// c0 + l, c0 + l + kLanes, ...), which are then combined by the butterfly
+// v[l] += v[l ^ off] for off = 16, 8, 4, 2, 1 (lane 0's value is kept).
+// Sparse part: each subject's positive entries the same way. A subject's total
+// is 0 + its dense pieces in range order + its sparse piece.
+constexpr int kWarps = 8;
+constexpr int kLanes = 32;
+
+struct Tree {
+  int nv;
+  std::vector<double> lanes, next;  // kLanes x nv each
+  explicit Tree(int n) : nv(n), lanes(static_cast<size_t>(kLanes) * n, 0.0), next(lanes.size()) {}
+  double* lane(int l) { return &lanes[static_cast<size_t>(l) * nv]; }
+  void clear() { std::fill(lanes.begin(), lanes.end(), 0.0); }
+  void reduce(double* out) {
+    for (int off = 16; off > 0; off >>= 1) {
+      for (int l = 0; l < kLanes; ++l) {
+        const double* a = &lanes[static_cast<size_t>(l) * nv];
+        const double* b = &lanes[static_cast<size_t>(l ^ off) * nv];
+        double* o = &next[static_cast<size_t>(l) * nv];
+        for (int v = 0; v < nv; ++v) o[v] = a[v] + b[v];
+      }
+      lanes.swap(next);
+    }
+    for (int v = 0; v < nv; ++v) out[v] = lanes[v];
+  }
+};
+
+size_t warp_start(const PmlData& d, int w) { return d.n_cells * static_cast<size_t>(w) / kWarps; }
+
+int subject_of(const PmlData& d, size_t c) {
+  int s = 0;
+  while (d.subject_start[s + 1] <= c) ++s;
+  return s;
+}
+
+// Runs `cell(lane_acc, r, s)` over every cell (dense) and `pos(lane_acc, i, s)`
+// over every positive entry (sparse) through the tree; returns per-subject
+// totals, K x nv.
+template <typename Dense, typename Sparse>
+std::vector<double> tree_sums(const PmlData& d, const std::vector<size_t>& run, int nv, Dense cell, Sparse pos) {
+  const int k = d.k;
+  std::vector<double> dense(static_cast<size_t>(k + kWarps) * nv, 0.0), sparse(static_cast<size_t>(k) * nv, 0.0);
+  Tree tree(nv);
+  for (int w = 0; w < kWarps; ++w) {
+    const size_t c_begin = warp_start(d, w), c_end = warp_start(d, w + 1);
+    if (c_begin >= c_end) continue;
+    int s = subject_of(d, c_begin);
+    for (size_t c0 = c_begin; c0 < c_end; ++s) {
+      const size_t s_end = std::min<size_t>(c_end, d.subject_start[s + 1]);
+      tree.clear();
+      for (int l = 0; l < kLanes; ++l)
+        for (size_t r = c0 + l; r < s_end; r += kLanes) cell(tree.lane(l), r, s);
+      tree.reduce(&dense[static_cast<size_t>(s + w) * nv]);
+      c0 = s_end;
+    }
+  }
+  for (int s = 0; s < k; ++s) {
+    tree.clear();
+    for (int l = 0; l < kLanes; ++l)
+      for (size_t i = run[s] + l; i < run[s + 1]; i += kLanes) pos(tree.lane(l), i, s);
+    tree.reduce(&sparse[static_cast<size_t>(s) * nv]);
+  }
+  std::vector<double> total(static_cast<size_t>(k) * nv);
+  for (int s = 0; s < k; ++s) {
+    for (int v = 0; v < nv; ++v) {
+      double t = 0.0;
+      for (int w = 0; w < kWarps; ++w)
+        if (warp_start(d, w) < d.subject_start[s + 1] && warp_start(d, w + 1) > d.subject_start[s])
+          t += dense[static_cast<size_t>(s + w) * nv + v];
+      t += sparse[static_cast<size_t>(s) * nv + v];
+      total[static_cast<size_t>(s) * nv + v] = t;
+    }
+  }
+  return total;
+}
+
+// Slot layout of a per-subject partial: resid, weight, sum ln t, sum y eta,
+// sum y ln t, X'd (nb), sum p x (nb), sum p x x' (upper triangle).
+enum { kResid = 0, kWeight = 1, kSumLog = 2, kLinear = 3, kWlog = 4, kScore = 5 };
+
+double eta_of(const PmlData& d, const std::vector<double>& beta, size_t r) {
+  const double* row = d.design + r * d.n_beta;
+  double eta = d.offset[r];
+  for (int j = 0; j < d.n_beta; ++j) eta = nebula::nb_fma(row[j], beta[j], eta);
+  return eta;
+}
+
+// The fold of pml.rs:1469-1489: d into the gradient, p into the curvature.
+void fold(double* acc, const double* x, int nb, double dd, double p) {
+  acc[kResid] += dd;
+  acc[kWeight] += p;
+  double* score = acc + kScore;
+  double* first = score + nb;
+  double* second = first + nb;
+  int t = 0;
+  for (int a = 0; a < nb; ++a) {
+    score[a] = nebula::nb_fma(x[a], dd, score[a]);
+    double pa = p * x[a];
+    first[a] += pa;
+    for (int b = a; b < nb; ++b) {
+      second[t] = nebula::nb_fma(pa, x[b], second[t]);
+      ++t;
+    }
+  }
+}
+
 // sweep_width (pml.rs:1419-1590): each subject is a dense part over every cell
 // at a count of zero, then a sparse part adding what the positive counts
 // change.
 void sweep(const PmlData& d, const std::vector<double>& beta, const std::vector<double>& log_w,
-           double gamma, const Penalty& pen, std::vector<double>& stored,
-           const std::vector<size_t>& run, Sweep& out) {
-  const int nb = d.n_beta, k = d.k;
-  std::vector<double> sums(2 * nb + nb * nb);
-  std::fill(out.db.begin(), out.db.end(), 0.0);
-  std::fill(out.vb.begin(), out.vb.end(), 0.0);
-  double ll = 0.0;
+           double gamma, const Penalty& pen, const std::vector<size_t>& run, Sweep& out) {
+  const int nb = d.n_beta, k = d.k, T = nb * (nb + 1) / 2, nv = 5 + 2 * nb + T;
+  auto dense = [&](double* acc, size_t r, int s) {
+    double eta = eta_of(d, beta, r);
+    double e = nebula::nb_exp(eta + log_w[s]);
+    double t = e + gamma;
+    acc[kSumLog] += nebula::nb_log(t);
+    double inv = 1.0 / t;
+    double u = e * inv;
+    fold(acc, d.design + r * nb, nb, -gamma * u, (gamma * u) * inv);
+  };
+  auto sparse = [&](double* acc, size_t i, int s) {
+    size_t c = d.cells[i];
+    double y = d.counts[i];
+    double eta = eta_of(d, beta, c);
+    double e = nebula::nb_exp(eta + log_w[s]);
+    double t = e + gamma;
+    acc[kLinear] = nebula::nb_fma(eta, y, acc[kLinear]);
+    acc[kWlog] = nebula::nb_fma(y, nebula::nb_log(t), acc[kWlog]);
+    double inv = 1.0 / t;
+    double u = e * inv;
+    fold(acc, d.design + c * nb, nb, y * (1.0 - u), (y * u) * inv);
+  };
+  std::vector<double> tot = tree_sums(d, run, nv, dense, sparse);
+  std::vector<double> llv(k);
   for (int s = 0; s < k; ++s) {
-    const size_t c0 = d.subject_start[s], c1 = d.subject_start[s + 1];
-    const double log_w_s = log_w[s];
-    const double w_s = std::exp(log_w_s);
-    std::fill(sums.begin(), sums.end(), 0.0);
-    double* score = sums.data();
-    double* first = score + nb;
-    double* second = first + nb;
-    double resid = 0, weight = 0, sum_log = 0, linear = 0, weighted_log = 0;
-    auto fold = [&](size_t r, double dd, double p) {
-      const double* row = d.design + r * nb;
-      resid += dd;
-      weight += p;
-      for (int a = 0; a < nb; ++a) {
-        score[a] += row[a] * dd;
-        double pa = p * row[a];
-        first[a] += pa;
-        for (int b = a; b < nb; ++b) second[a * nb + b] += pa * row[b];
-      }
-    };
-    for (size_t r = c0; r < c1; ++r) {
-      const double* row = d.design + r * nb;
-      double eta = d.offset[r];
-      for (int j = 0; j < nb; ++j) eta += row[j] * beta[j];
-      stored[r] = std::exp(eta + log_w_s);
-    }
-    for (size_t r = c0; r < c1; ++r) {
-      double extb = stored[r];
-      double t = extb + gamma;
-      sum_log += std::log(t);
-      double inv = 1.0 / t;
-      double u = extb * inv;
-      fold(r, -gamma * u, gamma * u * inv);
-    }
-    for (size_t i = run[s]; i < run[s + 1]; ++i) {
-      size_t c = d.cells[i];
-      double y = d.counts[i];
-      const double* row = d.design + c * nb;
-      double eta = d.offset[c];
-      for (int j = 0; j < nb; ++j) eta += row[j] * beta[j];
-      double extb = stored[c];
-      double t = extb + gamma;
-      linear += eta * y;
-      weighted_log += y * std::log(t);
-      double inv = 1.0 / t;
-      double u = extb * inv;
-      fold(c, y * (1.0 - u), y * u * inv);
-    }
-    ll += linear + log_w_s * d.subject_total[s] - gamma * sum_log - weighted_log;
+    const double* S = &tot[static_cast<size_t>(s) * nv];
+    const double lw = log_w[s];
+    const double w_s = nebula::nb_exp(lw);
+    llv[s] = S[kLinear] + lw * d.subject_total[s] - gamma * S[kSumLog] - S[kWlog];
     out.w[s] = w_s;
-    out.dw[s] = resid + pen.gradient(log_w_s, w_s);
-    out.vw[s] = gamma * weight + pen.curvature(w_s);
-    for (int a = 0; a < nb; ++a) {
-      out.db[a] += score[a];
-      out.vwb[static_cast<size_t>(s) * nb + a] = gamma * first[a];
-      for (int b = a; b < nb; ++b) out.vb[a * nb + b] += gamma * second[a * nb + b];
+    out.dw[s] = S[kResid] + pen.gradient(lw, w_s);
+    out.vw[s] = gamma * S[kWeight] + pen.curvature(w_s);
+    for (int a = 0; a < nb; ++a) out.vwb[static_cast<size_t>(s) * nb + a] = gamma * S[kScore + nb + a];
+  }
+  for (int a = 0; a < nb; ++a) {
+    double acc = 0.0;
+    for (int s = 0; s < k; ++s) acc += tot[static_cast<size_t>(s) * nv + kScore + a];
+    out.db[a] = acc;
+  }
+  int t = 0;
+  for (int a = 0; a < nb; ++a) {
+    for (int b = a; b < nb; ++b, ++t) {
+      double acc = 0.0;
+      for (int s = 0; s < k; ++s) acc += gamma * tot[static_cast<size_t>(s) * nv + kScore + 2 * nb + t];
+      out.vb[a * nb + b] = acc;
+      out.vb[b * nb + a] = acc;
     }
   }
-  for (int a = 0; a < nb; ++a)
-    for (int b = a + 1; b < nb; ++b) out.vb[b * nb + a] = out.vb[a * nb + b];
+  double ll = 0.0;
+  for (int s = 0; s < k; ++s) ll += llv[s];
   out.ll = pen.accumulate(ll, log_w, out.w);
 }
 
@@ -218,41 +318,35 @@ double determinant(std::vector<double> a, int n) {
 }
 
 // Higher-order Laplace terms at the final iterate (pml.rs:1828-1919).
-double laplace_correction(const PmlData& d, const std::vector<double>& stored,
-                          const std::vector<size_t>& run, const std::vector<double>& w_cur,
-                          double gamma, double lambda, int ord) {
+double laplace_correction(const PmlData& d, const std::vector<double>& beta, const std::vector<double>& log_w,
+                          const std::vector<size_t>& run, const std::vector<double>& w_cur, double gamma,
+                          double lambda, int ord) {
   const bool high = ord > 2;
-  auto terms = [gamma](double e, double f[4]) {
+  auto terms = [&](double e, double scale, double* acc) {
     double t = e + gamma;
-    double p2 = e / (t * t);
-    double p3 = p2 / t;
-    double p4 = p3 / t;
-    double p5 = p4 / t;
-    double e2 = e * e;
-    f[0] = p2;
-    f[1] = p3 * (gamma - e);
-    f[2] = p4 * (gamma * gamma + e2 - (4.0 * gamma) * e);
-    f[3] = p5 * (gamma * gamma * gamma - (11.0 * gamma * gamma) * e + (11.0 * gamma) * e2 - e2 * e);
+    double p2 = e / (t * t), p3 = p2 / t, p4 = p3 / t, p5 = p4 / t, e2 = e * e;
+    acc[0] += scale * p2;
+    acc[1] += scale * (p3 * (gamma - e));
+    acc[2] += scale * (p4 * (gamma * gamma + e2 - (4.0 * gamma) * e));
+    acc[3] += scale * (p5 * (gamma * gamma * gamma - (11.0 * gamma * gamma) * e + (11.0 * gamma) * e2 - e2 * e));
   };
+  auto dense = [&](double* acc, size_t r, int s) {
+    terms(nebula::nb_exp(eta_of(d, beta, r) + log_w[s]), gamma, acc);
+  };
+  auto sparse = [&](double* acc, size_t i, int s) {
+    terms(nebula::nb_exp(eta_of(d, beta, d.cells[i]) + log_w[s]), d.counts[i], acc);
+  };
+  std::vector<double> tot = tree_sums(d, run, 4, dense, sparse);
   double third_acc = 0, fourth_acc = 0, fifth_acc = 0;
   for (int s = 0; s < d.k; ++s) {
-    double sums[4] = {0, 0, 0, 0}, f[4];
-    for (size_t r = d.subject_start[s]; r < d.subject_start[s + 1]; ++r) {
-      terms(stored[r], f);
-      for (int j = 0; j < 4; ++j) sums[j] += gamma * f[j];
-    }
-    for (size_t i = run[s]; i < run[s + 1]; ++i) {
-      double y = d.counts[i];
-      terms(stored[d.cells[i]], f);
-      for (int j = 0; j < 4; ++j) sums[j] += y * f[j];
-    }
+    const double* S = &tot[static_cast<size_t>(s) * 4];
     double prior = lambda * w_cur[s];
-    double vw = gamma * sums[0] + prior;
-    double third = gamma * sums[1] + prior;
+    double vw = gamma * S[0] + prior;
+    double third = gamma * S[1] + prior;
     third_acc += third * third / (vw * vw * vw);
     if (high) {
-      double fourth = gamma * sums[2] + prior;
-      double fifth = gamma * sums[3] + prior;
+      double fourth = gamma * S[2] + prior;
+      double fifth = gamma * S[3] + prior;
       double vs = vw * vw;
       fourth_acc += fourth / vs;
       fifth_acc += fifth * third / (vs * vs);
@@ -325,7 +419,7 @@ bool opt_pml(const PmlData& d, const double* beta_init, const double* log_w_init
              double gamma, const PmlParams& params, Prior prior, PmlResult* out) {
   Penalty pen{prior, 0.0, 0.0};
   if (prior == Prior::Gamma) {  // gamma_penalty (pml.rs:432-441)
-    double exps = std::exp(subject);
+    double exps = nebula::nb_exp(subject);
     if (!(std::isfinite(exps) && exps > 1.0)) return false;
     pen.alpha = 1.0 / (exps - 1.0);
     pen.lambda = 1.0 / (std::sqrt(exps) * (exps - 1.0));
@@ -338,7 +432,6 @@ bool opt_pml(const PmlData& d, const double* beta_init, const double* log_w_init
   std::vector<double> beta(beta_init, beta_init + nb);
   std::vector<double> log_w(k, 0.0);
   if (log_w_init) log_w.assign(log_w_init, log_w_init + k);
-  std::vector<double> stored(d.n_cells, 0.0);
   std::vector<size_t> run = positive_runs(d);
   Sweep cur, trial;
   cur.init(nb, k);
@@ -346,7 +439,7 @@ bool opt_pml(const PmlData& d, const double* beta_init, const double* log_w_init
   std::vector<double> vw_step(k, 0), vb2(nb * nb, 0), step_beta(nb), step_log_w(k), dwvw(k);
   std::vector<double> damp_beta(nb), damp_log_w(k), new_beta(nb), new_log_w(k);
   int sweeps = 0;
-  sweep(d, beta, log_w, gamma, pen, stored, run, cur);
+  sweep(d, beta, log_w, gamma, pen, run, cur);
   ++sweeps;
   double ll = cur.ll, ll_prev = 0.0, likdif = 0.0;
   int step = 0, backtracks = 0;
@@ -380,7 +473,7 @@ bool opt_pml(const PmlData& d, const double* beta_init, const double* log_w_init
     for (int j = 0; j < nb; ++j) new_beta[j] = beta[j] + step_beta[j];
     for (int s = 0; s < k; ++s) new_log_w[s] = log_w[s] + step_log_w[s];
     ll_prev = ll;
-    sweep(d, new_beta, new_log_w, gamma, pen, stored, run, trial);
+    sweep(d, new_beta, new_log_w, gamma, pen, run, trial);
     ++sweeps;
     ll = trial.ll;
     likdif = ll - ll_prev;
@@ -420,7 +513,7 @@ bool opt_pml(const PmlData& d, const double* beta_init, const double* log_w_init
           new_log_w[s] = log_w[s] - min_step;
         }
       }
-      sweep(d, new_beta, new_log_w, gamma, pen, stored, run, trial);
+      sweep(d, new_beta, new_log_w, gamma, pen, run, trial);
       ++sweeps;
       ll = trial.ll;
       likdif = ll - ll_prev;
@@ -430,11 +523,11 @@ bool opt_pml(const PmlData& d, const double* beta_init, const double* log_w_init
     std::swap(cur, trial);
   }
   double log_det = 0.0;
-  for (int s = 0; s < k; ++s) log_det += std::log(std::fabs(vw_step[s]));
-  if (params.reml) log_det += std::log(std::fabs(determinant(vb2, nb)));
+  for (int s = 0; s < k; ++s) log_det += nebula::nb_log(std::fabs(vw_step[s]));
+  if (params.reml) log_det += nebula::nb_log(std::fabs(determinant(vb2, nb)));
   double second = 0.0;
   if (prior == Prior::Gamma && params.ord > 1) {
-    second = laplace_correction(d, stored, run, cur.w, gamma, pen.lambda, params.ord);
+    second = laplace_correction(d, beta, log_w, run, cur.w, gamma, pen.lambda, params.ord);
     ++sweeps;
   }
   out->beta = beta;
@@ -455,10 +548,10 @@ double pml_objective_gradient(const PmlData& d, const double* beta, const double
                               double subject, double gamma, double* gradient) {
   Penalty pen{Prior::Gamma, subject, subject};  // nebula's Gamma(alpha, alpha) reading
   const int nb = d.n_beta, k = d.k;
-  std::vector<double> b(beta, beta + nb), lw(log_w, log_w + k), stored(d.n_cells);
+  std::vector<double> b(beta, beta + nb), lw(log_w, log_w + k);
   Sweep cur;
   cur.init(nb, k);
-  sweep(d, b, lw, gamma, pen, stored, positive_runs(d), cur);
+  sweep(d, b, lw, gamma, pen, positive_runs(d), cur);
   for (int j = 0; j < nb; ++j) gradient[j] = -cur.db[j];
   for (int s = 0; s < k; ++s) gradient[nb + s] = -cur.dw[s];
   return -cur.ll;

@@ -1,0 +1,103 @@
+"""The oracle pinned to the reference's own goldens before it checks the CUDA path.
+
+- opt_pml against nebula:::opt_pml at 1e-11 (src/sc/pml.rs:2188, 2232-2700)
+- the 8-gene x 150-cell nebula 1.5.8 golden (src/sc/nebula.rs:2290-2496)
+- the NEBULA-HL end-to-end datasets at tests/e2e_nebula.rs's gates (:66-256)
+"""
+import numpy as np
+import pytest
+
+import golden_io as gio
+import oracle_ffi as of
+from edge_rs_b200.api import NebulaParams
+from pml_fixtures import fixture
+
+TOL = 1e-11  # pml.rs:2188
+CASES = gio.inline()["pml_cases"]
+
+
+def check_case(case, got):
+    for key in ("beta", "log_w", "information", "log_likelihood", "log_det", "second_order"):
+        if key in case:
+            ok, worst = gio.close(got[key], case[key], TOL, 1e-12)
+            assert ok, f"{case['name']}: {key} off by {worst:.2e}"
+    for key in ("iterations", "backtracks", "convergence"):
+        if key in case:
+            assert got[key] == case[key], f"{case['name']}: {key} {got[key]} != {case[key]}"
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
+def test_oracle_opt_pml_matches_nebula(case):
+    f, nb = fixture(case)
+    got = of.opt_pml(f["design"], f["offset"], nb, f["counts"], f["cells"], f["subject_start"],
+                     f["subject_total"], case["beta_init"], case["subject"], case["cell"],
+                     reml=case.get("reml", False), eps=case.get("eps", 1e-6), ord=case.get("ord", 1),
+                     lognormal=case.get("prior") == "lognormal")
+    check_case(case, got)
+
+
+def test_oracle_penalised_gradient_matches_nebula():
+    import ctypes
+    g = gio.inline()["pml_gradient"]
+    f, nb = fixture({"fixture": "A"})
+    grad = np.zeros(nb + 3)
+    arrs = [np.ascontiguousarray(f[k], t) for k, t in (("design", np.float64), ("offset", np.float64),
+                                                          ("counts", np.float64), ("cells", np.uint32),
+                                                          ("subject_start", np.uint64), ("subject_total", np.float64))]
+    beta = np.array(g["beta"])
+    log_w = np.array(g["log_w"])
+    p = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    obj = of.lib().oracle_pml_objective_gradient(p(arrs[0]), p(arrs[1]), ctypes.c_uint64(12), ctypes.c_uint32(nb),
+                                                 p(arrs[2]), p(arrs[3]), ctypes.c_uint64(arrs[2].size), p(arrs[4]),
+                                                 ctypes.c_uint32(3), p(arrs[5]), p(beta), p(log_w),
+                                                 ctypes.c_double(g["subject"]), ctypes.c_double(g["cell"]), p(grad))
+    assert gio.close(obj, g["objective"], TOL)[0]
+    assert gio.close(grad, g["gradient"], TOL, 1e-12)[0]
+
+
+def test_oracle_min_eigenvalue_known_matrix():
+    import ctypes
+    a = np.array([2.0, 1.0, 1.0, 2.0])
+    v = of.lib().oracle_min_eigenvalue(a.ctypes.data_as(ctypes.c_void_p), ctypes.c_uint32(2))
+    assert abs(v - 1.0) < 1e-13
+
+
+def test_oracle_nebula_matches_r_eight_gene_golden():
+    d = gio.load_eight_gene()
+    w = gio.expected_eight_gene()
+    fit, _ = of.nebula_sparse(d["csr"], d["subject"], d["design"], 3, d["offset"],
+                              NebulaParams(cutoff_cell=0.0), threads=4)
+    assert list(fit.gene_index) == list(range(8))
+    # nebula.rs:2299-2321
+    assert gio.close(fit.coefficients, w["coef"], 5e-6)[0]
+    assert gio.close(fit.se, w["se"], 1e-5)[0]
+    assert gio.close(fit.subject_overdispersion, w["subject"], 1e-5)[0]
+    assert gio.close(fit.cell_overdispersion, w["cell"], 1e-5)[0]
+    assert gio.close(fit.covariance, w["cov"], 1e-5)[0]
+    assert all(c in (1, -10) for c in fit.convergence)
+
+
+# tests/e2e_nebula.rs:66-197 base gates, with its per-dataset loosenings (:232-256)
+BASE = dict(coef=(3e-5, 1e-9), se=(1e-4, 0.0), cov=(1e-3, 1e-12), subject=(2e-4, 1e-6), cell=(1e-4, 0.0))
+LOOSE = {"sc_high": dict(coef=(3e-4, 1e-9), subject=(2e-3, 1e-6), cov=(2.5e-2, 1e-12))}
+
+
+def gates(tag):
+    g = dict(BASE)
+    g.update(LOOSE.get(tag, {}))
+    return g
+
+
+@pytest.mark.parametrize("tag", gio.inline()["e2e_hl"])
+def test_oracle_nebula_matches_r_hl_datasets(tag):
+    d = gio.load_e2e(tag)
+    w = gio.expected_e2e(tag, d["n_coef"])
+    fit, _ = of.nebula_sparse(d["csr"], d["subject"], d["design"], d["n_coef"], d["offset"],
+                              NebulaParams(method=d["method"]), threads=4)
+    assert np.array_equal(fit.gene_index, w["gene_index"])
+    g = gates(tag)
+    for key, got, want in (("coef", fit.coefficients, w["coef"]), ("se", fit.se, w["se"]),
+                           ("subject", fit.subject_overdispersion, w["subject"]),
+                           ("cell", fit.cell_overdispersion, w["cell"]), ("cov", fit.covariance, w["cov"])):
+        ok, worst = gio.close(got, want, *g[key])
+        assert ok, f"{tag}: {key} off by {worst:.2e}"
