@@ -1,0 +1,281 @@
+"""Benchmark of NEBULA-HL stage two on B200: genes/s at 100k cells.
+
+Workload: 500 genes x 100,000 cells, 20 subjects (Dirichlet(2) sizes, min 500),
+4-column design (intercept, subject-level binary, cell covariate, subject-level
+batch), seeded synthetic counts from NEBULA's generative model, forced HL.
+
+A step fits every gene of the workload:
+- `value`: stages two and three (every inner fit on the GPU) on inputs already
+  resident in HBM (nb_session_fit), device time from CUDA events recorded on the
+  library's launching stream around the step; L2 is flushed between steps.
+- `e2e`: the drop-in nebula_sparse_cuda call from host buffers (validation,
+  stage one on host threads, upload, stages two and three, download).
+- `roofline`: the fit kernel against the measured FP64 FMA peak of this GPU
+  (its work is FP64 arithmetic; neither HBM nor the tensor cores bound it).
+- `cpu_baseline`: the FP64 CPU oracle (the reference's nebula_sparse restated)
+  on a bounded gene sample of the same workload, all host threads.
+
+`--impl reference` times that CPU path alone on the same workload and metric.
+Multi-GPU (torchrun): genes shard across ranks with no collective on the data
+path (weak scaling); each rank fits its own 500-gene workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from edge_rs_b200 import NebulaParams, workloads  # noqa: E402
+
+METRIC = "NEBULA-HL genes/s @100k cells, 1 B200: warm-start+batched vs plain; roofline %"
+PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "fit_kernel_traffic.json")
+
+
+def flops_per_visit(nb):
+    """FP64 operations of one cell visit of the fit kernel's sweep.
+
+    eta (nb FMAs), exp (34), t, log (35), 1/t and the fold scalars (5), the
+    fold: resid and weight (2), per column X'd FMA, p x and its sum (4 nb),
+    the p x x' triangle (nb(nb+1) as FMAs); an FMA counts two, a division one.
+    """
+    return 2 * nb + 1 + 34 + 1 + 35 + 5 + 1 + 2 + 4 * nb + nb * (nb + 1)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c1")
+    ap.add_argument("--genes", type=int, default=None)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-genes", type=int, default=32, help="gene sample of the CPU baseline")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._thread = None
+
+    def start(self):
+        def run():
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                         timeout=5).stdout.strip()
+                    if out:
+                        self.rows.append([v.strip() for v in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+        self._thread = threading.Thread(target=run, daemon=True)
+        self._thread.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._thread:
+            self._thread.join(timeout=10)
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 4 + i and r[4 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+        return world, rank, local, dist
+    return 1, 0, local, None
+
+
+def barrier_max(dist, value):
+    """Max of a float over ranks (one all-reduce), or the value itself."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_sample(work, n_genes):
+    """The first n_genes genes of a workload as their own CSR."""
+    n = min(n_genes, work.n_genes)
+    end = int(work.indptr[n])
+    return (work.indptr[: n + 1].copy(), work.indices[:end], work.data[:end], (n, work.n_cells))
+
+
+def run_cpu(work, n_genes, threads):
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_ffi  # the oracle: checker and CPU baseline only
+    csr = cpu_sample(work, n_genes)
+    t0 = time.perf_counter()
+    fit, _ = oracle_ffi.nebula_sparse(csr, work.subject, work.design, work.n_coef, work.offset,
+                                      NebulaParams(method="HL"), threads=threads)
+    el = time.perf_counter() - t0
+    return len(fit.gene_index) / el, len(fit.gene_index), el
+
+
+def reference_arm(args, world, rank, dist):
+    if rank != 0:
+        return
+    work = workloads.make(args.config, seed=1000, n_genes=args.genes)
+    threads = os.cpu_count() or 1
+    vals = []
+    for i in range(args.warmup + args.steps):
+        v, n, el = run_cpu(work, args.cpu_genes, threads)
+        if i >= args.warmup:
+            vals.append(v)
+    value = float(np.mean(vals))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "genes/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * args.cpu_genes / value,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded NEBULA generative model)",
+            "config": {"workload": f"{args.config}: {work.n_genes} genes x {work.n_cells} cells, "
+                                   f"{len(work.truth['sizes'])} subjects, {work.n_coef} columns, forced HL",
+                       "sample_genes_per_step": args.cpu_genes},
+            "cpu_baseline": {"value": value, "unit": "genes/s", "cores": threads, "kind": "port",
+                             "sample": f"first {args.cpu_genes} genes of the workload per step"},
+            "e2e": {"value": value, "unit": "genes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def l2_flush(buf):
+    buf.add_(1.0)
+
+
+def ours_arm(args, world, rank, local, dist):
+    import torch
+    from edge_rs_b200.api import Session, measure_fp64_tflops, nebula_sparse_cuda
+    torch.cuda.set_device(local)
+    work = workloads.make(args.config, seed=1000 + rank, n_genes=args.genes)
+    params = NebulaParams(method="HL")
+    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > 126 MB L2
+    session = Session(work.csr, work.subject, work.design, work.n_coef, work.offset, params)
+    for _ in range(args.warmup):
+        session.fit()
+    sampler = ClockSampler(local)
+    sampler.start()
+    step_ms, stats = [], []
+    t_wall = 0.0
+    for _ in range(args.steps):
+        l2_flush(flush)
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fit = session.fit()
+        torch.cuda.synchronize()
+        t_wall += time.perf_counter() - t0
+        step_ms.append(fit.stats["ms_step_device"])
+        stats.append(fit.stats)
+    clocks = sampler.stop()
+    genes = len(fit.gene_index)
+    total_ms = barrier_max(dist, float(np.sum(step_ms)))
+    value = world * genes * args.steps / (total_ms / 1000.0)
+    launches = int(np.sum([s["gpu_launches"] for s in stats]))
+    visits = float(np.sum([s["cell_visits"] for s in stats]))
+    kernel_ms = float(np.sum([s["ms_device"] for s in stats]))
+    fp64_peak = measure_fp64_tflops(5)
+    achieved = visits * flops_per_visit(work.n_coef) / (kernel_ms / 1000.0) / 1e12
+    traffic = None
+    if os.path.exists(PROFILE_SUMMARY):
+        try:
+            with open(PROFILE_SUMMARY) as fh:
+                traffic = json.load(fh).get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+    # end to end through the drop-in C-ABI call from host buffers
+    e2e_vals, h2d, d2h = [], 0, 0
+    e2e_stats = {"ms_stage_one": None, "ms_stage_two": None, "ms_stage_three": None}
+    for _ in range(args.e2e_steps):
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        f2 = nebula_sparse_cuda(work.csr, work.subject, work.design, work.n_coef, work.offset, params)
+        torch.cuda.synchronize()
+        el = barrier_max(dist, time.perf_counter() - t0)
+        e2e_vals.append(world * len(f2.gene_index) / el)
+        h2d = f2.stats["h2d_bytes"]
+        d2h = f2.stats["d2h_bytes"]
+        e2e_stats = f2.stats
+    session.close()
+    if rank != 0:
+        return
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        cv, n, el = run_cpu(work, args.cpu_genes, os.cpu_count() or 1)
+        cpu = {"value": cv, "unit": "genes/s", "cores": os.cpu_count() or 1, "kind": "port",
+               "sample": f"first {n} of the workload's genes ({el:.1f} s of CPU work)"}
+    line = {
+        "metric": METRIC, "value": value, "unit": "genes/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded NEBULA generative model; no public dataset)",
+        "config": {"workload": f"{args.config}: {work.n_genes} genes x {work.n_cells} cells, "
+                               f"{len(work.truth['sizes'])} subjects, {work.n_coef} columns, forced HL, plain cold start",
+                   "genes_per_rank": genes, "nnz_per_rank": work.nnz, "l2": "flushed (256 MiB write) before each step",
+                   "step": "stages two and three on device-resident inputs (nb_session_fit)"},
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                     "frac": achieved / fp64_peak if fp64_peak > 0 else None, "traffic": traffic,
+                     "kernel": "fit_kernel", "flops_per_visit": flops_per_visit(work.n_coef),
+                     "peak_source": "measured on this GPU: FP64 FMA chains (nb_measure_fp64_tflops)"},
+        "e2e": {"value": float(np.mean(e2e_vals)) if e2e_vals else None, "unit": "genes/s",
+                "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "ms_stage_one": e2e_stats["ms_stage_one"],
+                "ms_stage_two": e2e_stats["ms_stage_two"], "ms_stage_three": e2e_stats["ms_stage_three"]},
+        "gpu_launches": launches,
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+        "detail": {"rounds_per_step": stats[-1]["rounds"], "requests_per_step": stats[-1]["requests"],
+                   "sweeps_per_step": stats[-1]["sweeps"], "cell_visits_per_step": stats[-1]["cell_visits"],
+                   "kernel_ms_per_step": kernel_ms / args.steps, "wall_ms_per_step": 1000.0 * t_wall / args.steps},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":  # rank 0 alone times the CPU path; other ranks exit
+        reference_arm(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), None)
+        return
+    world, rank, local, dist = dist_setup(args)
+    try:
+        ours_arm(args, world, rank, local, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

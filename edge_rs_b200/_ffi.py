@@ -63,8 +63,9 @@ class NbStats(ctypes.Structure):
                 ("gpu_launches", ctypes.c_uint64), ("ms_total", ctypes.c_double),
                 ("ms_prepare", ctypes.c_double), ("ms_stage_one", ctypes.c_double),
                 ("ms_stage_two", ctypes.c_double), ("ms_stage_three", ctypes.c_double),
-                ("ms_device", ctypes.c_double), ("audited", ctypes.c_uint64),
-                ("refit_cold", ctypes.c_uint64)]
+                ("ms_device", ctypes.c_double), ("ms_step_device", ctypes.c_double),
+                ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64),
+                ("audited", ctypes.c_uint64), ("refit_cold", ctypes.c_uint64)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -82,6 +83,12 @@ PRODUCT_SIGNATURES = {
                                                ctypes.POINTER(NbParams), ctypes.POINTER(NbOptions),
                                                ctypes.POINTER(NbFit), ctypes.POINTER(NbStats),
                                                ctypes.c_char_p, ctypes.c_size_t]),
+    "nb_session_create": (ctypes.c_int32, [ctypes.POINTER(NbCsr), c_u64_p, c_double_p, ctypes.c_uint32,
+                                           c_double_p, ctypes.POINTER(NbParams), ctypes.POINTER(NbOptions),
+                                           ctypes.POINTER(ctypes.c_void_p), ctypes.c_char_p, ctypes.c_size_t]),
+    "nb_session_fit": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(NbFit), ctypes.POINTER(NbStats),
+                                        ctypes.c_char_p, ctypes.c_size_t]),
+    "nb_session_free": (None, [ctypes.c_void_p]),
     "nb_glm_sc_test": (ctypes.c_int32, [c_double_p, c_double_p, ctypes.c_uint64, ctypes.c_uint64,
                                         c_double_p, c_double_p, c_double_p, c_double_p, c_double_p,
                                         c_double_p, c_double_p, ctypes.c_char_p, ctypes.c_size_t]),
@@ -92,6 +99,7 @@ PRODUCT_SIGNATURES = {
     "nb_bobyqa_result": (ctypes.c_int32, [ctypes.c_void_p, c_double_p, c_double_p,
                                           ctypes.POINTER(ctypes.c_uint32)]),
     "nb_bobyqa_free": (None, [ctypes.c_void_p]),
+    "nb_measure_fp64_tflops": (ctypes.c_double, [ctypes.c_int]),
 }
 
 

@@ -160,3 +160,54 @@ def glm_sc_test(coefficients, covariance, coef=None, contrast=None):
     if rc != 0:
         raise NebulaError(rc, err.value.decode(errors="replace"))
     return ScTestResult(*outs)
+
+
+class Session:
+    """nb_session_create / nb_session_fit: inputs validated, stage one run and
+    the data made resident on the device once; `fit()` runs stages two and
+    three on the resident copy."""
+
+    def __init__(self, counts, subject_id, design, n_coef, offset=None, params: Optional[NebulaParams] = None,
+                 warm_start=False, device=-1, host_threads=0, audit_percent=5):
+        self._lib = _ffi.product_library()
+        self._keep = []
+        csr = _as_csr(counts)
+        subject = np.ascontiguousarray(subject_id, dtype=np.uint64)
+        design = np.ascontiguousarray(design, dtype=np.float64).reshape(-1)
+        off = None if offset is None else np.ascontiguousarray(offset, dtype=np.float64)
+        self.n_genes = int(csr.struct.n_genes)
+        self.n_coef = int(n_coef)
+        p = (params or NebulaParams()).to_c()
+        opts = _ffi.NbOptions(int(device), int(bool(warm_start)), int(host_threads), int(audit_percent), None)
+        self._keep = [csr, subject, design, off, p, opts]
+        handle = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(512)
+        rc = self._lib.nb_session_create(ctypes.byref(csr.struct), _ffi.ptr(subject, ctypes.c_uint64),
+                                         _ffi.ptr(design, ctypes.c_double), ctypes.c_uint32(n_coef),
+                                         _ffi.ptr(off, ctypes.c_double), ctypes.byref(p), ctypes.byref(opts),
+                                         ctypes.byref(handle), err, len(err))
+        if rc != 0:
+            raise NebulaError(rc, err.value.decode(errors="replace"))
+        self._handle = handle
+
+    def fit(self):
+        out = _ffi.FitArrays(self.n_genes, self.n_coef)
+        stats = _ffi.NbStats()
+        err = ctypes.create_string_buffer(512)
+        rc = self._lib.nb_session_fit(self._handle, ctypes.byref(out.struct), ctypes.byref(stats), err, len(err))
+        if rc != 0:
+            raise NebulaError(rc, err.value.decode(errors="replace"))
+        return fit_from_arrays(out, self.n_coef, stats.as_dict())
+
+    def close(self):
+        if getattr(self, "_handle", None):
+            self._lib.nb_session_free(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        self.close()
+
+
+def measure_fp64_tflops(repeats=5):
+    """Measured FP64 FMA throughput of the current device (TFLOP/s)."""
+    return float(_ffi.product_library().nb_measure_fp64_tflops(int(repeats)))

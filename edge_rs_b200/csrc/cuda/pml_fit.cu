@@ -174,8 +174,28 @@ __device__ __forceinline__ void fold(double* acc, const double* x, double d, dou
 template <int NB>
 __device__ __forceinline__ void load_row(const double* __restrict__ design, int r, double* x) {
   const double* row = design + static_cast<size_t>(r) * NB;
+  if constexpr (NB % 2 == 0) {  // rows start on 16 bytes: vector loads
+    const double2* row2 = reinterpret_cast<const double2*>(row);
 #pragma unroll
-  for (int j = 0; j < NB; ++j) x[j] = __ldg(row + j);
+    for (int j = 0; j < NB / 2; ++j) {
+      const double2 v = __ldg(row2 + j);
+      x[2 * j] = v.x;
+      x[2 * j + 1] = v.y;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < NB; ++j) x[j] = __ldg(row + j);
+  }
+}
+
+// The four per-cell Laplace sums (pml.rs:1842-1856, 1863-1868, 1893-1899),
+// each term scaled by gamma (dense) or the count (sparse).
+__device__ __forceinline__ void laplace_terms(double* acc, double e, double t, double gamma, double scale) {
+  const double p2 = e / (t * t), p3 = p2 / t, p4 = p3 / t, p5 = p4 / t, e2 = e * e;
+  acc[0] += scale * p2;
+  acc[1] += scale * (p3 * (gamma - e));
+  acc[2] += scale * (p4 * (gamma * gamma + e2 - (4.0 * gamma) * e));
+  acc[3] += scale * (p5 * (gamma * gamma * gamma - (11.0 * gamma * gamma) * e + (11.0 * gamma) * e2 - e2 * e));
 }
 
 template <int NB>
@@ -218,24 +238,31 @@ __device__ void sweep_sums(const GeneData& d, Smem<NB>& sm, int gene, const doub
       double acc[NV];
 #pragma unroll
       for (int v = 0; v < NV; ++v) acc[v] = 0.0;
-      for (int r = c0 + lane; r < s_end; r += 32) {
-        double x[NB];
-        load_row<NB>(d.design, r, x);
-        double eta = linear_eta<NB>(x, beta, __ldg(d.log_offset + r));
-        double e = nb_exp(eta + lw);
-        double t = e + gamma;
+      // Two cells (r and r + 32) per iteration: their exp/log/division chains
+      // are independent and interleave; each accumulator still takes cell r
+      // before cell r + 32, the order of the lane's sequential sum.
+      for (int r = c0 + lane; r < s_end; r += 64) {
+        const bool has_b = r + 32 < s_end;
+        const int rb = has_b ? r + 32 : r;
+        double xa[NB], xb[NB];
+        load_row<NB>(d.design, r, xa);
+        load_row<NB>(d.design, rb, xb);
+        const double ea = nb_exp(linear_eta<NB>(xa, beta, __ldg(d.log_offset + r)) + lw);
+        const double eb = nb_exp(linear_eta<NB>(xb, beta, __ldg(d.log_offset + rb)) + lw);
+        const double ta = ea + gamma, tb = eb + gamma;
         if (MODE == 0) {
-          acc[kSumLog] += nb_log(t);
-          double inv = 1.0 / t;
-          double u = e * inv;
-          fold<NB>(acc, x, -gamma * u, (gamma * u) * inv);
+          const double la = nb_log(ta), lb = nb_log(tb);
+          const double inva = 1.0 / ta, invb = 1.0 / tb;
+          const double ua = ea * inva, ub = eb * invb;
+          acc[kSumLog] += la;
+          fold<NB>(acc, xa, -gamma * ua, (gamma * ua) * inva);
+          if (has_b) {
+            acc[kSumLog] += lb;
+            fold<NB>(acc, xb, -gamma * ub, (gamma * ub) * invb);
+          }
         } else {
-          double p2 = e / (t * t), p3 = p2 / t, p4 = p3 / t, p5 = p4 / t, e2 = e * e;
-          acc[0] += gamma * p2;
-          acc[1] += gamma * (p3 * (gamma - e));
-          acc[2] += gamma * (p4 * (gamma * gamma + e2 - (4.0 * gamma) * e));
-          acc[3] += gamma * (p5 * (gamma * gamma * gamma - (11.0 * gamma * gamma) * e +
-                                   (11.0 * gamma) * e2 - e2 * e));
+          laplace_terms(acc, ea, ta, gamma, gamma);
+          if (has_b) laplace_terms(acc, eb, tb, gamma, gamma);
         }
       }
       reduce_to<NV>(acc, sm.slots_dense + (s + warp) * Dims<NB>::NS, lane);
@@ -250,27 +277,33 @@ __device__ void sweep_sums(const GeneData& d, Smem<NB>& sm, int gene, const doub
     double acc[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) acc[v] = 0.0;
-    for (uint64_t p = p0 + lane; p < p1; p += 32) {
-      const int c = static_cast<int>(__ldg(d.cells + p));
-      const double y = __ldg(d.counts + p);
-      double x[NB];
-      load_row<NB>(d.design, c, x);
-      double eta = linear_eta<NB>(x, beta, __ldg(d.log_offset + c));
-      double e = nb_exp(eta + lw);
-      double t = e + gamma;
+    for (uint64_t p = p0 + lane; p < p1; p += 64) {
+      const bool has_b = p + 32 < p1;
+      const uint64_t pb = has_b ? p + 32 : p;
+      const int ca = static_cast<int>(__ldg(d.cells + p)), cb = static_cast<int>(__ldg(d.cells + pb));
+      const double ya = __ldg(d.counts + p), yb = __ldg(d.counts + pb);
+      double xa[NB], xb[NB];
+      load_row<NB>(d.design, ca, xa);
+      load_row<NB>(d.design, cb, xb);
+      const double eta_a = linear_eta<NB>(xa, beta, __ldg(d.log_offset + ca));
+      const double eta_b = linear_eta<NB>(xb, beta, __ldg(d.log_offset + cb));
+      const double ea = nb_exp(eta_a + lw), eb = nb_exp(eta_b + lw);
+      const double ta = ea + gamma, tb = eb + gamma;
       if (MODE == 0) {
-        acc[kLinear] = nb_fma(eta, y, acc[kLinear]);
-        acc[kWlog] = nb_fma(y, nb_log(t), acc[kWlog]);
-        double inv = 1.0 / t;
-        double u = e * inv;
-        fold<NB>(acc, x, y * (1.0 - u), (y * u) * inv);
+        const double la = nb_log(ta), lb = nb_log(tb);
+        const double inva = 1.0 / ta, invb = 1.0 / tb;
+        const double ua = ea * inva, ub = eb * invb;
+        acc[kLinear] = nb_fma(eta_a, ya, acc[kLinear]);
+        acc[kWlog] = nb_fma(ya, la, acc[kWlog]);
+        fold<NB>(acc, xa, ya * (1.0 - ua), (ya * ua) * inva);
+        if (has_b) {
+          acc[kLinear] = nb_fma(eta_b, yb, acc[kLinear]);
+          acc[kWlog] = nb_fma(yb, lb, acc[kWlog]);
+          fold<NB>(acc, xb, yb * (1.0 - ub), (yb * ub) * invb);
+        }
       } else {
-        double p2 = e / (t * t), p3 = p2 / t, p4 = p3 / t, p5 = p4 / t, e2 = e * e;
-        acc[0] += y * p2;
-        acc[1] += y * (p3 * (gamma - e));
-        acc[2] += y * (p4 * (gamma * gamma + e2 - (4.0 * gamma) * e));
-        acc[3] += y * (p5 * (gamma * gamma * gamma - (11.0 * gamma * gamma) * e + (11.0 * gamma) * e2 -
-                             e2 * e));
+        laplace_terms(acc, ea, ta, gamma, ya);
+        if (has_b) laplace_terms(acc, eb, tb, gamma, yb);
       }
     }
     reduce_to<NV>(acc, sm.slots_sparse + s * Dims<NB>::NS, lane);
@@ -452,7 +485,7 @@ __device__ double determinant(double* a) {
 }
 
 template <int NB>
-__global__ void __launch_bounds__(kThreads) fit_kernel(GeneData d, FitControl ctl,
+__global__ void __launch_bounds__(kThreads, (NB <= 4 ? 2 : 1)) fit_kernel(GeneData d, FitControl ctl,
                                                        const FitRequest* __restrict__ requests,
                                                        FitResult* __restrict__ results,
                                                        const int32_t* __restrict__ n_requests,

@@ -104,6 +104,9 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
       runs[g * (K + 1) + s] = gene_ptr[g] + static_cast<uint64_t>(it - gc.cells.begin());
     }
   }
+  gene_nnz_.resize(G);
+  for (size_t g = 0; g < G; ++g) gene_nnz_[g] = genes[g].cells.size();
+  n_cells_ = sh.n_cells;
   std::vector<uint32_t> fid(sh.fid.begin(), sh.fid.end());
   std::vector<uint32_t> wcells(device::kWarps + 1);
   for (int w = 0; w <= device::kWarps; ++w)
@@ -118,6 +121,9 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
   data_.runs = device_copy(runs.data(), runs.size(), &owned_);
   data_.totals = device_copy(totals.data(), totals.size(), &owned_);
   data_.warp_cells = device_copy(wcells.data(), wcells.size(), &owned_);
+  h2d_bytes_ = (sh.design.size() + sh.log_offset.size() + counts.size() + totals.size()) * sizeof(double) +
+               (fid.size() + cells.size() + wcells.size()) * sizeof(uint32_t) +
+               (gene_ptr.size() + runs.size()) * sizeof(uint64_t);
   data_.n_cells = static_cast<int32_t>(sh.n_cells);
   data_.n_subjects = K;
   data_.n_coef = sh.n_coef;
@@ -137,6 +143,24 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
   owned_.push_back(d_counter_);
   cuda_check(cudaEventCreate(&ev0_), "event");
   cuda_check(cudaEventCreate(&ev1_), "event");
+  cuda_check(cudaEventCreate(&step0_), "event");
+  cuda_check(cudaEventCreate(&step1_), "event");
+  cuda_check(cudaMallocHost(reinterpret_cast<void**>(&h_header_), 2 * sizeof(int32_t)), "cudaMallocHost");
+}
+
+void DeviceFitter::reset_counters() {
+  device_ms_ = 0.0;
+  launches_ = requests_ = sweeps_ = cell_visits_ = h2d_bytes_ = d2h_bytes_ = 0;
+}
+
+void DeviceFitter::begin_step() { cuda_check(cudaEventRecord(step0_, stream_), "event"); }
+
+double DeviceFitter::end_step() {
+  cuda_check(cudaEventRecord(step1_, stream_), "event");
+  cuda_check(cudaEventSynchronize(step1_), "event");
+  float ms = 0.0f;
+  cuda_check(cudaEventElapsedTime(&ms, step0_, step1_), "event time");
+  return ms;
 }
 
 DeviceFitter::~DeviceFitter() {
@@ -147,6 +171,9 @@ DeviceFitter::~DeviceFitter() {
   if (h_res_) cudaFreeHost(h_res_);
   if (ev0_) cudaEventDestroy(ev0_);
   if (ev1_) cudaEventDestroy(ev1_);
+  if (step0_) cudaEventDestroy(step0_);
+  if (step1_) cudaEventDestroy(step1_);
+  if (h_header_) cudaFreeHost(h_header_);
   if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -169,10 +196,12 @@ const device::FitResult* DeviceFitter::run(const std::vector<device::FitRequest>
   if (n == 0) return nullptr;
   reserve(n);
   std::memcpy(h_req_, reqs.data(), n * sizeof(device::FitRequest));
-  int32_t header[2] = {static_cast<int32_t>(n), 0};
+  h_header_[0] = static_cast<int32_t>(n);
+  h_header_[1] = 0;
   cuda_check(cudaMemcpyAsync(d_req_, h_req_, n * sizeof(device::FitRequest), cudaMemcpyHostToDevice, stream_),
              "request copy");
-  cuda_check(cudaMemcpyAsync(d_counter_, header, sizeof(header), cudaMemcpyHostToDevice, stream_), "count copy");
+  cuda_check(cudaMemcpyAsync(d_counter_, h_header_, 2 * sizeof(int32_t), cudaMemcpyHostToDevice, stream_),
+             "count copy");
   cuda_check(cudaEventRecord(ev0_, stream_), "event");
   int grid = static_cast<int>(std::min<size_t>(grid_, n));
   cuda_check(static_cast<cudaError_t>(device::launch_fit(data_, ctl_, d_req_, d_res_, d_counter_, d_counter_ + 1,
@@ -187,8 +216,12 @@ const device::FitResult* DeviceFitter::run(const std::vector<device::FitRequest>
   device_ms_ += ms;
   ++launches_;
   requests_ += n;
+  h2d_bytes_ += n * sizeof(device::FitRequest) + 2 * sizeof(int32_t);
+  d2h_bytes_ += n * sizeof(device::FitResult);
   for (size_t i = 0; i < n; ++i) {
-    sweeps_ += static_cast<uint64_t>(h_res_[i].sweeps);
+    const uint64_t sw = static_cast<uint64_t>(h_res_[i].sweeps);
+    sweeps_ += sw;
+    cell_visits_ += sw * (n_cells_ + gene_nnz_[reqs[i].gene]);
   }
   return h_res_;
 }
@@ -198,7 +231,6 @@ const device::FitResult* DeviceFitter::run(const std::vector<device::FitRequest>
 namespace {
 
 struct GeneTask {
-  GenePlan plan;
   std::unique_ptr<StageTwoSearch> search;
   VarianceObjective objective;
   std::optional<std::optional<std::pair<std::vector<double>, bool>>> refit;
@@ -213,6 +245,186 @@ void write_err(char* err, size_t len, const std::string& msg) {
 
 }  // namespace
 
+// One call's validated inputs, stage-one plans and resident device copy.
+struct Session {
+  Prepared prep;
+  std::vector<GeneCounts> genes;
+  std::vector<GenePlan> plans;
+  std::unique_ptr<DeviceFitter> fitter;
+  nb_options opt{};
+  double ms_prepare = 0.0, ms_stage_one = 0.0, ms_upload = 0.0;
+};
+
+std::unique_ptr<Session> create_session(const nb_csr* counts, const uint64_t* subject_id, const double* design,
+                                        uint32_t n_coef, const double* offset, const nb_params* params,
+                                        const nb_options* options) {
+  auto t0 = Clock::now();
+  auto ss = std::make_unique<Session>();
+  ss->opt.device = -1;
+  ss->opt.audit_percent = 5;
+  if (options) ss->opt = *options;
+  if (n_coef > static_cast<uint32_t>(device::kMaxCoef))
+    fail(NB_ERR_UNSUPPORTED, "the device path takes at most 8 design columns");
+  ss->prep = prepare(counts, subject_id, design, n_coef, offset, params);
+  const Shared& sh = ss->prep.shared;
+  const size_t G = ss->prep.kept.size();
+  ss->genes.resize(G);
+  for (size_t g = 0; g < G; ++g) ss->genes[g] = positive_indices(ss->prep.counts, ss->prep.kept[g]);
+  ss->ms_prepare = ms_since(t0);
+  // stage one on host threads (nebula.rs:812-901)
+  auto t1 = Clock::now();
+  ss->plans.resize(G);
+  parallel_for(G, ss->opt.host_threads, [&](size_t g) {
+    ss->plans[g] = plan_gene(sh, ss->genes[g], &ss->prep.totals[ss->prep.kept[g] * sh.n_subjects]);
+  });
+  ss->ms_stage_one = ms_since(t1);
+  auto t2 = Clock::now();
+  ss->fitter = std::make_unique<DeviceFitter>(ss->prep, ss->genes, ss->opt.device);
+  ss->ms_upload = ms_since(t2);
+  return ss;
+}
+
+// Stages two and three on the resident data, into `out`.
+void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
+  const Shared& sh = ss.prep.shared;
+  const size_t G = ss.genes.size();
+  DeviceFitter& fitter = *ss.fitter;
+  fitter.reset_counters();
+  fitter.begin_step();
+  // stage two: every search in lockstep, one launch per round
+  auto t2 = Clock::now();
+  std::vector<GeneTask> tasks(G);
+  std::vector<size_t> active;
+  for (size_t g = 0; g < G; ++g) {
+    GeneTask& t = tasks[g];
+    const GenePlan& plan = ss.plans[g];
+    if (plan.refit == Refit::None) continue;
+    std::optional<double> fixed_cell;
+    std::vector<double> start;
+    if (plan.refit == Refit::Both) {
+      start = {plan.sigma, plan.gamma};
+    } else {
+      start = {plan.sigma};
+      fixed_cell = plan.gamma;
+    }
+    std::vector<double> lower, upper;
+    variance_bounds(sh.params, fixed_cell.has_value(), &lower, &upper);
+    t.search = std::make_unique<StageTwoSearch>(start, lower, upper, plan.ord);
+    t.objective = VarianceObjective::make(sh, ss.genes[g], fixed_cell);
+    active.push_back(g);
+  }
+  struct Slot {
+    double subject, cell;
+    int request;  // index into the batch, -1 when the point is outside the domain
+  };
+  std::vector<device::FitRequest> batch;
+  std::vector<Slot> slots;
+  uint64_t rounds = 0;
+  while (!active.empty()) {
+    batch.clear();
+    slots.clear();
+    for (size_t g : active) {
+      GeneTask& t = tasks[g];
+      const auto& points = t.search->ask();
+      for (size_t p = 0; p < points.size(); ++p) {
+        double subject = 0.0, cell = 0.0;
+        std::vector<double> beta;
+        Slot slot{0.0, 0.0, -1};
+        if (t.objective.request(points[p], ss.plans[g].beta_start, &subject, &cell, &beta)) {
+          device::FitRequest r{};
+          r.gene = static_cast<int32_t>(g);
+          r.ord = t.search->order();
+          r.reml = sh.params.reml ? 1 : 0;
+          r.subject = subject;
+          r.cell = cell;
+          for (int j = 0; j < sh.n_coef; ++j) r.beta[j] = beta[j];
+          slot = Slot{subject, cell, static_cast<int>(batch.size())};
+          batch.push_back(r);
+        }
+        slots.push_back(slot);
+      }
+    }
+    const device::FitResult* res = fitter.run(batch);
+    ++rounds;
+    std::vector<double> values;
+    size_t si = 0;
+    std::vector<size_t> still;
+    for (size_t g : active) {
+      GeneTask& t = tasks[g];
+      const size_t n_points = t.search->ask().size();
+      values.assign(n_points, std::numeric_limits<double>::infinity());
+      for (size_t p = 0; p < n_points; ++p, ++si) {
+        const Slot& s = slots[si];
+        if (s.request < 0) continue;
+        const device::FitResult& r = res[s.request];
+        if (r.status != 0) continue;
+        InnerFit fit{r.log_likelihood, r.log_likelihood_prev, r.log_det, r.second_order};
+        values[p] = t.objective.assemble(s.subject, s.cell, fit, t.objective.tail(s.cell));
+      }
+      t.search->tell(values);
+      if (t.search->done()) {
+        t.refit = t.search->result();
+        t.search.reset();
+      } else {
+        still.push_back(g);
+      }
+    }
+    active.swap(still);
+  }
+  const double ms_stage_two = ms_since(t2);
+
+  // stage three: one final fit per gene at order one (nebula.rs:948-967)
+  auto t3 = Clock::now();
+  std::vector<double> sigma(G), gamma(G);
+  std::vector<int> conv(G);
+  batch.clear();
+  for (size_t g = 0; g < G; ++g) {
+    apply_refit(ss.plans[g], tasks[g].refit, &sigma[g], &gamma[g], &conv[g]);
+    device::FitRequest r{};
+    r.gene = static_cast<int32_t>(g);
+    r.ord = 1;
+    r.reml = sh.params.reml ? 1 : 0;
+    r.subject = sigma[g];
+    r.cell = gamma[g];
+    for (int j = 0; j < sh.n_coef; ++j) r.beta[j] = ss.plans[g].beta_start[j];
+    r.beta[sh.intercept] -= sigma[g] / 2.0;
+    batch.push_back(r);
+  }
+  const device::FitResult* res = fitter.run(batch);
+  std::vector<GeneOutcome> outcomes(G);
+  for (size_t g = 0; g < G; ++g) {
+    const device::FitResult& r = res[g];
+    if (r.status != 0) fail(NB_ERR_INVALID_ARGUMENT, "opt_pml rejected the final variance components");
+    FinalFit ff;
+    ff.beta.assign(r.beta, r.beta + sh.n_coef);
+    ff.information.resize(static_cast<size_t>(sh.n_coef) * sh.n_coef);
+    for (int a = 0; a < sh.n_coef; ++a)
+      for (int b = 0; b < sh.n_coef; ++b) ff.information[a * sh.n_coef + b] = r.information[a * sh.n_coef + b];
+    ff.log_likelihood = r.log_likelihood;
+    ff.iterations = r.iterations;
+    ff.backtracks = r.backtracks;
+    outcomes[g] = finish_gene(sh, sigma[g], gamma[g], conv[g], ff);
+  }
+  const double ms_stage_three = ms_since(t3);
+  const double ms_step = fitter.end_step();
+  assemble_fit(sh, outcomes, ss.prep.kept, out);
+  if (stats) {
+    stats->rounds = rounds;
+    stats->requests = fitter.requests();
+    stats->sweeps = fitter.sweeps();
+    stats->cell_visits = fitter.cell_visits();
+    stats->gpu_launches = fitter.launches();
+    stats->ms_prepare = ss.ms_prepare;
+    stats->ms_stage_one = ss.ms_stage_one;
+    stats->ms_stage_two = ms_stage_two;
+    stats->ms_stage_three = ms_stage_three;
+    stats->ms_device = fitter.device_ms();
+    stats->ms_step_device = ms_step;
+    stats->h2d_bytes = fitter.h2d_bytes();
+    stats->d2h_bytes = fitter.d2h_bytes();
+  }
+}
+
 int32_t run_nebula_device(const nb_csr* counts, const uint64_t* subject_id, const double* design,
                           uint32_t n_coef, const double* offset, const nb_params* params,
                           const nb_options* options, nb_fit* out, nb_stats* stats, char* err,
@@ -220,159 +432,12 @@ int32_t run_nebula_device(const nb_csr* counts, const uint64_t* subject_id, cons
   const auto t_start = Clock::now();
   try {
     if (!out) fail(NB_ERR_INVALID_ARGUMENT, "out is null");
-    nb_options opt{};
-    opt.device = -1;
-    opt.audit_percent = 5;
-    if (options) opt = *options;
-    if (n_coef > static_cast<uint32_t>(device::kMaxCoef))
-      fail(NB_ERR_UNSUPPORTED, "the device path takes at most 8 design columns");
-    Prepared prep = prepare(counts, subject_id, design, n_coef, offset, params);
-    const Shared& sh = prep.shared;
-    const size_t G = prep.kept.size();
-    std::vector<GeneCounts> genes(G);
-    for (size_t g = 0; g < G; ++g) genes[g] = positive_indices(prep.counts, prep.kept[g]);
-    const double ms_prepare = ms_since(t_start);
-
-    // stage one on host threads (nebula.rs:812-901)
-    auto t1 = Clock::now();
-    std::vector<GeneTask> tasks(G);
-    parallel_for(G, opt.host_threads, [&](size_t g) {
-      tasks[g].plan = plan_gene(sh, genes[g], &prep.totals[prep.kept[g] * sh.n_subjects]);
-    });
-    const double ms_stage_one = ms_since(t1);
-
-    DeviceFitter fitter(prep, genes, opt.device);
-
-    // stage two: every search in lockstep, one launch per round
-    auto t2 = Clock::now();
-    std::vector<size_t> active;
-    for (size_t g = 0; g < G; ++g) {
-      GeneTask& t = tasks[g];
-      if (t.plan.refit == Refit::None) continue;
-      std::optional<double> fixed_cell;
-      std::vector<double> start;
-      if (t.plan.refit == Refit::Both) {
-        start = {t.plan.sigma, t.plan.gamma};
-      } else {
-        start = {t.plan.sigma};
-        fixed_cell = t.plan.gamma;
-      }
-      std::vector<double> lower, upper;
-      variance_bounds(sh.params, fixed_cell.has_value(), &lower, &upper);
-      t.search = std::make_unique<StageTwoSearch>(start, lower, upper, t.plan.ord);
-      t.objective = VarianceObjective::make(sh, genes[g], fixed_cell);
-      active.push_back(g);
-    }
-    struct Slot {
-      size_t gene;
-      size_t point;
-      double subject, cell;
-      int request;  // index into the batch, -1 when the point is outside the domain
-    };
-    std::vector<device::FitRequest> batch;
-    std::vector<Slot> slots;
-    uint64_t rounds = 0;
-    while (!active.empty()) {
-      batch.clear();
-      slots.clear();
-      for (size_t g : active) {
-        GeneTask& t = tasks[g];
-        const auto& points = t.search->ask();
-        for (size_t p = 0; p < points.size(); ++p) {
-          double subject = 0.0, cell = 0.0;
-          std::vector<double> beta;
-          Slot slot{g, p, 0.0, 0.0, -1};
-          if (t.objective.request(points[p], t.plan.beta_start, &subject, &cell, &beta)) {
-            device::FitRequest r{};
-            r.gene = static_cast<int32_t>(g);
-            r.ord = t.search->order();
-            r.reml = sh.params.reml ? 1 : 0;
-            r.subject = subject;
-            r.cell = cell;
-            for (int j = 0; j < sh.n_coef; ++j) r.beta[j] = beta[j];
-            slot.subject = subject;
-            slot.cell = cell;
-            slot.request = static_cast<int>(batch.size());
-            batch.push_back(r);
-          }
-          slots.push_back(slot);
-        }
-      }
-      const device::FitResult* res = fitter.run(batch);
-      ++rounds;
-      std::vector<double> values;
-      size_t si = 0;
-      std::vector<size_t> still;
-      for (size_t g : active) {
-        GeneTask& t = tasks[g];
-        const size_t n_points = t.search->ask().size();
-        values.assign(n_points, std::numeric_limits<double>::infinity());
-        for (size_t p = 0; p < n_points; ++p, ++si) {
-          const Slot& s = slots[si];
-          if (s.request < 0) continue;
-          const device::FitResult& r = res[s.request];
-          if (r.status != 0) continue;
-          InnerFit fit{r.log_likelihood, r.log_likelihood_prev, r.log_det, r.second_order};
-          values[p] = t.objective.assemble(s.subject, s.cell, fit, t.objective.tail(s.cell));
-        }
-        t.search->tell(values);
-        if (t.search->done()) {
-          t.refit = t.search->result();
-          t.search.reset();
-        } else {
-          still.push_back(g);
-        }
-      }
-      active.swap(still);
-    }
-    const double ms_stage_two = ms_since(t2);
-
-    // stage three: one final fit per gene at order one (nebula.rs:948-967)
-    auto t3 = Clock::now();
-    std::vector<double> sigma(G), gamma(G);
-    std::vector<int> conv(G);
-    batch.clear();
-    for (size_t g = 0; g < G; ++g) {
-      apply_refit(tasks[g].plan, tasks[g].refit, &sigma[g], &gamma[g], &conv[g]);
-      device::FitRequest r{};
-      r.gene = static_cast<int32_t>(g);
-      r.ord = 1;
-      r.reml = sh.params.reml ? 1 : 0;
-      r.subject = sigma[g];
-      r.cell = gamma[g];
-      for (int j = 0; j < sh.n_coef; ++j) r.beta[j] = tasks[g].plan.beta_start[j];
-      r.beta[sh.intercept] -= sigma[g] / 2.0;
-      batch.push_back(r);
-    }
-    const device::FitResult* res = fitter.run(batch);
-    std::vector<GeneOutcome> outcomes(G);
-    for (size_t g = 0; g < G; ++g) {
-      const device::FitResult& r = res[g];
-      if (r.status != 0) fail(NB_ERR_INVALID_ARGUMENT, "opt_pml rejected the final variance components");
-      FinalFit ff;
-      ff.beta.assign(r.beta, r.beta + sh.n_coef);
-      ff.information.resize(static_cast<size_t>(sh.n_coef) * sh.n_coef);
-      for (int a = 0; a < sh.n_coef; ++a)
-        for (int b = 0; b < sh.n_coef; ++b) ff.information[a * sh.n_coef + b] = r.information[a * sh.n_coef + b];
-      ff.log_likelihood = r.log_likelihood;
-      ff.iterations = r.iterations;
-      ff.backtracks = r.backtracks;
-      outcomes[g] = finish_gene(sh, sigma[g], gamma[g], conv[g], ff);
-    }
-    const double ms_stage_three = ms_since(t3);
-    assemble_fit(sh, outcomes, prep.kept, out);
+    std::unique_ptr<Session> ss = create_session(counts, subject_id, design, n_coef, offset, params, options);
+    const uint64_t upload = ss->fitter->h2d_bytes();
+    if (stats) *stats = nb_stats{};
+    fit_session(*ss, out, stats);
     if (stats) {
-      *stats = nb_stats{};
-      stats->rounds = rounds;
-      stats->requests = fitter.requests();
-      stats->sweeps = fitter.sweeps();
-      stats->cell_visits = 0;
-      stats->gpu_launches = fitter.launches();
-      stats->ms_prepare = ms_prepare;
-      stats->ms_stage_one = ms_stage_one;
-      stats->ms_stage_two = ms_stage_two;
-      stats->ms_stage_three = ms_stage_three;
-      stats->ms_device = fitter.device_ms();
+      stats->h2d_bytes += upload;
       stats->ms_total = ms_since(t_start);
     }
     return NB_OK;
@@ -383,6 +448,43 @@ int32_t run_nebula_device(const nb_csr* counts, const uint64_t* subject_id, cons
 }
 
 }  // namespace nebula
+
+struct nb_session {
+  std::unique_ptr<nebula::Session> impl;
+};
+
+NB_API int32_t nb_session_create(const nb_csr* counts, const uint64_t* subject_id, const double* design,
+                                 uint32_t n_coef, const double* offset_or_null, const nb_params* params_or_null,
+                                 const nb_options* options, nb_session** out, char* err, size_t err_len) {
+  try {
+    if (!out) nebula::fail(NB_ERR_INVALID_ARGUMENT, "out is null");
+    auto s = std::make_unique<nb_session>();
+    s->impl = nebula::create_session(counts, subject_id, design, n_coef, offset_or_null, params_or_null, options);
+    *out = s.release();
+    return NB_OK;
+  } catch (const nebula::NbError& e) {
+    nebula::write_err(err, err_len, e.message);
+    return e.code;
+  }
+}
+
+NB_API int32_t nb_session_fit(nb_session* session, nb_fit* out, nb_stats* stats, char* err, size_t err_len) {
+  try {
+    if (!session || !out) nebula::fail(NB_ERR_INVALID_ARGUMENT, "null session or output");
+    if (stats) *stats = nb_stats{};
+    nebula::fit_session(*session->impl, out, stats);
+    if (stats) {
+      stats->ms_prepare = session->impl->ms_prepare;
+      stats->ms_stage_one = session->impl->ms_stage_one;
+    }
+    return NB_OK;
+  } catch (const nebula::NbError& e) {
+    nebula::write_err(err, err_len, e.message);
+    return e.code;
+  }
+}
+
+NB_API void nb_session_free(nb_session* session) { delete session; }
 
 NB_API void nb_params_default(nb_params* p) {
   if (!p) return;

@@ -27,11 +27,22 @@ class DeviceFitter {
   uint64_t launches() const { return launches_; }
   uint64_t requests() const { return requests_; }
   uint64_t sweeps() const { return sweeps_; }
+  uint64_t cell_visits() const { return cell_visits_; }
+  uint64_t h2d_bytes() const { return h2d_bytes_; }
+  uint64_t d2h_bytes() const { return d2h_bytes_; }
+  void reset_counters();
+  // Brackets a step with events on the launching stream; end_step returns
+  // the device time between them in milliseconds.
+  void begin_step();
+  double end_step();
 
  private:
   void reserve(size_t n);
   cudaStream_t stream_ = nullptr;
-  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr, step0_ = nullptr, step1_ = nullptr;
+  std::vector<uint64_t> gene_nnz_;
+  size_t n_cells_ = 0;
+  int32_t* h_header_ = nullptr;  // pinned: request count and queue counter
   device::GeneData data_{};
   device::FitControl ctl_{};
   std::vector<void*> owned_;
@@ -43,8 +54,11 @@ class DeviceFitter {
   size_t capacity_ = 0;
   int grid_ = 0;
   double device_ms_ = 0.0;
-  uint64_t launches_ = 0, requests_ = 0, sweeps_ = 0;
+  uint64_t launches_ = 0, requests_ = 0, sweeps_ = 0, cell_visits_ = 0;
+  uint64_t h2d_bytes_ = 0, d2h_bytes_ = 0;
 };
+
+struct Session;
 
 int32_t run_nebula_device(const nb_csr* counts, const uint64_t* subject_id, const double* design,
                           uint32_t n_coef, const double* offset, const nb_params* params,

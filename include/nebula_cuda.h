@@ -113,7 +113,10 @@ typedef struct nb_stats {
   uint64_t cell_visits;     /* dense + sparse cell visits on the device */
   uint64_t gpu_launches;    /* kernels launched */
   double ms_total, ms_prepare, ms_stage_one, ms_stage_two, ms_stage_three;
-  double ms_device;         /* sum of device time of the stage-two fit kernel */
+  double ms_device;         /* sum of the fit kernels' device times */
+  double ms_step_device;    /* device time from the first stage-two copy to the
+                               last stage-three copy, CUDA events */
+  uint64_t h2d_bytes, d2h_bytes; /* host<->device bytes the call moved */
   uint64_t audited, refit_cold;
 } nb_stats;
 
@@ -134,6 +137,23 @@ int32_t nebula_sparse_cuda_ex(const nb_csr* counts, const uint64_t* subject_id,
                               const nb_params* params_or_null,
                               const nb_options* options, nb_fit* out,
                               nb_stats* stats, char* err, size_t err_len);
+
+/* nebula_sparse_cuda in two parts, for callers that fit the same inputs
+ * more than once or time the device-resident stages alone:
+ * nb_session_create validates and preprocesses the inputs, runs stage one and
+ * uploads the design, offsets and kept genes' counts to the device;
+ * nb_session_fit runs stages two and three on that resident copy and fills
+ * `out` exactly as nebula_sparse_cuda does. */
+typedef struct nb_session nb_session;
+int32_t nb_session_create(const nb_csr* counts, const uint64_t* subject_id,
+                          const double* design, uint32_t n_coef,
+                          const double* offset_or_null,
+                          const nb_params* params_or_null,
+                          const nb_options* options, nb_session** out,
+                          char* err, size_t err_len);
+int32_t nb_session_fit(nb_session* session, nb_fit* out, nb_stats* stats,
+                       char* err, size_t err_len);
+void nb_session_free(nb_session* session);
 
 /* opt_pml (src/sc/pml.rs:468-508) for a batch of variance points of one
  * gene on the device (the batched twin of the reference's device entry,
@@ -176,6 +196,10 @@ void nb_bobyqa_tell(nb_bobyqa* h, double value);
 int32_t nb_bobyqa_result(const nb_bobyqa* h, double* x, double* f,
                          uint32_t* evaluations);
 void nb_bobyqa_free(nb_bobyqa* h);
+
+/* Measured FP64 FMA throughput of the current device in TFLOP/s (best of
+ * `repeats` launches), the peak the fit kernel's roofline is taken against. */
+double nb_measure_fp64_tflops(int repeats);
 
 #ifdef __cplusplus
 }
