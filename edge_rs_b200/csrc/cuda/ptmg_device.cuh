@@ -1,0 +1,31 @@
+// Layout shared by the host driver and the stage-one kernel (ptmg_eval.cu).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include "pml_device.cuh"
+
+namespace nebula {
+namespace device {
+
+// One marginal-likelihood evaluation at [beta, sigma, phi]; alpha, lambda
+// and gamma are the host's Terms of (sigma, phi).
+struct alignas(16) PtmgRequest {
+  int32_t gene;
+  int32_t pad;
+  double alpha, lambda, gamma;
+  double beta[kMaxCoef];
+};
+
+// Per request the kernel writes (2 + ptmg_width_of(n_coef)) * n_subjects
+// doubles: cumsumxtb (K), ylin (K), then K rows of the pass-two sums.
+size_t ptmg_smem_bytes(int n_subjects);
+int ptmg_width_of(int n_coef);
+size_t ptmg_scratch_doubles(int n_subjects, int n_coef);  // per CTA
+
+int launch_ptmg(const GeneData& d, const PtmgRequest* req, double* results, double* scratch,
+                const int32_t* n_requests, int32_t* counter, int grid, void* stream);
+
+}  // namespace device
+}  // namespace nebula

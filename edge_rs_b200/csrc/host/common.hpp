@@ -76,6 +76,9 @@ struct GeneCounts {
   std::vector<double> counts;
   double mean_count = 0.0;
   size_t n_one = 0, n_two = 0;
+  // distinct counts other than one and two, increasing, with multiplicities:
+  // the gamma-function terms take one lgamma per distinct value
+  std::vector<double> big_values, big_mult;
 };
 GeneCounts positive_indices(const CsrView& csr, size_t gene);
 

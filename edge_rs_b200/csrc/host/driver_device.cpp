@@ -163,7 +163,61 @@ double DeviceFitter::end_step() {
   return ms;
 }
 
+const double* DeviceFitter::run_ptmg(const std::vector<device::PtmgRequest>& reqs) {
+  const size_t n = reqs.size();
+  if (n == 0) return nullptr;
+  const int K = data_.n_subjects;
+  const size_t stride = static_cast<size_t>(2 + device::ptmg_width_of(data_.n_coef)) * K;
+  if (!d_scratch_) {
+    int sms = 0, dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute");
+    pgrid_ = sms;  // one CTA per SM (the kernel is bound to one resident block)
+    cuda_check(cudaMalloc(reinterpret_cast<void**>(&d_scratch_),
+                          static_cast<size_t>(pgrid_) * device::ptmg_scratch_doubles(K, data_.n_coef) * sizeof(double)),
+               "cudaMalloc");
+    owned_.push_back(d_scratch_);
+  }
+  if (n > pcapacity_) {
+    size_t cap = std::max<size_t>(n, pcapacity_ * 2);
+    if (d_preq_) cudaFree(d_preq_);
+    if (d_pres_) cudaFree(d_pres_);
+    if (h_preq_) cudaFreeHost(h_preq_);
+    if (h_pres_) cudaFreeHost(h_pres_);
+    cuda_check(cudaMalloc(reinterpret_cast<void**>(&d_preq_), cap * sizeof(device::PtmgRequest)), "cudaMalloc");
+    cuda_check(cudaMalloc(reinterpret_cast<void**>(&d_pres_), cap * stride * sizeof(double)), "cudaMalloc");
+    cuda_check(cudaMallocHost(reinterpret_cast<void**>(&h_preq_), cap * sizeof(device::PtmgRequest)),
+               "cudaMallocHost");
+    cuda_check(cudaMallocHost(reinterpret_cast<void**>(&h_pres_), cap * stride * sizeof(double)),
+               "cudaMallocHost");
+    pcapacity_ = cap;
+  }
+  std::memcpy(h_preq_, reqs.data(), n * sizeof(device::PtmgRequest));
+  h_header_[0] = static_cast<int32_t>(n);
+  h_header_[1] = 0;
+  cuda_check(cudaMemcpyAsync(d_preq_, h_preq_, n * sizeof(device::PtmgRequest), cudaMemcpyHostToDevice, stream_),
+             "stage-one request copy");
+  cuda_check(cudaMemcpyAsync(d_counter_, h_header_, 2 * sizeof(int32_t), cudaMemcpyHostToDevice, stream_),
+             "count copy");
+  const int grid = static_cast<int>(std::min<size_t>(pgrid_, n));
+  cuda_check(static_cast<cudaError_t>(
+                 device::launch_ptmg(data_, d_preq_, d_pres_, d_scratch_, d_counter_, d_counter_ + 1, grid, stream_)),
+             "stage-one kernel launch");
+  cuda_check(cudaMemcpyAsync(h_pres_, d_pres_, n * stride * sizeof(double), cudaMemcpyDeviceToHost, stream_),
+             "stage-one result copy");
+  cuda_check(cudaStreamSynchronize(stream_), "stage-one kernel");
+  ++launches_;
+  h2d_bytes_ += n * sizeof(device::PtmgRequest) + 2 * sizeof(int32_t);
+  d2h_bytes_ += n * stride * sizeof(double);
+  for (size_t i = 0; i < n; ++i) cell_visits_ += 2 * (n_cells_ + gene_nnz_[reqs[i].gene]);
+  return h_pres_;
+}
+
 DeviceFitter::~DeviceFitter() {
+  if (d_preq_) cudaFree(d_preq_);
+  if (d_pres_) cudaFree(d_pres_);
+  if (h_preq_) cudaFreeHost(h_preq_);
+  if (h_pres_) cudaFreeHost(h_pres_);
   for (void* p : owned_) cudaFree(p);
   if (d_req_) cudaFree(d_req_);
   if (d_res_) cudaFree(d_res_);
@@ -271,16 +325,65 @@ std::unique_ptr<Session> create_session(const nb_csr* counts, const uint64_t* su
   ss->genes.resize(G);
   for (size_t g = 0; g < G; ++g) ss->genes[g] = positive_indices(ss->prep.counts, ss->prep.kept[g]);
   ss->ms_prepare = ms_since(t0);
-  // stage one on host threads (nebula.rs:812-901)
-  auto t1 = Clock::now();
-  ss->plans.resize(G);
-  parallel_for(G, ss->opt.host_threads, [&](size_t g) {
-    ss->plans[g] = plan_gene(sh, ss->genes[g], &ss->prep.totals[ss->prep.kept[g] * sh.n_subjects]);
-  });
-  ss->ms_stage_one = ms_since(t1);
   auto t2 = Clock::now();
   ss->fitter = std::make_unique<DeviceFitter>(ss->prep, ss->genes, ss->opt.device);
   ss->ms_upload = ms_since(t2);
+  // stage one (nebula.rs:812-901): every gene's projected Newton in lockstep,
+  // one batched launch of marginal-likelihood cell passes per round
+  auto t1 = Clock::now();
+  const int nb = sh.n_coef, K = sh.n_subjects, np = nb + 2;
+  const int W = ptmg_width(nb);
+  std::vector<std::unique_ptr<MarginalSearch>> search(G);
+  std::vector<std::vector<double>> xy(G);
+  std::vector<size_t> active;
+  for (size_t g = 0; g < G; ++g) {
+    std::vector<double> start, lower, upper;
+    marginal_box(sh, ss->genes[g], &start, &lower, &upper);
+    search[g] = std::make_unique<MarginalSearch>(start, lower, upper, nb);
+    xy[g] = positive_xy(sh, ss->genes[g]);
+    active.push_back(g);
+  }
+  ss->plans.resize(G);
+  std::vector<device::PtmgRequest> batch;
+  while (!active.empty()) {
+    batch.clear();
+    for (size_t g : active) {
+      const double* x = search[g]->ask();
+      Terms t(x[nb], x[nb + 1]);
+      device::PtmgRequest r{};
+      r.gene = static_cast<int32_t>(g);
+      r.alpha = t.alpha;
+      r.lambda = t.lambda;
+      r.gamma = t.gamma;
+      for (int j = 0; j < nb; ++j) r.beta[j] = x[j];
+      batch.push_back(r);
+    }
+    const double* res = ss->fitter->run_ptmg(batch);
+    const size_t stride = static_cast<size_t>(2 + W) * K;
+    std::vector<char> finished(active.size(), 0);
+    parallel_for(active.size(), ss->opt.host_threads, [&](size_t i) {
+      const size_t g = active[i];
+      const double* r = res + i * stride;
+      PtmgSums sums;
+      sums.cumsumxtb.assign(r, r + K);
+      sums.ylin.assign(r + K, r + 2 * K);
+      sums.sums.assign(r + 2 * K, r + stride);
+      MarginalGene mg{&sh, &ss->genes[g], &ss->prep.totals[ss->prep.kept[g] * K], xy[g].data()};
+      std::vector<double> grad(np), hess(static_cast<size_t>(np) * np);
+      std::vector<double> x(search[g]->ask(), search[g]->ask() + np);
+      double f = ptmg_assemble(mg, x.data(), sums, grad.data(), hess.data());
+      search[g]->tell(f, grad.data(), hess.data());
+      if (search[g]->done()) {
+        ss->plans[g] = plan_from(sh, ss->genes[g], search[g]->best(), search[g]->failed());
+        finished[i] = 1;
+      }
+    });
+    std::vector<size_t> still;
+    for (size_t i = 0; i < active.size(); ++i)
+      if (!finished[i]) still.push_back(active[i]);
+    active.swap(still);
+  }
+  ss->ms_stage_one = ms_since(t1);
   return ss;
 }
 

@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "../cuda/pml_device.cuh"
+#include "../cuda/ptmg_device.cuh"
 #include "common.hpp"
 
 namespace nebula {
@@ -22,6 +23,9 @@ class DeviceFitter {
   // Runs one batch; the returned results (pinned host memory) stay valid
   // until the next call.
   const device::FitResult* run(const std::vector<device::FitRequest>& reqs);
+  // One batch of stage-one evaluations: per request (2 + W) * K doubles,
+  // valid until the next call.
+  const double* run_ptmg(const std::vector<device::PtmgRequest>& reqs);
 
   double device_ms() const { return device_ms_; }
   uint64_t launches() const { return launches_; }
@@ -53,6 +57,14 @@ class DeviceFitter {
   device::FitResult* h_res_ = nullptr;
   size_t capacity_ = 0;
   int grid_ = 0;
+  // stage-one buffers
+  device::PtmgRequest* d_preq_ = nullptr;
+  device::PtmgRequest* h_preq_ = nullptr;
+  double* d_pres_ = nullptr;
+  double* h_pres_ = nullptr;
+  double* d_scratch_ = nullptr;
+  size_t pcapacity_ = 0;
+  int pgrid_ = 0;
   double device_ms_ = 0.0;
   uint64_t launches_ = 0, requests_ = 0, sweeps_ = 0, cell_visits_ = 0;
   uint64_t h2d_bytes_ = 0, d2h_bytes_ = 0;

@@ -5,6 +5,7 @@
 // cell_level_columns (ptmg.rs:1962-2005), cumsum_y (ptmg.rs:1596-1644), the
 // LN->HL override (nebula.rs:612-617) and the expression filter
 // (nebula.rs:621-639).
+#include <algorithm>
 #include <cmath>
 #include <sstream>
 #include <unordered_set>
@@ -255,6 +256,18 @@ GeneCounts positive_indices(const CsrView& csr, size_t gene) {
     }
   }
   out.mean_count = sum / static_cast<double>(csr.n_cells);
+  std::vector<double> big;
+  for (double y : out.counts)
+    if (y != 1.0 && y != 2.0) big.push_back(y);
+  std::sort(big.begin(), big.end());
+  for (double y : big) {
+    if (!out.big_values.empty() && out.big_values.back() == y) {
+      out.big_mult.back() += 1.0;
+    } else {
+      out.big_values.push_back(y);
+      out.big_mult.push_back(1.0);
+    }
+  }
   return out;
 }
 

@@ -15,6 +15,7 @@
 
 #include "common.hpp"
 #include "pml_cpu.hpp"
+#include "ptmg_cpu.hpp"
 #include "search.hpp"
 #include "special.hpp"
 #include "stage_one.hpp"
@@ -40,7 +41,8 @@ GeneOutcome fit_gene_cpu(const Shared& sh, const CsrView& csr, const std::vector
   const int k = sh.n_subjects;
   const double* tot = &totals[g * k];
   GeneCounts gc = positive_indices(csr, g);
-  GenePlan plan = plan_gene(sh, gc, tot);
+  int marginal_evaluations = 0;
+  GenePlan plan = oracle::plan_gene(sh, gc, tot, &marginal_evaluations);
   oracle::PmlData data = pml_view(sh, gc, tot);
   std::optional<std::optional<std::pair<std::vector<double>, bool>>> refit;
   if (plan.refit != Refit::None) {

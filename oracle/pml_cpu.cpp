@@ -7,6 +7,7 @@
 #include "pml_cpu.hpp"
 
 #include "nbmath.hpp"
+#include "tree_cpu.hpp"
 
 #include <algorithm>
 #include <cfloat>
@@ -54,6 +55,8 @@ struct Sweep {  // pml.rs:1171-1210
   }
 };
 
+}  // namespace
+
 // Start of each subject's run of positive counts (pml.rs:1155-1160).
 std::vector<size_t> positive_runs(const PmlData& d) {
   std::vector<size_t> run(d.k + 1);
@@ -66,85 +69,7 @@ std::vector<size_t> positive_runs(const PmlData& d) {
   return run;
 }
 
-// The summation tree both this oracle and the CUDA kernel use for a sweep's
-// per-subject sums, so that the two agree bit for bit. Dense part: the cells
-// are cut into kWarps equal contiguous ranges; within a range each subject
-// piece is summed by kLanes strided partial sums (lane l takes cells
-// c0 + l, c0 + l + kLanes, ...), which are then combined by the butterfly
-// v[l] += v[l ^ off] for off = 16, 8, 4, 2, 1 (lane 0's value is kept).
-// Sparse part: each subject's positive entries the same way. A subject's total
-// is 0 + its dense pieces in range order + its sparse piece.
-constexpr int kWarps = 8;
-constexpr int kLanes = 32;
-
-struct Tree {
-  int nv;
-  std::vector<double> lanes, next;  // kLanes x nv each
-  explicit Tree(int n) : nv(n), lanes(static_cast<size_t>(kLanes) * n, 0.0), next(lanes.size()) {}
-  double* lane(int l) { return &lanes[static_cast<size_t>(l) * nv]; }
-  void clear() { std::fill(lanes.begin(), lanes.end(), 0.0); }
-  void reduce(double* out) {
-    for (int off = 16; off > 0; off >>= 1) {
-      for (int l = 0; l < kLanes; ++l) {
-        const double* a = &lanes[static_cast<size_t>(l) * nv];
-        const double* b = &lanes[static_cast<size_t>(l ^ off) * nv];
-        double* o = &next[static_cast<size_t>(l) * nv];
-        for (int v = 0; v < nv; ++v) o[v] = a[v] + b[v];
-      }
-      lanes.swap(next);
-    }
-    for (int v = 0; v < nv; ++v) out[v] = lanes[v];
-  }
-};
-
-size_t warp_start(const PmlData& d, int w) { return d.n_cells * static_cast<size_t>(w) / kWarps; }
-
-int subject_of(const PmlData& d, size_t c) {
-  int s = 0;
-  while (d.subject_start[s + 1] <= c) ++s;
-  return s;
-}
-
-// Runs `cell(lane_acc, r, s)` over every cell (dense) and `pos(lane_acc, i, s)`
-// over every positive entry (sparse) through the tree; returns per-subject
-// totals, K x nv.
-template <typename Dense, typename Sparse>
-std::vector<double> tree_sums(const PmlData& d, const std::vector<size_t>& run, int nv, Dense cell, Sparse pos) {
-  const int k = d.k;
-  std::vector<double> dense(static_cast<size_t>(k + kWarps) * nv, 0.0), sparse(static_cast<size_t>(k) * nv, 0.0);
-  Tree tree(nv);
-  for (int w = 0; w < kWarps; ++w) {
-    const size_t c_begin = warp_start(d, w), c_end = warp_start(d, w + 1);
-    if (c_begin >= c_end) continue;
-    int s = subject_of(d, c_begin);
-    for (size_t c0 = c_begin; c0 < c_end; ++s) {
-      const size_t s_end = std::min<size_t>(c_end, d.subject_start[s + 1]);
-      tree.clear();
-      for (int l = 0; l < kLanes; ++l)
-        for (size_t r = c0 + l; r < s_end; r += kLanes) cell(tree.lane(l), r, s);
-      tree.reduce(&dense[static_cast<size_t>(s + w) * nv]);
-      c0 = s_end;
-    }
-  }
-  for (int s = 0; s < k; ++s) {
-    tree.clear();
-    for (int l = 0; l < kLanes; ++l)
-      for (size_t i = run[s] + l; i < run[s + 1]; i += kLanes) pos(tree.lane(l), i, s);
-    tree.reduce(&sparse[static_cast<size_t>(s) * nv]);
-  }
-  std::vector<double> total(static_cast<size_t>(k) * nv);
-  for (int s = 0; s < k; ++s) {
-    for (int v = 0; v < nv; ++v) {
-      double t = 0.0;
-      for (int w = 0; w < kWarps; ++w)
-        if (warp_start(d, w) < d.subject_start[s + 1] && warp_start(d, w + 1) > d.subject_start[s])
-          t += dense[static_cast<size_t>(s + w) * nv + v];
-      t += sparse[static_cast<size_t>(s) * nv + v];
-      total[static_cast<size_t>(s) * nv + v] = t;
-    }
-  }
-  return total;
-}
+namespace {
 
 // Slot layout of a per-subject partial: resid, weight, sum ln t, sum y eta,
 // sum y ln t, X'd (nb), sum p x (nb), sum p x x' (upper triangle).

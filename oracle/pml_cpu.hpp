@@ -53,6 +53,9 @@ bool opt_pml(const PmlData& data, const double* beta_init, const double* log_w_i
              double subject, double cell, const PmlParams& params, Prior prior, PmlResult* out);
 
 double min_eigenvalue(const double* a, int n);
+
+// Start of each subject's run of positive counts (pml.rs:1155-1160).
+std::vector<size_t> positive_runs(const PmlData& d);
 int check_convergence(const PmlResult& r, const PmlParams& p, bool at_bound, int initial);
 
 // pml_log_likelihood_gradient (pml.rs:573-615): the negated objective and

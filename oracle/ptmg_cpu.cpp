@@ -1,0 +1,190 @@
+// ORACLE — test infrastructure only. Stage one's per-subject cell sums on the
+// CPU (the reference's ptmg.rs linear_predictor 661-708 and the cell loops of
+// evaluate 926-966 / hessian_subject 1381-1428), in the summation tree and
+// with the exp/log and fused multiply-adds the device kernel ptmg_eval.cu
+// uses, so the two agree bit for bit; plus stage one driven by the CPU.
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "nbmath.hpp"
+#include "pml_cpu.hpp"
+#include "ptmg_cpu.hpp"
+#include "stage_one.hpp"
+#include "tree_cpu.hpp"
+
+namespace oracle {
+namespace {
+
+using nebula::nb_exp;
+using nebula::nb_fma;
+using nebula::nb_log;
+
+double eta_at(const PmlData& d, const double* beta, size_t r) {
+  const double* row = d.design + r * d.n_beta;
+  double eta = d.offset[r];
+  for (int j = 0; j < d.n_beta; ++j) eta = nb_fma(row[j], beta[j], eta);
+  return eta;
+}
+
+}  // namespace
+
+nebula::PtmgSums ptmg_sums(const PmlData& d, const double* beta, double alpha, double lambda, double gamma) {
+  const int nb = d.n_beta, k = d.k, T = nb * (nb + 1) / 2, W = nebula::ptmg_width(nb);
+  const int kXf = 9, kD41 = kXf + nb, kT1 = kD41 + nb, kT2 = kT1 + nb, kBp = kT2 + nb, kBq = kBp + T;
+  const std::vector<size_t> run = positive_runs(d);
+  nebula::PtmgSums out;
+  // pass one: sum e over every cell, sum y eta over the positive ones
+  auto dense1 = [&](double* acc, size_t r, int) { acc[0] += nb_exp(eta_at(d, beta, r)); };
+  auto sparse1 = [&](double* acc, size_t i, int) {
+    acc[1] = nb_fma(eta_at(d, beta, d.cells[i]), d.counts[i], acc[1]);
+  };
+  std::vector<double> p1 = tree_sums(d, run, 2, dense1, sparse1);
+  out.cumsumxtb.resize(k);
+  out.ylin.resize(k);
+  std::vector<double> ym(k);
+  for (int s = 0; s < k; ++s) {
+    out.cumsumxtb[s] = p1[2 * s];
+    out.ylin[s] = p1[2 * s + 1];
+    ym[s] = (d.subject_total[s] + alpha) / (p1[2 * s] + lambda);
+  }
+  // pass two
+  auto dense2 = [&](double* acc, size_t r, int s) {
+    const double* x = d.design + r * nb;
+    const double e = nb_exp(eta_at(d, beta, r));
+    const double yms = ym[s];
+    const double we = yms * e;
+    const double w = we + gamma;
+    const double lw = nb_log(w);
+    const double iw = 1.0 / w;
+    const double gg = gamma * iw;
+    const double gt = gg * iw;
+    const double gte = gt * e;
+    acc[0] += we;
+    acc[1] += lw;
+    acc[2] = nb_fma(gamma, lw, acc[2]);
+    acc[3] += gg;
+    acc[4] += iw;
+    acc[5] += gt;
+    acc[6] = nb_fma(gg, e, acc[6]);
+    acc[7] += gte - e * iw;
+    acc[8] = nb_fma(gte, e, acc[8]);
+    const double f1 = gt - iw;
+    const double q = yms * (yms * gte - gg);
+    int t = 0;
+    for (int a = 0; a < nb; ++a) {
+      const double xe = x[a] * e;
+      acc[kXf + a] += xe;
+      acc[kD41 + a] = nb_fma(gg, xe, acc[kD41 + a]);
+      acc[kT1 + a] = nb_fma(xe, f1, acc[kT1 + a]);
+      acc[kT2 + a] = nb_fma(xe, gte, acc[kT2 + a]);
+      for (int b = a; b < nb; ++b) {
+        const double c = xe * x[b];
+        acc[kBp + t] += c;
+        acc[kBq + t] = nb_fma(c, q, acc[kBq + t]);
+        ++t;
+      }
+    }
+  };
+  auto sparse2 = [&](double* acc, size_t i, int s) {
+    const size_t c = d.cells[i];
+    const double* x = d.design + c * nb;
+    const double y = d.counts[i];
+    const double e = nb_exp(eta_at(d, beta, c));
+    const double yms = ym[s];
+    const double w = yms * e + gamma;
+    const double lw = nb_log(w);
+    const double iw = 1.0 / w;
+    const double gg = y * iw;
+    const double gt = gg * iw;
+    const double gte = gt * e;
+    acc[2] = nb_fma(y, lw, acc[2]);
+    acc[3] += gg;
+    acc[5] += gt;
+    acc[6] = nb_fma(gg, e, acc[6]);
+    acc[7] += gte;
+    acc[8] = nb_fma(gte, e, acc[8]);
+    const double q = yms * (yms * gte - gg);
+    int t = 0;
+    for (int a = 0; a < nb; ++a) {
+      const double xe = x[a] * e;
+      acc[kD41 + a] = nb_fma(gg, xe, acc[kD41 + a]);
+      acc[kT1 + a] = nb_fma(xe, gt, acc[kT1 + a]);
+      acc[kT2 + a] = nb_fma(xe, gte, acc[kT2 + a]);
+      for (int b = a; b < nb; ++b) {
+        const double cc = xe * x[b];
+        acc[kBq + t] = nb_fma(cc, q, acc[kBq + t]);
+        ++t;
+      }
+    }
+  };
+  out.sums = tree_sums(d, run, W, dense2, sparse2);
+  return out;
+}
+
+nebula::GenePlan plan_gene(const nebula::Shared& sh, const nebula::GeneCounts& gc, const double* totals,
+                           int* evaluations) {
+  PmlData d{sh.design.data(), sh.log_offset.data(), sh.n_cells, sh.n_coef, gc.counts.data(), gc.cells.data(),
+            gc.counts.size(), sh.fid.data(), sh.n_subjects, totals};
+  const std::vector<double> xy = nebula::positive_xy(sh, gc);
+  nebula::MarginalGene mg{&sh, &gc, totals, xy.data()};
+  std::vector<double> start, lower, upper;
+  nebula::marginal_box(sh, gc, &start, &lower, &upper);
+  nebula::MarginalSearch search(start, lower, upper, sh.n_coef);
+  const int np = sh.n_coef + 2;
+  std::vector<double> g(np), h(static_cast<size_t>(np) * np);
+  while (const double* x = search.ask()) {
+    nebula::Terms t(x[sh.n_coef], x[sh.n_coef + 1]);
+    nebula::PtmgSums sums = ptmg_sums(d, x, t.alpha, t.lambda, t.gamma);
+    double f = nebula::ptmg_assemble(mg, x, sums, g.data(), h.data());
+    search.tell(f, g.data(), h.data());
+  }
+  if (evaluations) *evaluations = search.evaluations();
+  return nebula::plan_from(sh, gc, search.best(), search.failed());
+}
+
+}  // namespace oracle
+
+#define ORACLE_API extern "C" __attribute__((visibility("default")))
+
+// Value, gradient and Hessian of the marginal negative log-likelihood at
+// params = [beta, sigma, phi] (nebula:::ptmg_ll_der_hes, ptmg.rs:615).
+ORACLE_API double oracle_ptmg_eval(const double* design, const double* log_offset, uint64_t n_cells,
+                                   uint32_t n_coef, const double* counts, const uint32_t* cells, uint64_t n_pos,
+                                   const uint64_t* fid, uint32_t k, const double* totals, const double* params,
+                                   double* grad, double* hess) {
+  nebula::Shared sh;
+  sh.design.assign(design, design + n_cells * n_coef);
+  sh.log_offset.assign(log_offset, log_offset + n_cells);
+  sh.fid.assign(fid, fid + k + 1);
+  sh.n_cells = n_cells;
+  sh.n_coef = static_cast<int>(n_coef);
+  sh.n_subjects = static_cast<int>(k);
+  nebula::GeneCounts gc;
+  gc.counts.assign(counts, counts + n_pos);
+  gc.cells.assign(cells, cells + n_pos);
+  for (double y : gc.counts) {  // the tallies positive_indices keeps (ptmg.rs:1708-1719)
+    if (y == 1.0) {
+      ++gc.n_one;
+    } else if (y == 2.0) {
+      ++gc.n_two;
+    } else {
+      size_t i = 0;
+      while (i < gc.big_values.size() && gc.big_values[i] < y) ++i;
+      if (i < gc.big_values.size() && gc.big_values[i] == y) {
+        gc.big_mult[i] += 1.0;
+      } else {
+        gc.big_values.insert(gc.big_values.begin() + i, y);
+        gc.big_mult.insert(gc.big_mult.begin() + i, 1.0);
+      }
+    }
+  }
+  oracle::PmlData d{sh.design.data(), sh.log_offset.data(), n_cells, static_cast<int>(n_coef), gc.counts.data(),
+                    gc.cells.data(), n_pos, sh.fid.data(), static_cast<int>(k), totals};
+  const std::vector<double> xy = nebula::positive_xy(sh, gc);
+  nebula::MarginalGene mg{&sh, &gc, totals, xy.data()};
+  nebula::Terms t(params[n_coef], params[n_coef + 1]);
+  nebula::PtmgSums sums = oracle::ptmg_sums(d, params, t.alpha, t.lambda, t.gamma);
+  return nebula::ptmg_assemble(mg, params, sums, grad, hess);
+}

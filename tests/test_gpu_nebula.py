@@ -19,6 +19,13 @@ REL_LOGP = 1e-4    # log p-value against the oracle
 
 def compare_to_oracle(dev, ref, label):
     assert np.array_equal(dev.gene_index, ref.gene_index), label
+    # the device path and the oracle share their summation trees and exp/log,
+    # so they agree bit for bit; the tolerances below are the stated bar
+    for key in ("coefficients", "se", "covariance", "subject_overdispersion", "cell_overdispersion",
+                "convergence"):
+        a, b = getattr(dev, key), getattr(ref, key)
+        same = np.array_equal(a, b, equal_nan=True)
+        assert same, f"{label}: {key} not bit-identical (max diff {np.nanmax(np.abs(a - b)):.3e})"
     for key in ("coefficients", "subject_overdispersion", "cell_overdispersion"):
         ok, worst = gio.close(getattr(dev, key), getattr(ref, key), REL_PARAM, 1e-9)
         assert ok, f"{label}: {key} off by {worst:.2e}"
