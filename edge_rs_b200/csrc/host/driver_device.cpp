@@ -323,7 +323,8 @@ std::unique_ptr<Session> create_session(const nb_csr* counts, const uint64_t* su
   const Shared& sh = ss->prep.shared;
   const size_t G = ss->prep.kept.size();
   ss->genes.resize(G);
-  for (size_t g = 0; g < G; ++g) ss->genes[g] = positive_indices(ss->prep.counts, ss->prep.kept[g]);
+  parallel_for(G, ss->opt.host_threads,
+               [&](size_t g) { ss->genes[g] = positive_indices(ss->prep.counts, ss->prep.kept[g]); });
   ss->ms_prepare = ms_since(t0);
   auto t2 = Clock::now();
   ss->fitter = std::make_unique<DeviceFitter>(ss->prep, ss->genes, ss->opt.device);

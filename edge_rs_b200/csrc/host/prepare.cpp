@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <sstream>
+#include <unordered_map>
 #include <unordered_set>
 
 #include "common.hpp"
@@ -236,6 +237,8 @@ Prepared prepare(const nb_csr* counts, const uint64_t* subject_id, const double*
 
 GeneCounts positive_indices(const CsrView& csr, size_t gene) {
   GeneCounts out;
+  out.cells.reserve(csr.indptr[gene + 1] - csr.indptr[gene]);
+  out.counts.reserve(csr.indptr[gene + 1] - csr.indptr[gene]);
   double sum = 0.0;
   uint32_t prev = 0;
   bool have_prev = false;
@@ -256,17 +259,31 @@ GeneCounts positive_indices(const CsrView& csr, size_t gene) {
     }
   }
   out.mean_count = sum / static_cast<double>(csr.n_cells);
-  std::vector<double> big;
-  for (double y : out.counts)
-    if (y != 1.0 && y != 2.0) big.push_back(y);
-  std::sort(big.begin(), big.end());
-  for (double y : big) {
-    if (!out.big_values.empty() && out.big_values.back() == y) {
-      out.big_mult.back() += 1.0;
-    } else {
-      out.big_values.push_back(y);
-      out.big_mult.push_back(1.0);
+  // distinct counts other than one and two: small whole counts tallied by
+  // index, anything else in a map, then merged in increasing order
+  constexpr int kDirect = 1024;
+  std::vector<double> direct(kDirect, 0.0);
+  std::unordered_map<double, double> other;
+  for (double y : out.counts) {
+    if (y == 1.0 || y == 2.0) continue;
+    if (y < kDirect && y == std::floor(y)) direct[static_cast<int>(y)] += 1.0;
+    else other[y] += 1.0;
+  }
+  std::vector<std::pair<double, double>> rest(other.begin(), other.end());
+  std::sort(rest.begin(), rest.end());
+  size_t r = 0;
+  for (int v = 0; v < kDirect; ++v) {
+    if (direct[v] == 0.0) continue;
+    for (; r < rest.size() && rest[r].first < v; ++r) {
+      out.big_values.push_back(rest[r].first);
+      out.big_mult.push_back(rest[r].second);
     }
+    out.big_values.push_back(static_cast<double>(v));
+    out.big_mult.push_back(direct[v]);
+  }
+  for (; r < rest.size(); ++r) {
+    out.big_values.push_back(rest[r].first);
+    out.big_mult.push_back(rest[r].second);
   }
   return out;
 }
