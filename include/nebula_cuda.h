@@ -175,6 +175,32 @@ int32_t nb_opt_pml_cuda(const double* design, const double* offset,
                         double* scalars_out, int32_t* ints_out, char* err,
                         size_t err_len);
 
+/* nb_opt_pml_cuda for callers that cannot allocate device memory: an engine
+ * whose HBM belongs to its own pool or arena, a real-time loop that cannot
+ * take cudaMalloc's implicit synchronisation, a plugin that must not
+ * allocate after start-up. It has no counterpart in the reference. Every
+ * array argument is a DEVICE pointer (same meaning and layout as
+ * nb_opt_pml_cuda; ord may be NULL); the fit's working memory lives in one
+ * fixed 2 MiB device array inside this library, so the call allocates
+ * nothing. Limits: at most 2048 requests and 8192 subjects per call, else
+ * NB_ERR_INVALID_ARGUMENT before any launch. Runs on the calling thread's
+ * current device and `stream` (NULL: the default stream), and returns once
+ * the outputs are written. The first call on a device looks up the array's
+ * address; make it before any stream capture. All calls on a device share
+ * the array: calls whose GPU work overlaps race, so issue them one at a
+ * time. */
+int32_t nb_opt_pml_cuda_noalloc(const double* design, const double* offset,
+                                uint64_t n_cells, uint32_t n_beta,
+                                const double* counts, const uint32_t* cells,
+                                uint64_t n_pos, const uint64_t* subject_start,
+                                uint32_t k, const double* subject_total,
+                                uint32_t n_requests, const double* beta_init,
+                                const double* subject, const double* cell,
+                                const int32_t* ord, int32_t reml, double eps,
+                                double* beta_out, double* information_out,
+                                double* scalars_out, int32_t* ints_out,
+                                void* stream, char* err, size_t err_len);
+
 /* glm_sc_test (src/sc/test.rs:96-200): Wald test of the contrast c per gene,
  * z = c'beta / sqrt(c'Vc), p = chisq_sf(z^2, 1), BH FDR. log_p_value keeps
  * the tail in log space where p underflows. Any output may be NULL. */
