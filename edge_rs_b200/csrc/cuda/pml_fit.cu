@@ -32,7 +32,7 @@
 #include <cfloat>
 #include <cstdint>
 
-#include "../host/nbmath.hpp"
+#include "nbmath_device.cuh"
 #include "pml_device.cuh"
 
 namespace nebula {
@@ -64,6 +64,7 @@ __device__ __forceinline__ double warp_sum(double v) {
 template <int NB>
 struct Smem {
   int K;
+  NbTableData* tab;      // exp/log tables (nbmath.hpp)
   double* slots_dense;   // (K + kWarps) x NS
   double* slots_sparse;  // K x NS, per-subject totals after the combine
   double* sw[2];         // two sweeps: w K, dw K, vw K, vwb K*NB, db NB, vb NB*NB, ll 1
@@ -86,14 +87,16 @@ struct Smem {
 
   __host__ __device__ static size_t sweep_doubles(int K) { return 3 * K + K * NB + NB + NB * NB + 1; }
   __host__ __device__ static size_t doubles(int K) {
-    return (size_t)(2 * K + kWarps) * Dims<NB>::NS + 2 * sweep_doubles(K) + 4 * NB + 7 * K +
-           2 * NB * NB + 16;
+    return (size_t)kNbTableDoubles + (size_t)(2 * K + kWarps) * Dims<NB>::NS + 2 * sweep_doubles(K) + 4 * NB +
+           7 * K + 2 * NB * NB + 16;
   }
   __host__ __device__ static size_t bytes(int K) { return doubles(K) * 8 + (K + 1 + kWarps + 1) * 4 + 16; }
 
   __device__ void carve(double* base, int K_) {
     K = K_;
     double* p = base;
+    tab = reinterpret_cast<NbTableData*>(p);
+    p += kNbTableDoubles;
     slots_dense = p;
     p += (K + kWarps) * Dims<NB>::NS;
     slots_sparse = p;
@@ -191,7 +194,8 @@ __device__ __forceinline__ void load_row(const double* __restrict__ design, int 
 // The four per-cell Laplace sums (pml.rs:1842-1856, 1863-1868, 1893-1899),
 // each term scaled by gamma (dense) or the count (sparse).
 __device__ __forceinline__ void laplace_terms(double* acc, double e, double t, double gamma, double scale) {
-  const double p2 = e / (t * t), p3 = p2 / t, p4 = p3 / t, p5 = p4 / t, e2 = e * e;
+  const double inv = 1.0 / t;
+  const double p2 = (e * inv) * inv, p3 = p2 * inv, p4 = p3 * inv, p5 = p4 * inv, e2 = e * e;
   acc[0] += scale * p2;
   acc[1] += scale * (p3 * (gamma - e));
   acc[2] += scale * (p4 * (gamma * gamma + e2 - (4.0 * gamma) * e));
@@ -224,6 +228,7 @@ __device__ void sweep_sums(const GeneData& d, Smem<NB>& sm, int gene, const doub
   constexpr int NV = MODE == 0 ? Dims<NB>::NS : kLaplaceSums;
   const int K = sm.K;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const NbTableData* tab = sm.tab;
   double beta[NB];
 #pragma unroll
   for (int j = 0; j < NB; ++j) beta[j] = beta_sm[j];
@@ -247,11 +252,11 @@ __device__ void sweep_sums(const GeneData& d, Smem<NB>& sm, int gene, const doub
         double xa[NB], xb[NB];
         load_row<NB>(d.design, r, xa);
         load_row<NB>(d.design, rb, xb);
-        const double ea = nb_exp(linear_eta<NB>(xa, beta, __ldg(d.log_offset + r)) + lw);
-        const double eb = nb_exp(linear_eta<NB>(xb, beta, __ldg(d.log_offset + rb)) + lw);
+        const double ea = nb_exp_tab(linear_eta<NB>(xa, beta, __ldg(d.log_offset + r)) + lw, tab);
+        const double eb = nb_exp_tab(linear_eta<NB>(xb, beta, __ldg(d.log_offset + rb)) + lw, tab);
         const double ta = ea + gamma, tb = eb + gamma;
         if (MODE == 0) {
-          const double la = nb_log(ta), lb = nb_log(tb);
+          const double la = nb_log_tab(ta, tab), lb = nb_log_tab(tb, tab);
           const double inva = 1.0 / ta, invb = 1.0 / tb;
           const double ua = ea * inva, ub = eb * invb;
           acc[kSumLog] += la;
@@ -287,10 +292,10 @@ __device__ void sweep_sums(const GeneData& d, Smem<NB>& sm, int gene, const doub
       load_row<NB>(d.design, cb, xb);
       const double eta_a = linear_eta<NB>(xa, beta, __ldg(d.log_offset + ca));
       const double eta_b = linear_eta<NB>(xb, beta, __ldg(d.log_offset + cb));
-      const double ea = nb_exp(eta_a + lw), eb = nb_exp(eta_b + lw);
+      const double ea = nb_exp_tab(eta_a + lw, tab), eb = nb_exp_tab(eta_b + lw, tab);
       const double ta = ea + gamma, tb = eb + gamma;
       if (MODE == 0) {
-        const double la = nb_log(ta), lb = nb_log(tb);
+        const double la = nb_log_tab(ta, tab), lb = nb_log_tab(tb, tab);
         const double inva = 1.0 / ta, invb = 1.0 / tb;
         const double ua = ea * inva, ub = eb * invb;
         acc[kLinear] = nb_fma(eta_a, ya, acc[kLinear]);
@@ -495,6 +500,7 @@ __global__ void __launch_bounds__(kThreads, (NB <= 4 ? 2 : 1)) fit_kernel(GeneDa
   const int K = d.n_subjects;
   sm.carve(smem_raw, K);
   const int tid = threadIdx.x;
+  nb_load_tables(sm.tab);
   for (int i = tid; i <= K; i += blockDim.x) sm.fid[i] = d.fid[i];
   if (tid <= kWarps) sm.wcells[tid] = d.warp_cells[tid];
   __shared__ int next_req;

@@ -16,6 +16,22 @@
 // Both are within about one ulp of the correctly rounded result (checked
 // against the C library over the ranges the fits use) and handle 0, inf,
 // NaN and subnormals.
+//
+// nb_exp_tab / nb_log_tab: the per-cell pair, by Tang's table-driven method
+// (P. T. P. Tang, ACM TOMS 15(2) 1989 for exp, 16(4) 1990 for log), with the
+// tables of nbmath_tables.inc (gen_nbmath_tables.py) passed by pointer so a
+// kernel can serve them from shared memory. Fewer operations and a shorter
+// dependency chain than the pair above, and no division:
+//
+// exp: n = rint(x 256/ln2), r = x - n ln2/256 (two-part constant, |r| <=
+// ln2/512), exp(x) = 2^m 2^(j/256) (1 + q(r)) with n = 256 m + j, q the
+// Taylor polynomial of exp(r) - 1 to degree 5 (truncation below 1e-20), the
+// table value as hi + lo.
+//
+// log: x = 2^e m, m in [1, 2), j = round(256 (m - 1)) (j = 256 folds into
+// e + 1, m / 2, j = 0), r = m inv_j - 1 exact in one FMA because inv_j has
+// nine significant bits and |r| <= 2^-8, ln x = e ln2 + (-ln inv_j) +
+// log1p(r), log1p's Taylor polynomial to degree 7 (truncation below 2^-59).
 #pragma once
 
 #include <cstdint>
@@ -138,6 +154,83 @@ NB_HD double nb_log(double x) {
   const double ln2_lo = 1.90821492927058770002e-10;
   const double ed = static_cast<double>(e);
   return nb_fma(ed, ln2_hi, nb_fma(ed, ln2_lo, lnm));
+}
+
+// Tables of nb_exp_tab / nb_log_tab.
+struct alignas(16) NbPair {
+  double a, b;
+};
+struct NbTableData {
+  NbPair exp2_frac[256];   // {hi, lo} of 2^(j/256)
+  NbPair log_inv_hi[256];  // {inv_j, hi of -ln inv_j}
+  double log_lo[256];      // lo of -ln inv_j
+};
+constexpr int kNbTableDoubles = static_cast<int>(sizeof(NbTableData) / sizeof(double));
+
+// The host copy; device code reads a __device__ copy (nbmath_device.cuh)
+// or a shared-memory copy of it.
+inline constexpr NbTableData kNbTables = {
+#include "nbmath_tables.inc"
+};
+
+NB_HD double nb_exp_tab(double x, const NbTableData* t) {
+  if (!(x == x)) return x;                      // NaN
+  if (x > 709.782712893384) return 1.0 / 0.0;  // overflow
+  if (x < -745.1332191019412) return 0.0;      // underflow
+  const double inv_l = 0x1.71547652b82fep+8;    // 256 / ln 2
+  const double l_hi = 0x1.62e42fef80000p-9;     // ln 2 / 256, 34 bits
+  const double l_lo = 0x1.1cf79abc9e3b4p-44;
+  const double n = nb_rint(x * inv_l);
+  double r = nb_fma(-n, l_hi, x);
+  r = nb_fma(-n, l_lo, r);
+  double p = nb_fma(r, 1.0 / 120.0, 1.0 / 24.0);
+  p = nb_fma(p, r, 1.0 / 6.0);
+  p = nb_fma(p, r, 0.5);
+  const double q = nb_fma(r * r, p, r);
+  const int ni = static_cast<int>(n);
+  const int j = ni & 255;
+  const int m = (ni - j) / 256;
+  const NbPair s = t->exp2_frac[j];
+  const double er = s.a + nb_fma(s.a, q, s.b);
+  if (m >= -1021 && m <= 1023) return er * nb_pow2(m);
+  const int m1 = m / 2;
+  return (er * nb_pow2(m1)) * nb_pow2(m - m1);
+}
+
+NB_HD double nb_log_tab(double x, const NbTableData* t) {
+  if (!(x == x)) return x;         // NaN
+  if (x < 0.0) return 0.0 / 0.0;   // NaN
+  if (x == 0.0) return -1.0 / 0.0;
+  if (x == 1.0 / 0.0) return x;
+  int e = 0;
+  if (x < 2.2250738585072014e-308) {  // subnormal: scale into the normal range
+    x *= 18014398509481984.0;         // 2^54
+    e = -54;
+  }
+  const uint64_t u = nb_bits(x);
+  e += static_cast<int>((u >> 52) & 0x7ff) - 1023;
+  const uint64_t f = u & 0x000fffffffffffffULL;
+  double m = nb_from_bits(f | 0x3ff0000000000000ULL);  // [1, 2)
+  int j = static_cast<int>((f + (1ULL << 43)) >> 44);
+  if (j == 256) {
+    j = 0;
+    e += 1;
+    m *= 0.5;
+  }
+  const NbPair c = t->log_inv_hi[j];
+  const double r = nb_fma(m, c.a, -1.0);
+  double p = nb_fma(r, 1.0 / 7.0, -1.0 / 6.0);
+  p = nb_fma(p, r, 0.2);
+  p = nb_fma(p, r, -0.25);
+  p = nb_fma(p, r, 1.0 / 3.0);
+  p = nb_fma(p, r, -0.5);
+  const double l1p = nb_fma(r * r, p, r);
+  const double ln2_hi = 0x1.62e42fee00000p-1;  // 32 bits: e ln2_hi is exact
+  const double ln2_lo = 0x1.a39ef35793c76p-33;
+  const double ed = static_cast<double>(e);
+  const double hi = nb_fma(ed, ln2_hi, c.b);
+  const double lo = nb_fma(ed, ln2_lo, t->log_lo[j]);
+  return hi + (lo + l1p);
 }
 
 }  // namespace nebula

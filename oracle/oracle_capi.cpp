@@ -2,6 +2,7 @@
 // of bench.py load with ctypes. Never linked by the product library.
 #include <cstdint>
 
+#include "nbmath.hpp"
 #include "pml_cpu.hpp"
 
 #define ORACLE_API extern "C" __attribute__((visibility("default")))
@@ -56,4 +57,17 @@ ORACLE_API double oracle_pml_objective_gradient(const double* design, const doub
 
 ORACLE_API double oracle_min_eigenvalue(const double* a, uint32_t n) {
   return oracle::min_eigenvalue(a, static_cast<int>(n));
+}
+
+// The shared exp/log of nbmath.hpp over an array, for their accuracy tests:
+// which = 0 nb_exp, 1 nb_log, 2 nb_exp_tab, 3 nb_log_tab.
+ORACLE_API void oracle_nbmath(int32_t which, const double* x, double* out, uint64_t n) {
+  for (uint64_t i = 0; i < n; ++i) {
+    switch (which) {
+      case 0: out[i] = nebula::nb_exp(x[i]); break;
+      case 1: out[i] = nebula::nb_log(x[i]); break;
+      case 2: out[i] = nebula::nb_exp_tab(x[i], &nebula::kNbTables); break;
+      default: out[i] = nebula::nb_log_tab(x[i], &nebula::kNbTables); break;
+    }
+  }
 }

@@ -109,9 +109,9 @@ void sweep(const PmlData& d, const std::vector<double>& beta, const std::vector<
   const int nb = d.n_beta, k = d.k, T = nb * (nb + 1) / 2, nv = 5 + 2 * nb + T;
   auto dense = [&](double* acc, size_t r, int s) {
     double eta = eta_of(d, beta, r);
-    double e = nebula::nb_exp(eta + log_w[s]);
+    double e = nebula::nb_exp_tab(eta + log_w[s], &nebula::kNbTables);
     double t = e + gamma;
-    acc[kSumLog] += nebula::nb_log(t);
+    acc[kSumLog] += nebula::nb_log_tab(t, &nebula::kNbTables);
     double inv = 1.0 / t;
     double u = e * inv;
     fold(acc, d.design + r * nb, nb, -gamma * u, (gamma * u) * inv);
@@ -120,10 +120,10 @@ void sweep(const PmlData& d, const std::vector<double>& beta, const std::vector<
     size_t c = d.cells[i];
     double y = d.counts[i];
     double eta = eta_of(d, beta, c);
-    double e = nebula::nb_exp(eta + log_w[s]);
+    double e = nebula::nb_exp_tab(eta + log_w[s], &nebula::kNbTables);
     double t = e + gamma;
     acc[kLinear] = nebula::nb_fma(eta, y, acc[kLinear]);
-    acc[kWlog] = nebula::nb_fma(y, nebula::nb_log(t), acc[kWlog]);
+    acc[kWlog] = nebula::nb_fma(y, nebula::nb_log_tab(t, &nebula::kNbTables), acc[kWlog]);
     double inv = 1.0 / t;
     double u = e * inv;
     fold(acc, d.design + c * nb, nb, y * (1.0 - u), (y * u) * inv);
@@ -249,17 +249,18 @@ double laplace_correction(const PmlData& d, const std::vector<double>& beta, con
   const bool high = ord > 2;
   auto terms = [&](double e, double scale, double* acc) {
     double t = e + gamma;
-    double p2 = e / (t * t), p3 = p2 / t, p4 = p3 / t, p5 = p4 / t, e2 = e * e;
+    double inv = 1.0 / t;
+    double p2 = (e * inv) * inv, p3 = p2 * inv, p4 = p3 * inv, p5 = p4 * inv, e2 = e * e;
     acc[0] += scale * p2;
     acc[1] += scale * (p3 * (gamma - e));
     acc[2] += scale * (p4 * (gamma * gamma + e2 - (4.0 * gamma) * e));
     acc[3] += scale * (p5 * (gamma * gamma * gamma - (11.0 * gamma * gamma) * e + (11.0 * gamma) * e2 - e2 * e));
   };
   auto dense = [&](double* acc, size_t r, int s) {
-    terms(nebula::nb_exp(eta_of(d, beta, r) + log_w[s]), gamma, acc);
+    terms(nebula::nb_exp_tab(eta_of(d, beta, r) + log_w[s], &nebula::kNbTables), gamma, acc);
   };
   auto sparse = [&](double* acc, size_t i, int s) {
-    terms(nebula::nb_exp(eta_of(d, beta, d.cells[i]) + log_w[s]), d.counts[i], acc);
+    terms(nebula::nb_exp_tab(eta_of(d, beta, d.cells[i]) + log_w[s], &nebula::kNbTables), d.counts[i], acc);
   };
   std::vector<double> tot = tree_sums(d, run, 4, dense, sparse);
   double third_acc = 0, fourth_acc = 0, fifth_acc = 0;
