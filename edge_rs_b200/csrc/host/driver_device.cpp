@@ -139,13 +139,19 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
     fail(NB_ERR_UNSUPPORTED, "the fit kernel cannot be resident with " + std::to_string(K) +
                                  " subjects and " + std::to_string(sh.n_coef) + " columns");
   grid_ = per_sm * sms;
-  cuda_check(cudaMalloc(&d_counter_, 2 * sizeof(int32_t)), "cudaMalloc");
-  owned_.push_back(d_counter_);
-  cuda_check(cudaEventCreate(&ev0_), "event");
-  cuda_check(cudaEventCreate(&ev1_), "event");
+  for (Lane& lane : lanes_) {
+    cuda_check(cudaStreamCreateWithFlags(&lane.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    cuda_check(cudaEventCreate(&lane.ev0), "event");
+    cuda_check(cudaEventCreate(&lane.ev1), "event");
+    cuda_check(cudaMalloc(reinterpret_cast<void**>(&lane.d_counter), 2 * sizeof(int32_t)), "cudaMalloc");
+    owned_.push_back(lane.d_counter);
+    cuda_check(cudaMallocHost(reinterpret_cast<void**>(&lane.h_header), 2 * sizeof(int32_t)), "cudaMallocHost");
+  }
+  cuda_check(cudaMalloc(reinterpret_cast<void**>(&d_pcounter_), 2 * sizeof(int32_t)), "cudaMalloc");
+  owned_.push_back(d_pcounter_);
+  cuda_check(cudaMallocHost(reinterpret_cast<void**>(&h_pheader_), 2 * sizeof(int32_t)), "cudaMallocHost");
   cuda_check(cudaEventCreate(&step0_), "event");
   cuda_check(cudaEventCreate(&step1_), "event");
-  cuda_check(cudaMallocHost(reinterpret_cast<void**>(&h_header_), 2 * sizeof(int32_t)), "cudaMallocHost");
 }
 
 void DeviceFitter::reset_counters() {
@@ -153,9 +159,16 @@ void DeviceFitter::reset_counters() {
   launches_ = requests_ = sweeps_ = cell_visits_ = h2d_bytes_ = d2h_bytes_ = 0;
 }
 
-void DeviceFitter::begin_step() { cuda_check(cudaEventRecord(step0_, stream_), "event"); }
+void DeviceFitter::begin_step() {
+  cuda_check(cudaEventRecord(step0_, stream_), "event");
+  for (Lane& lane : lanes_) cuda_check(cudaStreamWaitEvent(lane.stream, step0_, 0), "stream wait");
+}
 
 double DeviceFitter::end_step() {
+  for (Lane& lane : lanes_) {
+    cuda_check(cudaEventRecord(lane.ev1, lane.stream), "event");
+    cuda_check(cudaStreamWaitEvent(stream_, lane.ev1, 0), "stream wait");
+  }
   cuda_check(cudaEventRecord(step1_, stream_), "event");
   cuda_check(cudaEventSynchronize(step1_), "event");
   float ms = 0.0f;
@@ -193,15 +206,15 @@ const double* DeviceFitter::run_ptmg(const std::vector<device::PtmgRequest>& req
     pcapacity_ = cap;
   }
   std::memcpy(h_preq_, reqs.data(), n * sizeof(device::PtmgRequest));
-  h_header_[0] = static_cast<int32_t>(n);
-  h_header_[1] = 0;
+  h_pheader_[0] = static_cast<int32_t>(n);
+  h_pheader_[1] = 0;
   cuda_check(cudaMemcpyAsync(d_preq_, h_preq_, n * sizeof(device::PtmgRequest), cudaMemcpyHostToDevice, stream_),
              "stage-one request copy");
-  cuda_check(cudaMemcpyAsync(d_counter_, h_header_, 2 * sizeof(int32_t), cudaMemcpyHostToDevice, stream_),
+  cuda_check(cudaMemcpyAsync(d_pcounter_, h_pheader_, 2 * sizeof(int32_t), cudaMemcpyHostToDevice, stream_),
              "count copy");
   const int grid = static_cast<int>(std::min<size_t>(pgrid_, n));
-  cuda_check(static_cast<cudaError_t>(
-                 device::launch_ptmg(data_, d_preq_, d_pres_, d_scratch_, d_counter_, d_counter_ + 1, grid, stream_)),
+  cuda_check(static_cast<cudaError_t>(device::launch_ptmg(data_, d_preq_, d_pres_, d_scratch_, d_pcounter_,
+                                                          d_pcounter_ + 1, grid, stream_)),
              "stage-one kernel launch");
   cuda_check(cudaMemcpyAsync(h_pres_, d_pres_, n * stride * sizeof(double), cudaMemcpyDeviceToHost, stream_),
              "stage-one result copy");
@@ -218,66 +231,90 @@ DeviceFitter::~DeviceFitter() {
   if (d_pres_) cudaFree(d_pres_);
   if (h_preq_) cudaFreeHost(h_preq_);
   if (h_pres_) cudaFreeHost(h_pres_);
+  for (Lane& lane : lanes_) {
+    if (lane.stream) cudaStreamSynchronize(lane.stream);
+    if (lane.d_req) cudaFree(lane.d_req);
+    if (lane.d_res) cudaFree(lane.d_res);
+    if (lane.h_req) cudaFreeHost(lane.h_req);
+    if (lane.h_res) cudaFreeHost(lane.h_res);
+    if (lane.h_header) cudaFreeHost(lane.h_header);
+    if (lane.ev0) cudaEventDestroy(lane.ev0);
+    if (lane.ev1) cudaEventDestroy(lane.ev1);
+    if (lane.stream) cudaStreamDestroy(lane.stream);
+  }
   for (void* p : owned_) cudaFree(p);
-  if (d_req_) cudaFree(d_req_);
-  if (d_res_) cudaFree(d_res_);
-  if (h_req_) cudaFreeHost(h_req_);
-  if (h_res_) cudaFreeHost(h_res_);
-  if (ev0_) cudaEventDestroy(ev0_);
-  if (ev1_) cudaEventDestroy(ev1_);
+  if (h_pheader_) cudaFreeHost(h_pheader_);
   if (step0_) cudaEventDestroy(step0_);
   if (step1_) cudaEventDestroy(step1_);
-  if (h_header_) cudaFreeHost(h_header_);
   if (stream_) cudaStreamDestroy(stream_);
 }
 
-void DeviceFitter::reserve(size_t n) {
-  if (n <= capacity_) return;
-  size_t cap = std::max<size_t>(n, capacity_ * 2);
-  if (d_req_) cudaFree(d_req_);
-  if (d_res_) cudaFree(d_res_);
-  if (h_req_) cudaFreeHost(h_req_);
-  if (h_res_) cudaFreeHost(h_res_);
-  cuda_check(cudaMalloc(reinterpret_cast<void**>(&d_req_), cap * sizeof(device::FitRequest)), "cudaMalloc");
-  cuda_check(cudaMalloc(reinterpret_cast<void**>(&d_res_), cap * sizeof(device::FitResult)), "cudaMalloc");
-  cuda_check(cudaMallocHost(reinterpret_cast<void**>(&h_req_), cap * sizeof(device::FitRequest)), "cudaMallocHost");
-  cuda_check(cudaMallocHost(reinterpret_cast<void**>(&h_res_), cap * sizeof(device::FitResult)), "cudaMallocHost");
-  capacity_ = cap;
+void DeviceFitter::reserve(Lane& lane, size_t n) {
+  if (n <= lane.capacity) return;
+  size_t cap = std::max<size_t>(n, lane.capacity * 2);
+  if (lane.d_req) cudaFree(lane.d_req);
+  if (lane.d_res) cudaFree(lane.d_res);
+  if (lane.h_req) cudaFreeHost(lane.h_req);
+  if (lane.h_res) cudaFreeHost(lane.h_res);
+  cuda_check(cudaMalloc(reinterpret_cast<void**>(&lane.d_req), cap * sizeof(device::FitRequest)), "cudaMalloc");
+  cuda_check(cudaMalloc(reinterpret_cast<void**>(&lane.d_res), cap * sizeof(device::FitResult)), "cudaMalloc");
+  cuda_check(cudaMallocHost(reinterpret_cast<void**>(&lane.h_req), cap * sizeof(device::FitRequest)),
+             "cudaMallocHost");
+  cuda_check(cudaMallocHost(reinterpret_cast<void**>(&lane.h_res), cap * sizeof(device::FitResult)),
+             "cudaMallocHost");
+  lane.capacity = cap;
 }
 
-const device::FitResult* DeviceFitter::run(const std::vector<device::FitRequest>& reqs) {
+void DeviceFitter::submit(int lane_index, const std::vector<device::FitRequest>& reqs) {
+  Lane& lane = lanes_[lane_index];
   const size_t n = reqs.size();
-  if (n == 0) return nullptr;
-  reserve(n);
-  std::memcpy(h_req_, reqs.data(), n * sizeof(device::FitRequest));
-  h_header_[0] = static_cast<int32_t>(n);
-  h_header_[1] = 0;
-  cuda_check(cudaMemcpyAsync(d_req_, h_req_, n * sizeof(device::FitRequest), cudaMemcpyHostToDevice, stream_),
+  lane.pending = n;
+  if (n == 0) return;
+  reserve(lane, n);
+  std::memcpy(lane.h_req, reqs.data(), n * sizeof(device::FitRequest));
+  lane.h_header[0] = static_cast<int32_t>(n);
+  lane.h_header[1] = 0;
+  cuda_check(cudaMemcpyAsync(lane.d_req, lane.h_req, n * sizeof(device::FitRequest), cudaMemcpyHostToDevice,
+                             lane.stream),
              "request copy");
-  cuda_check(cudaMemcpyAsync(d_counter_, h_header_, 2 * sizeof(int32_t), cudaMemcpyHostToDevice, stream_),
+  cuda_check(cudaMemcpyAsync(lane.d_counter, lane.h_header, 2 * sizeof(int32_t), cudaMemcpyHostToDevice,
+                             lane.stream),
              "count copy");
-  cuda_check(cudaEventRecord(ev0_, stream_), "event");
-  int grid = static_cast<int>(std::min<size_t>(grid_, n));
-  cuda_check(static_cast<cudaError_t>(device::launch_fit(data_, ctl_, d_req_, d_res_, d_counter_, d_counter_ + 1,
-                                                          grid, stream_)),
+  cuda_check(cudaEventRecord(lane.ev0, lane.stream), "event");
+  const int grid = static_cast<int>(std::min<size_t>(grid_, n));
+  cuda_check(static_cast<cudaError_t>(device::launch_fit(data_, ctl_, lane.d_req, lane.d_res, lane.d_counter,
+                                                          lane.d_counter + 1, grid, lane.stream)),
              "fit kernel launch");
-  cuda_check(cudaEventRecord(ev1_, stream_), "event");
-  cuda_check(cudaMemcpyAsync(h_res_, d_res_, n * sizeof(device::FitResult), cudaMemcpyDeviceToHost, stream_),
+  cuda_check(cudaEventRecord(lane.ev1, lane.stream), "event");
+  cuda_check(cudaMemcpyAsync(lane.h_res, lane.d_res, n * sizeof(device::FitResult), cudaMemcpyDeviceToHost,
+                             lane.stream),
              "result copy");
-  cuda_check(cudaStreamSynchronize(stream_), "fit kernel");
-  float ms = 0.0f;
-  cuda_check(cudaEventElapsedTime(&ms, ev0_, ev1_), "event time");
-  device_ms_ += ms;
   ++launches_;
   requests_ += n;
   h2d_bytes_ += n * sizeof(device::FitRequest) + 2 * sizeof(int32_t);
   d2h_bytes_ += n * sizeof(device::FitResult);
+}
+
+const device::FitResult* DeviceFitter::collect(int lane_index) {
+  Lane& lane = lanes_[lane_index];
+  const size_t n = lane.pending;
+  if (n == 0) return nullptr;
+  cuda_check(cudaStreamSynchronize(lane.stream), "fit kernel");
+  float ms = 0.0f;
+  cuda_check(cudaEventElapsedTime(&ms, lane.ev0, lane.ev1), "event time");
+  device_ms_ += ms;
   for (size_t i = 0; i < n; ++i) {
-    const uint64_t sw = static_cast<uint64_t>(h_res_[i].sweeps);
+    const uint64_t sw = static_cast<uint64_t>(lane.h_res[i].sweeps);
     sweeps_ += sw;
-    cell_visits_ += sw * (n_cells_ + gene_nnz_[reqs[i].gene]);
+    cell_visits_ += sw * (n_cells_ + gene_nnz_[lane.h_req[i].gene]);
   }
-  return h_res_;
+  lane.pending = 0;
+  return lane.h_res;
+}
+
+const device::FitResult* DeviceFitter::run(const std::vector<device::FitRequest>& reqs) {
+  submit(0, reqs);
+  return collect(0);
 }
 
 // ---------------------------------------------------------------------------
@@ -421,13 +458,20 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
     double subject, cell;
     int request;  // index into the batch, -1 when the point is outside the domain
   };
-  std::vector<device::FitRequest> batch;
-  std::vector<Slot> slots;
-  uint64_t rounds = 0;
-  while (!active.empty()) {
-    batch.clear();
-    slots.clear();
-    for (size_t g : active) {
+  // The genes are dealt round-robin onto the fitter's lanes. Each lane's
+  // searches advance in lockstep, one batch per round; the lanes leapfrog, so
+  // while one lane's batch runs on the device the host steps another lane's
+  // searches, and the lanes' kernels share the SMs. A gene's sequence of
+  // evaluations does not depend on which batch carries it.
+  constexpr int L = DeviceFitter::kLanes;
+  std::vector<size_t> lane_active[L];
+  std::vector<device::FitRequest> batch[L];
+  std::vector<Slot> slots[L];
+  for (size_t i = 0; i < active.size(); ++i) lane_active[i % L].push_back(active[i]);
+  auto build = [&](int l) {
+    batch[l].clear();
+    slots[l].clear();
+    for (size_t g : lane_active[l]) {
       GeneTask& t = tasks[g];
       const auto& points = t.search->ask();
       for (size_t p = 0; p < points.size(); ++p) {
@@ -442,23 +486,23 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
           r.subject = subject;
           r.cell = cell;
           for (int j = 0; j < sh.n_coef; ++j) r.beta[j] = beta[j];
-          slot = Slot{subject, cell, static_cast<int>(batch.size())};
-          batch.push_back(r);
+          slot = Slot{subject, cell, static_cast<int>(batch[l].size())};
+          batch[l].push_back(r);
         }
-        slots.push_back(slot);
+        slots[l].push_back(slot);
       }
     }
-    const device::FitResult* res = fitter.run(batch);
-    ++rounds;
+  };
+  auto absorb = [&](int l, const device::FitResult* res) {
     std::vector<double> values;
     size_t si = 0;
     std::vector<size_t> still;
-    for (size_t g : active) {
+    for (size_t g : lane_active[l]) {
       GeneTask& t = tasks[g];
       const size_t n_points = t.search->ask().size();
       values.assign(n_points, std::numeric_limits<double>::infinity());
       for (size_t p = 0; p < n_points; ++p, ++si) {
-        const Slot& s = slots[si];
+        const Slot& s = slots[l][si];
         if (s.request < 0) continue;
         const device::FitResult& r = res[s.request];
         if (r.status != 0) continue;
@@ -473,7 +517,29 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
         still.push_back(g);
       }
     }
-    active.swap(still);
+    lane_active[l].swap(still);
+  };
+  uint64_t rounds = 0;
+  int order[L];
+  int head = 0, count = 0;
+  for (int l = 0; l < L; ++l) {
+    if (lane_active[l].empty()) continue;
+    build(l);
+    fitter.submit(l, batch[l]);
+    order[(head + count++) % L] = l;
+  }
+  while (count > 0) {
+    const int l = order[head];
+    head = (head + 1) % L;
+    --count;
+    const device::FitResult* res = fitter.collect(l);
+    ++rounds;
+    absorb(l, res);
+    if (!lane_active[l].empty()) {
+      build(l);
+      fitter.submit(l, batch[l]);
+      order[(head + count++) % L] = l;
+    }
   }
   const double ms_stage_two = ms_since(t2);
 
@@ -481,7 +547,7 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
   auto t3 = Clock::now();
   std::vector<double> sigma(G), gamma(G);
   std::vector<int> conv(G);
-  batch.clear();
+  std::vector<device::FitRequest> final_batch;
   for (size_t g = 0; g < G; ++g) {
     apply_refit(ss.plans[g], tasks[g].refit, &sigma[g], &gamma[g], &conv[g]);
     device::FitRequest r{};
@@ -492,9 +558,9 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
     r.cell = gamma[g];
     for (int j = 0; j < sh.n_coef; ++j) r.beta[j] = ss.plans[g].beta_start[j];
     r.beta[sh.intercept] -= sigma[g] / 2.0;
-    batch.push_back(r);
+    final_batch.push_back(r);
   }
-  const device::FitResult* res = fitter.run(batch);
+  const device::FitResult* res = fitter.run(final_batch);
   std::vector<GeneOutcome> outcomes(G);
   for (size_t g = 0; g < G; ++g) {
     const device::FitResult& r = res[g];

@@ -13,16 +13,27 @@ namespace nebula {
 
 // Owns one call's device copy of the design, offsets and kept genes' counts,
 // and runs batches of inner fits on them.
+//
+// Batches go through lanes: each lane has its own stream, request/result
+// buffers and work-queue counter, so batches of different lanes run on the
+// device concurrently (a lane's kernel fills the SMs another lane's kernel
+// leaves idle) while the host prepares the next batch of another lane.
 class DeviceFitter {
  public:
+  static constexpr int kLanes = 4;
+
   DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& genes, int device);
   ~DeviceFitter();
   DeviceFitter(const DeviceFitter&) = delete;
   DeviceFitter& operator=(const DeviceFitter&) = delete;
 
-  // Runs one batch; the returned results (pinned host memory) stay valid
-  // until the next call.
+  // Runs one batch on lane 0 and waits; the returned results (pinned host
+  // memory) stay valid until lane 0's next batch.
   const device::FitResult* run(const std::vector<device::FitRequest>& reqs);
+  // Queues one batch on `lane` and returns at once; collect() waits for it
+  // and returns its results, valid until the lane's next submit().
+  void submit(int lane, const std::vector<device::FitRequest>& reqs);
+  const device::FitResult* collect(int lane);
   // One batch of stage-one evaluations: per request (2 + W) * K doubles,
   // valid until the next call.
   const double* run_ptmg(const std::vector<device::PtmgRequest>& reqs);
@@ -35,29 +46,38 @@ class DeviceFitter {
   uint64_t h2d_bytes() const { return h2d_bytes_; }
   uint64_t d2h_bytes() const { return d2h_bytes_; }
   void reset_counters();
-  // Brackets a step with events on the launching stream; end_step returns
-  // the device time between them in milliseconds.
+  // Brackets a step with events: begin_step orders every lane after it,
+  // end_step joins every lane and returns the device time between the two in
+  // milliseconds.
   void begin_step();
   double end_step();
 
  private:
-  void reserve(size_t n);
+  struct Lane {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int32_t* h_header = nullptr;  // pinned: request count and queue counter
+    int32_t* d_counter = nullptr;  // [0] request count, [1] work-queue counter
+    device::FitRequest* d_req = nullptr;
+    device::FitResult* d_res = nullptr;
+    device::FitRequest* h_req = nullptr;
+    device::FitResult* h_res = nullptr;
+    size_t capacity = 0;
+    size_t pending = 0;  // requests of the batch in flight
+  };
+  void reserve(Lane& lane, size_t n);
   cudaStream_t stream_ = nullptr;
-  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr, step0_ = nullptr, step1_ = nullptr;
+  cudaEvent_t step0_ = nullptr, step1_ = nullptr;
+  Lane lanes_[kLanes];
   std::vector<uint64_t> gene_nnz_;
   size_t n_cells_ = 0;
-  int32_t* h_header_ = nullptr;  // pinned: request count and queue counter
   device::GeneData data_{};
   device::FitControl ctl_{};
   std::vector<void*> owned_;
-  int32_t* d_counter_ = nullptr;  // [0] request count, [1] work-queue counter
-  device::FitRequest* d_req_ = nullptr;
-  device::FitResult* d_res_ = nullptr;
-  device::FitRequest* h_req_ = nullptr;
-  device::FitResult* h_res_ = nullptr;
-  size_t capacity_ = 0;
   int grid_ = 0;
   // stage-one buffers
+  int32_t* h_pheader_ = nullptr;
+  int32_t* d_pcounter_ = nullptr;
   device::PtmgRequest* d_preq_ = nullptr;
   device::PtmgRequest* h_preq_ = nullptr;
   double* d_pres_ = nullptr;
