@@ -65,7 +65,8 @@ class NbStats(ctypes.Structure):
                 ("ms_stage_two", ctypes.c_double), ("ms_stage_three", ctypes.c_double),
                 ("ms_device", ctypes.c_double), ("ms_step_device", ctypes.c_double),
                 ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64),
-                ("audited", ctypes.c_uint64), ("refit_cold", ctypes.c_uint64)]
+                ("audited", ctypes.c_uint64), ("refit_cold", ctypes.c_uint64),
+                ("fit_slots", ctypes.c_uint64), ("slot_cycles", ctypes.c_uint64)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

@@ -15,6 +15,8 @@ namespace device {
 constexpr int kMaxCoef = 8;        // the device path's width cap (pml_kernel.rs:1208-1212)
 constexpr int kThreads = 256;      // threads per fit CTA
 constexpr int kWarps = kThreads / 32;
+constexpr int kRanges = 64;        // fixed cell ranges of a sweep's summation tree
+constexpr int kMaxCluster = 8;     // CTAs one request may be spread over
 
 // One inner fit to run.
 struct alignas(16) FitRequest {
@@ -33,6 +35,8 @@ struct alignas(16) FitResult {
   double beta[kMaxCoef];
   double information[kMaxCoef * kMaxCoef];
   int32_t iterations, backtracks, sweeps, status;  // status 0 ok, 1 rejected arguments
+  int64_t cycles;  // SM clock cycles the CTA spent on the request
+  int64_t pad;
 };
 
 // Resident per-call data, device pointers.
@@ -45,7 +49,9 @@ struct GeneData {
   const double* counts;      // positive counts
   const uint64_t* runs;      // n_genes x (n_subjects + 1): first positive entry of each subject
   const double* totals;      // n_genes x n_subjects count totals
-  const uint32_t* warp_cells;  // kWarps + 1 boundaries of the dense pass's warp ranges
+  const uint32_t* warp_cells;  // kWarps + 1 boundaries of stage one's warp ranges
+  const uint32_t* range_cells; // kRanges + 1 boundaries of the sweep's cell ranges
+  const uint64_t* range_pos;   // n_genes x (kRanges + 1): first positive entry at or after each boundary
   int32_t n_cells;
   int32_t n_subjects;
   int32_t n_coef;
@@ -62,13 +68,19 @@ size_t fit_smem_bytes(int n_subjects, int n_coef);
 
 // Launches the persistent fit kernel over *n_requests (read on the device)
 // requests; `counter` must be zeroed before each launch (work queue).
-// `grid` CTAs loop over the queue. Returns cudaError_t as int.
+// `grid` CTAs, in thread-block clusters of `cluster` (1, 2, 4 or 8; grid a
+// multiple of it), loop over the queue, each cluster taking one request at a
+// time and sharing its sweeps. Returns cudaError_t as int.
 int launch_fit(const GeneData& data, const FitControl& ctl, const FitRequest* requests,
                FitResult* results, const int32_t* n_requests, int32_t* counter, int grid,
-               void* stream);
+               int cluster, void* stream);
 
 // CTAs per SM the fit kernel can keep resident for this shape.
 int fit_blocks_per_sm(int n_subjects, int n_coef);
+
+// Clusters of `cluster` CTAs the fit kernel can keep resident at once (0 if
+// none fits).
+int fit_max_clusters(int n_subjects, int n_coef, int cluster);
 
 }  // namespace device
 }  // namespace nebula

@@ -27,6 +27,7 @@
 // same exp/log (nbmath.hpp), fused multiply-adds only where written (the
 // file is compiled with -fmad=false), and the same summation tree, so the
 // two agree bit for bit and the stage-two search retraces the same points.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <cfloat>
@@ -34,6 +35,8 @@
 
 #include "nbmath_device.cuh"
 #include "pml_device.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace nebula {
 namespace device {
@@ -65,8 +68,8 @@ template <int NB>
 struct Smem {
   int K;
   NbTableData* tab;      // exp/log tables (nbmath.hpp)
-  double* slots_dense;   // (K + kWarps) x NS
-  double* slots_sparse;  // K x NS, per-subject totals after the combine
+  double* pieces[2];     // (K + kRanges) x NS each: one sweep's (subject, range) pieces, by sweep parity
+  double* totals;        // K x NS, per-subject totals after the combine
   double* sw[2];         // two sweeps: w K, dw K, vw K, vwb K*NB, db NB, vb NB*NB, ll 1
   double* beta;          // NB
   double* log_w;         // K
@@ -82,24 +85,32 @@ struct Smem {
   double* factor;        // NB*NB
   double* llv;           // K (per-subject log-likelihood terms)
   double* sc;            // 16 scalars
+  uint64_t* rpos;        // kRanges + 1: the request's gene's range_pos row
+  uint64_t* runs;        // K + 1: the request's gene's first positive entry per subject
   uint32_t* fid;         // K + 1
-  uint32_t* wcells;      // kWarps + 1
+  uint32_t* rcells;      // kRanges + 1
+  int32_t* vlo;          // K: first range meeting each subject
+  int32_t* vhi;          // K: last range meeting each subject
 
   __host__ __device__ static size_t sweep_doubles(int K) { return 3 * K + K * NB + NB + NB * NB + 1; }
   __host__ __device__ static size_t doubles(int K) {
-    return (size_t)kNbTableDoubles + (size_t)(2 * K + kWarps) * Dims<NB>::NS + 2 * sweep_doubles(K) + 4 * NB +
-           7 * K + 2 * NB * NB + 16;
+    return (size_t)kNbTableDoubles + (size_t)(3 * K + 2 * kRanges) * Dims<NB>::NS + 2 * sweep_doubles(K) +
+           4 * NB + 7 * K + 2 * NB * NB + 16 + (kRanges + 1) + (K + 1);
   }
-  __host__ __device__ static size_t bytes(int K) { return doubles(K) * 8 + (K + 1 + kWarps + 1) * 4 + 16; }
+  __host__ __device__ static size_t bytes(int K) {
+    return doubles(K) * 8 + (size_t)(K + 1 + kRanges + 1 + 2 * K) * 4 + 16;
+  }
 
   __device__ void carve(double* base, int K_) {
     K = K_;
     double* p = base;
     tab = reinterpret_cast<NbTableData*>(p);
     p += kNbTableDoubles;
-    slots_dense = p;
-    p += (K + kWarps) * Dims<NB>::NS;
-    slots_sparse = p;
+    pieces[0] = p;
+    p += (K + kRanges) * Dims<NB>::NS;
+    pieces[1] = p;
+    p += (K + kRanges) * Dims<NB>::NS;
+    totals = p;
     p += K * Dims<NB>::NS;
     sw[0] = p;
     p += sweep_doubles(K);
@@ -119,8 +130,14 @@ struct Smem {
     factor = p; p += NB * NB;
     llv = p; p += K;
     sc = p; p += 16;
+    rpos = reinterpret_cast<uint64_t*>(p);
+    p += kRanges + 1;
+    runs = reinterpret_cast<uint64_t*>(p);
+    p += K + 1;
     fid = reinterpret_cast<uint32_t*>(p);
-    wcells = fid + K + 1;
+    rcells = fid + K + 1;
+    vlo = reinterpret_cast<int32_t*>(rcells + kRanges + 1);
+    vhi = vlo + K;
   }
 };
 
@@ -219,33 +236,61 @@ __device__ __forceinline__ void reduce_to(double* acc, double* slot, int lane) {
   }
 }
 
-// One sweep's partial sums into the slots (dense then sparse), then the
-// per-subject combine into slots_sparse. Mode 0: the fit sums of
+// Which CTA of its cluster this is, and how many CTAs share each request.
+struct Cluster {
+  int rank, size;
+};
+
+__device__ __forceinline__ void cluster_barrier(const Cluster& cl) {
+  if (cl.size > 1) cg::this_cluster().sync();
+  else __syncthreads();
+}
+
+// One sweep's per-subject sums into sm.totals. Mode 0: the fit sums of
 // sweep_width; mode 1: the four Laplace sums (pml.rs:1842-1899).
+//
+// The cells are cut into kRanges fixed ranges; the cluster's CTAs split the
+// ranges (rank r takes kRanges / size consecutive ones) and a CTA's warps
+// take its ranges in turn. Within a range, each subject segment is one
+// piece: lanes stride the segment's cells at a count of zero (dense), then,
+// into the same partials, the gene's positive entries in the segment
+// (sparse, what each count changes), then the warp butterfly-reduces the
+// partials into the piece's slot (subject + range, unique because both
+// advance together). After a cluster barrier every CTA combines, per
+// subject and in range order, the pieces of the ranges that meet it, reading
+// other CTAs' pieces through distributed shared memory. The pieces are
+// double-buffered by sweep parity, so the next sweep's writes never race this
+// combine and one barrier per sweep suffices.
 template <int NB, int MODE>
-__device__ void sweep_sums(const GeneData& d, Smem<NB>& sm, int gene, const double* beta_sm,
-                           const double* log_w, double gamma) {
+__device__ void sweep_sums(const GeneData& d, Smem<NB>& sm, const double* beta_sm, const double* log_w,
+                           double gamma, int parity, const Cluster& cl) {
   constexpr int NV = MODE == 0 ? Dims<NB>::NS : kLaplaceSums;
+  constexpr int NS = Dims<NB>::NS;
   const int K = sm.K;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const NbTableData* tab = sm.tab;
+  double* pieces = sm.pieces[parity];
   double beta[NB];
 #pragma unroll
   for (int j = 0; j < NB; ++j) beta[j] = beta_sm[j];
 
-  // dense part: every cell at a count of zero
-  const int c_begin = static_cast<int>(sm.wcells[warp]), c_end = static_cast<int>(sm.wcells[warp + 1]);
-  if (c_begin < c_end) {
-    int s = subject_of(sm.fid, K, c_begin);
-    for (int c0 = c_begin; c0 < c_end; ++s) {
-      const int s_end = min(c_end, static_cast<int>(sm.fid[s + 1]));
+  const int per_cta = kRanges / cl.size;
+  for (int v = cl.rank * per_cta + warp; v < (cl.rank + 1) * per_cta; v += kWarps) {
+    const int a = static_cast<int>(sm.rcells[v]), b = static_cast<int>(sm.rcells[v + 1]);
+    if (a >= b) continue;
+    int s = subject_of(sm.fid, K, a);
+    uint64_t pa = sm.rpos[v];
+    const uint64_t pv_end = sm.rpos[v + 1];
+    for (int c0 = a; c0 < b; ++s) {
+      const int s_end = min(b, static_cast<int>(sm.fid[s + 1]));
+      const uint64_t p_end = min(sm.runs[s + 1], pv_end);
       const double lw = log_w[s];
       double acc[NV];
 #pragma unroll
-      for (int v = 0; v < NV; ++v) acc[v] = 0.0;
-      // Two cells (r and r + 32) per iteration: their exp/log/division chains
-      // are independent and interleave; each accumulator still takes cell r
-      // before cell r + 32, the order of the lane's sequential sum.
+      for (int x = 0; x < NV; ++x) acc[x] = 0.0;
+      // dense: two cells (r and r + 32) per iteration; their exp/log/division
+      // chains interleave, and each accumulator still takes cell r before
+      // cell r + 32, the order of the lane's sequential sum
       for (int r = c0 + lane; r < s_end; r += 64) {
         const bool has_b = r + 32 < s_end;
         const int rb = has_b ? r + 32 : r;
@@ -270,61 +315,54 @@ __device__ void sweep_sums(const GeneData& d, Smem<NB>& sm, int gene, const doub
           if (has_b) laplace_terms(acc, eb, tb, gamma, gamma);
         }
       }
-      reduce_to<NV>(acc, sm.slots_dense + (s + warp) * Dims<NB>::NS, lane);
+      // sparse: the segment's positive entries, into the same partials
+      for (uint64_t p = pa + lane; p < p_end; p += 64) {
+        const bool has_b = p + 32 < p_end;
+        const uint64_t pb = has_b ? p + 32 : p;
+        const int ca = static_cast<int>(__ldg(d.cells + p)), cb = static_cast<int>(__ldg(d.cells + pb));
+        const double ya = __ldg(d.counts + p), yb = __ldg(d.counts + pb);
+        double xa[NB], xb[NB];
+        load_row<NB>(d.design, ca, xa);
+        load_row<NB>(d.design, cb, xb);
+        const double eta_a = linear_eta<NB>(xa, beta, __ldg(d.log_offset + ca));
+        const double eta_b = linear_eta<NB>(xb, beta, __ldg(d.log_offset + cb));
+        const double ea = nb_exp_tab(eta_a + lw, tab), eb = nb_exp_tab(eta_b + lw, tab);
+        const double ta = ea + gamma, tb = eb + gamma;
+        if (MODE == 0) {
+          const double la = nb_log_tab(ta, tab), lb = nb_log_tab(tb, tab);
+          const double inva = 1.0 / ta, invb = 1.0 / tb;
+          const double ua = ea * inva, ub = eb * invb;
+          acc[kLinear] = nb_fma(eta_a, ya, acc[kLinear]);
+          acc[kWlog] = nb_fma(ya, la, acc[kWlog]);
+          fold<NB>(acc, xa, ya * (1.0 - ua), (ya * ua) * inva);
+          if (has_b) {
+            acc[kLinear] = nb_fma(eta_b, yb, acc[kLinear]);
+            acc[kWlog] = nb_fma(yb, lb, acc[kWlog]);
+            fold<NB>(acc, xb, yb * (1.0 - ub), (yb * ub) * invb);
+          }
+        } else {
+          laplace_terms(acc, ea, ta, gamma, ya);
+          if (has_b) laplace_terms(acc, eb, tb, gamma, yb);
+        }
+      }
+      reduce_to<NV>(acc, pieces + (s + v) * NS, lane);
+      pa = p_end;
       c0 = s_end;
     }
   }
-  // sparse part: what the positive counts change
-  const uint64_t* runs = d.runs + static_cast<size_t>(gene) * (K + 1);
-  for (int s = warp; s < K; s += kWarps) {
-    const uint64_t p0 = runs[s], p1 = runs[s + 1];
-    const double lw = log_w[s];
-    double acc[NV];
-#pragma unroll
-    for (int v = 0; v < NV; ++v) acc[v] = 0.0;
-    for (uint64_t p = p0 + lane; p < p1; p += 64) {
-      const bool has_b = p + 32 < p1;
-      const uint64_t pb = has_b ? p + 32 : p;
-      const int ca = static_cast<int>(__ldg(d.cells + p)), cb = static_cast<int>(__ldg(d.cells + pb));
-      const double ya = __ldg(d.counts + p), yb = __ldg(d.counts + pb);
-      double xa[NB], xb[NB];
-      load_row<NB>(d.design, ca, xa);
-      load_row<NB>(d.design, cb, xb);
-      const double eta_a = linear_eta<NB>(xa, beta, __ldg(d.log_offset + ca));
-      const double eta_b = linear_eta<NB>(xb, beta, __ldg(d.log_offset + cb));
-      const double ea = nb_exp_tab(eta_a + lw, tab), eb = nb_exp_tab(eta_b + lw, tab);
-      const double ta = ea + gamma, tb = eb + gamma;
-      if (MODE == 0) {
-        const double la = nb_log_tab(ta, tab), lb = nb_log_tab(tb, tab);
-        const double inva = 1.0 / ta, invb = 1.0 / tb;
-        const double ua = ea * inva, ub = eb * invb;
-        acc[kLinear] = nb_fma(eta_a, ya, acc[kLinear]);
-        acc[kWlog] = nb_fma(ya, la, acc[kWlog]);
-        fold<NB>(acc, xa, ya * (1.0 - ua), (ya * ua) * inva);
-        if (has_b) {
-          acc[kLinear] = nb_fma(eta_b, yb, acc[kLinear]);
-          acc[kWlog] = nb_fma(yb, lb, acc[kWlog]);
-          fold<NB>(acc, xb, yb * (1.0 - ub), (yb * ub) * invb);
-        }
-      } else {
-        laplace_terms(acc, ea, ta, gamma, ya);
-        if (has_b) laplace_terms(acc, eb, tb, gamma, yb);
-      }
-    }
-    reduce_to<NV>(acc, sm.slots_sparse + s * Dims<NB>::NS, lane);
-  }
-  __syncthreads();
-  // combine: per subject, the dense pieces in warp order, then the sparse part
+  cluster_barrier(cl);
+  // combine: per subject, the pieces of the non-empty ranges that meet it, in range order
   for (int idx = threadIdx.x; idx < K * NV; idx += blockDim.x) {
-    const int s = idx / NV, v = idx - s * NV;
-    const uint32_t a0 = sm.fid[s], a1 = sm.fid[s + 1];
+    const int s = idx / NV, x = idx - s * NV;
     double total = 0.0;
-#pragma unroll
-    for (int w = 0; w < kWarps; ++w) {
-      if (sm.wcells[w] < a1 && sm.wcells[w + 1] > a0) total += sm.slots_dense[(s + w) * Dims<NB>::NS + v];
+    for (int v = sm.vlo[s]; v <= sm.vhi[s]; ++v) {
+      if (sm.rcells[v] >= sm.rcells[v + 1]) continue;
+      const double* src = pieces + (s + v) * NS + x;
+      const int owner = v / per_cta;
+      if (owner != cl.rank) src = cg::this_cluster().map_shared_rank(src, owner);
+      total += *src;
     }
-    total += sm.slots_sparse[s * Dims<NB>::NS + v];
-    sm.slots_sparse[s * Dims<NB>::NS + v] = total;
+    sm.totals[s * NS + x] = total;
   }
   __syncthreads();
 }
@@ -332,14 +370,15 @@ __device__ void sweep_sums(const GeneData& d, Smem<NB>& sm, int gene, const doub
 // A full sweep into `out` (pml.rs:1564-1589).
 template <int NB>
 __device__ void sweep(const GeneData& d, Smem<NB>& sm, int gene, const double* beta, const double* log_w,
-                      SweepView<NB> out) {
+                      SweepView<NB> out, int& parity, const Cluster& cl) {
   const int K = sm.K;
   const double gamma = sm.sc[kGamma], alpha = sm.sc[kAlpha], lambda = sm.sc[kLambda];
-  sweep_sums<NB, 0>(d, sm, gene, beta, log_w, gamma);
+  sweep_sums<NB, 0>(d, sm, beta, log_w, gamma, parity, cl);
+  parity ^= 1;
   const double* tot = d.totals + static_cast<size_t>(gene) * K;
   const int tid = threadIdx.x;
   for (int s = tid; s < K; s += blockDim.x) {
-    const double* T = sm.slots_sparse + s * Dims<NB>::NS;
+    const double* T = sm.totals + s * Dims<NB>::NS;
     const double lw = log_w[s];
     const double w_s = nb_exp(lw);
     sm.llv[s] = T[kLinear] + lw * __ldg(tot + s) - gamma * T[kSumLog] - T[kWlog];
@@ -353,7 +392,7 @@ __device__ void sweep(const GeneData& d, Smem<NB>& sm, int gene, const double* b
   // sums over subjects in subject order, as the CPU path adds them
   if (tid < NB) {
     double acc = 0.0;
-    for (int s = 0; s < K; ++s) acc += sm.slots_sparse[s * Dims<NB>::NS + kScore + tid];
+    for (int s = 0; s < K; ++s) acc += sm.totals[s * Dims<NB>::NS + kScore + tid];
     out.db[tid] = acc;
   } else if (tid < NB + Dims<NB>::T) {
     const int t = tid - NB;
@@ -364,7 +403,7 @@ __device__ void sweep(const GeneData& d, Smem<NB>& sm, int gene, const double* b
     }
     const int b = a + rem;
     double acc = 0.0;
-    for (int s = 0; s < K; ++s) acc += gamma * sm.slots_sparse[s * Dims<NB>::NS + Dims<NB>::kSecond + t];
+    for (int s = 0; s < K; ++s) acc += gamma * sm.totals[s * Dims<NB>::NS + Dims<NB>::kSecond + t];
     out.vb[a * NB + b] = acc;
     out.vb[b * NB + a] = acc;
   } else if (tid == 64) {
@@ -502,17 +541,47 @@ __global__ void __launch_bounds__(kThreads, (NB <= 4 ? 2 : 1)) fit_kernel(GeneDa
   const int tid = threadIdx.x;
   nb_load_tables(sm.tab);
   for (int i = tid; i <= K; i += blockDim.x) sm.fid[i] = d.fid[i];
-  if (tid <= kWarps) sm.wcells[tid] = d.warp_cells[tid];
+  for (int i = tid; i <= kRanges; i += blockDim.x) sm.rcells[i] = d.range_cells[i];
+  __syncthreads();
+  // the ranges that meet each subject: vlo = first with end > fid[s],
+  // vhi = last with start < fid[s + 1]
+  for (int s = tid; s < K; s += blockDim.x) {
+    int lo = 0;
+    while (lo < kRanges - 1 && sm.rcells[lo + 1] <= sm.fid[s]) ++lo;
+    int hi = kRanges - 1;
+    while (hi > 0 && sm.rcells[hi] >= sm.fid[s + 1]) --hi;
+    sm.vlo[s] = lo;
+    sm.vhi[s] = hi;
+  }
+  Cluster cl;
+  {
+    cg::cluster_group cluster = cg::this_cluster();
+    cl.rank = static_cast<int>(cluster.block_rank());
+    cl.size = static_cast<int>(cluster.num_blocks());
+  }
   __shared__ int next_req;
   const int total = *n_requests;
+  int parity = 0;  // sweep parity of the pieces buffers, identical in every thread of the cluster
 
   for (;;) {
-    __syncthreads();
-    if (tid == 0) next_req = atomicAdd(counter, 1);
-    __syncthreads();
+    // one request per cluster: rank 0 takes it off the queue and hands it to
+    // every CTA; the first barrier keeps it from overwriting a value a CTA
+    // has not read yet
+    cluster_barrier(cl);
+    if (cl.rank == 0 && tid == 0) {
+      const int taken = atomicAdd(counter, 1);
+      if (cl.size == 1) {
+        next_req = taken;
+      } else {
+        cg::cluster_group cluster = cg::this_cluster();
+        for (int r = 0; r < cl.size; ++r) *cluster.map_shared_rank(&next_req, r) = taken;
+      }
+    }
+    cluster_barrier(cl);
     const int q = next_req;
     if (q >= total) break;
     const FitRequest req = requests[q];
+    const long long t_start = clock64();
     const int gene = req.gene;
     FitResult* out = results + q;
 
@@ -520,10 +589,11 @@ __global__ void __launch_bounds__(kThreads, (NB <= 4 ? 2 : 1)) fit_kernel(GeneDa
     const double exps = nb_exp(req.subject);
     const bool bad = !(isfinite(exps) && exps > 1.0) || !(isfinite(req.cell) && req.cell > 0.0);
     if (bad) {
-      if (tid == 0) {
+      if (tid == 0 && cl.rank == 0) {
         out->status = 1;
         out->iterations = 0;
         out->sweeps = 0;
+        out->cycles = 0;
       }
       continue;
     }
@@ -535,10 +605,13 @@ __global__ void __launch_bounds__(kThreads, (NB <= 4 ? 2 : 1)) fit_kernel(GeneDa
     }
     if (tid < NB) sm.beta[tid] = req.beta[tid];
     for (int s = tid; s < K; s += blockDim.x) sm.log_w[s] = 0.0;
+    for (int i = tid; i <= kRanges; i += blockDim.x)
+      sm.rpos[i] = d.range_pos[static_cast<size_t>(gene) * (kRanges + 1) + i];
+    for (int i = tid; i <= K; i += blockDim.x) sm.runs[i] = d.runs[static_cast<size_t>(gene) * (K + 1) + i];
     __syncthreads();
 
     int cur = 0;  // index of the current sweep buffer (every thread tracks it identically)
-    sweep<NB>(d, sm, gene, sm.beta, sm.log_w, SweepView<NB>(sm.sw[cur], K));
+    sweep<NB>(d, sm, gene, sm.beta, sm.log_w, SweepView<NB>(sm.sw[cur], K), parity, cl);
     if (tid == 0) {
       sm.sc[kLl] = *SweepView<NB>(sm.sw[cur], K).ll;
       sm.sc[kLlPrev] = 0.0;
@@ -597,7 +670,7 @@ __global__ void __launch_bounds__(kThreads, (NB <= 4 ? 2 : 1)) fit_kernel(GeneDa
       if (tid < NB) sm.new_beta[tid] = sm.beta[tid] + sm.step_beta[tid];
       if (tid == 0) sm.sc[kLlPrev] = sm.sc[kLl];
       __syncthreads();
-      sweep<NB>(d, sm, gene, sm.new_beta, sm.new_log_w, tr);
+      sweep<NB>(d, sm, gene, sm.new_beta, sm.new_log_w, tr, parity, cl);
       if (tid == 0) {
         sm.sc[kLl] = *tr.ll;
         sm.sc[kLikdif] = sm.sc[kLl] - sm.sc[kLlPrev];
@@ -652,7 +725,7 @@ __global__ void __launch_bounds__(kThreads, (NB <= 4 ? 2 : 1)) fit_kernel(GeneDa
           }
         }
         __syncthreads();
-        sweep<NB>(d, sm, gene, sm.new_beta, sm.new_log_w, tr);
+        sweep<NB>(d, sm, gene, sm.new_beta, sm.new_log_w, tr, parity, cl);
         if (tid == 0) {
           sm.sc[kLl] = *tr.ll;
           sm.sc[kLikdif] = sm.sc[kLl] - sm.sc[kLlPrev];
@@ -681,13 +754,14 @@ __global__ void __launch_bounds__(kThreads, (NB <= 4 ? 2 : 1)) fit_kernel(GeneDa
     // higher-order Laplace correction at the final iterate (pml.rs:1828-1919)
     if (req.ord > 1) {
       SweepView<NB> c(sm.sw[cur], K);
-      sweep_sums<NB, 1>(d, sm, gene, sm.beta, sm.log_w, sm.sc[kGamma]);
+      sweep_sums<NB, 1>(d, sm, sm.beta, sm.log_w, sm.sc[kGamma], parity, cl);
+      parity ^= 1;
       if (tid == 0) {
         const double gamma = sm.sc[kGamma], lambda = sm.sc[kLambda];
         const bool high = req.ord > 2;
         double third_acc = 0.0, fourth_acc = 0.0, fifth_acc = 0.0;
         for (int s = 0; s < K; ++s) {
-          const double* S = sm.slots_sparse + s * Dims<NB>::NS;
+          const double* S = sm.totals + s * Dims<NB>::NS;
           const double prior = lambda * c.w[s];
           const double vw = gamma * S[0] + prior;
           const double third = gamma * S[1] + prior;
@@ -710,6 +784,7 @@ __global__ void __launch_bounds__(kThreads, (NB <= 4 ? 2 : 1)) fit_kernel(GeneDa
       }
       __syncthreads();
     }
+    if (cl.rank != 0) continue;  // rank 0 of the cluster writes the result
     if (tid < NB) out->beta[tid] = sm.beta[tid];
     for (int i = tid; i < NB * NB; i += blockDim.x) out->information[i] = sm.vb2[i];
     if (tid == 0) {
@@ -721,6 +796,7 @@ __global__ void __launch_bounds__(kThreads, (NB <= 4 ? 2 : 1)) fit_kernel(GeneDa
       out->backtracks = static_cast<int32_t>(sm.sc[kBacktracks]);
       out->sweeps = static_cast<int32_t>(sm.sc[kSweeps]);
       out->status = 0;
+      out->cycles = clock64() - t_start;
     }
   }
 }
@@ -741,12 +817,28 @@ cudaError_t configure_nb(size_t smem) {
 
 template <int NB>
 int launch_nb(const GeneData& d, const FitControl& ctl, const FitRequest* req, FitResult* res,
-              const int32_t* n_req, int32_t* counter, int grid, cudaStream_t stream) {
+              const int32_t* n_req, int32_t* counter, int grid, int cluster, cudaStream_t stream) {
   const size_t smem = Smem<NB>::bytes(d.n_subjects);
   cudaError_t e = configure_nb<NB>(smem);
   if (e != cudaSuccess) return e;
-  fit_kernel<NB><<<grid, kThreads, smem, stream>>>(d, ctl, req, res, n_req, counter);
-  return cudaGetLastError();
+  if (cluster <= 1) {
+    fit_kernel<NB><<<grid, kThreads, smem, stream>>>(d, ctl, req, res, n_req, counter);
+    return cudaGetLastError();
+  }
+  if (cluster > kMaxCluster || (cluster & (cluster - 1)) != 0 || grid % cluster != 0) return cudaErrorInvalidValue;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid, 1, 1);
+  cfg.blockDim = dim3(kThreads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, fit_kernel<NB>, d, ctl, req, res, n_req, counter);
 }
 
 template <int NB>
@@ -757,6 +849,26 @@ int blocks_nb(int K) {
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fit_kernel<NB>, kThreads, smem) != cudaSuccess)
     return 0;
   return blocks;
+}
+
+template <int NB>
+int clusters_nb(int K, int cluster) {
+  const size_t smem = Smem<NB>::bytes(K);
+  if (configure_nb<NB>(smem) != cudaSuccess) return 0;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(cluster, 1, 1);
+  cfg.blockDim = dim3(kThreads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, fit_kernel<NB>, &cfg) != cudaSuccess) return 0;
+  return n;
 }
 
 }  // namespace
@@ -789,18 +901,32 @@ int fit_blocks_per_sm(int n_subjects, int n_coef) {
   }
 }
 
+int fit_max_clusters(int n_subjects, int n_coef, int cluster) {
+  switch (n_coef) {
+    case 1: return clusters_nb<1>(n_subjects, cluster);
+    case 2: return clusters_nb<2>(n_subjects, cluster);
+    case 3: return clusters_nb<3>(n_subjects, cluster);
+    case 4: return clusters_nb<4>(n_subjects, cluster);
+    case 5: return clusters_nb<5>(n_subjects, cluster);
+    case 6: return clusters_nb<6>(n_subjects, cluster);
+    case 7: return clusters_nb<7>(n_subjects, cluster);
+    case 8: return clusters_nb<8>(n_subjects, cluster);
+    default: return 0;
+  }
+}
+
 int launch_fit(const GeneData& d, const FitControl& ctl, const FitRequest* req, FitResult* res,
-               const int32_t* n_req, int32_t* counter, int grid, void* stream) {
+               const int32_t* n_req, int32_t* counter, int grid, int cluster, void* stream) {
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   switch (d.n_coef) {
-    case 1: return launch_nb<1>(d, ctl, req, res, n_req, counter, grid, s);
-    case 2: return launch_nb<2>(d, ctl, req, res, n_req, counter, grid, s);
-    case 3: return launch_nb<3>(d, ctl, req, res, n_req, counter, grid, s);
-    case 4: return launch_nb<4>(d, ctl, req, res, n_req, counter, grid, s);
-    case 5: return launch_nb<5>(d, ctl, req, res, n_req, counter, grid, s);
-    case 6: return launch_nb<6>(d, ctl, req, res, n_req, counter, grid, s);
-    case 7: return launch_nb<7>(d, ctl, req, res, n_req, counter, grid, s);
-    case 8: return launch_nb<8>(d, ctl, req, res, n_req, counter, grid, s);
+    case 1: return launch_nb<1>(d, ctl, req, res, n_req, counter, grid, cluster, s);
+    case 2: return launch_nb<2>(d, ctl, req, res, n_req, counter, grid, cluster, s);
+    case 3: return launch_nb<3>(d, ctl, req, res, n_req, counter, grid, cluster, s);
+    case 4: return launch_nb<4>(d, ctl, req, res, n_req, counter, grid, cluster, s);
+    case 5: return launch_nb<5>(d, ctl, req, res, n_req, counter, grid, cluster, s);
+    case 6: return launch_nb<6>(d, ctl, req, res, n_req, counter, grid, cluster, s);
+    case 7: return launch_nb<7>(d, ctl, req, res, n_req, counter, grid, cluster, s);
+    case 8: return launch_nb<8>(d, ctl, req, res, n_req, counter, grid, cluster, s);
     default: return cudaErrorInvalidValue;
   }
 }

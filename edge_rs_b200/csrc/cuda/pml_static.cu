@@ -66,6 +66,8 @@ struct Layout {
   size_t runs;        // uint64 (k + 1) first positive entry of each subject
   size_t gene_ptr;    // uint64 2
   size_t warp_cells;  // uint32 kWarps + 1
+  size_t range_cells; // uint32 kRanges + 1
+  size_t range_pos;   // uint64 kRanges + 1
   size_t requests;    // FitRequest n
   size_t results;     // FitResult n
   size_t end;
@@ -78,7 +80,9 @@ constexpr Layout layout_for(size_t k, size_t n) {
   l.runs = l.fid + round_up((k + 1) * sizeof(uint32_t));
   l.gene_ptr = l.runs + round_up((k + 1) * sizeof(uint64_t));
   l.warp_cells = l.gene_ptr + round_up(2 * sizeof(uint64_t));
-  l.requests = l.warp_cells + round_up((kWarps + 1) * sizeof(uint32_t));
+  l.range_cells = l.warp_cells + round_up((kWarps + 1) * sizeof(uint32_t));
+  l.range_pos = l.range_cells + round_up((kRanges + 1) * sizeof(uint32_t));
+  l.requests = l.range_pos + round_up((kRanges + 1) * sizeof(uint64_t));
   l.results = l.requests + round_up(n * sizeof(FitRequest));
   l.end = l.results + round_up(n * sizeof(FitResult));
   return l;
@@ -110,6 +114,8 @@ __global__ void stage_noalloc(unsigned char* scratch, Layout L, const uint64_t* 
   uint64_t* runs = reinterpret_cast<uint64_t*>(scratch + L.runs);
   uint64_t* gene_ptr = reinterpret_cast<uint64_t*>(scratch + L.gene_ptr);
   uint32_t* warp_cells = reinterpret_cast<uint32_t*>(scratch + L.warp_cells);
+  uint32_t* range_cells = reinterpret_cast<uint32_t*>(scratch + L.range_cells);
+  uint64_t* range_pos = reinterpret_cast<uint64_t*>(scratch + L.range_pos);
   FitRequest* reqs = reinterpret_cast<FitRequest*>(scratch + L.requests);
   const uint64_t tid = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
@@ -142,6 +148,17 @@ __global__ void stage_noalloc(unsigned char* scratch, Layout L, const uint64_t* 
     reqs[q] = r;
   }
   if (tid <= static_cast<uint64_t>(kWarps)) warp_cells[tid] = static_cast<uint32_t>(n_cells * tid / kWarps);
+  for (uint64_t v = tid; v <= static_cast<uint64_t>(kRanges); v += stride) {
+    // the sweep's cell ranges and the first positive entry at or after each boundary
+    const uint64_t b = n_cells * v / kRanges;
+    range_cells[v] = static_cast<uint32_t>(b);
+    uint64_t lo = 0, hi = n_pos;
+    while (lo < hi) {
+      const uint64_t mid = lo + (hi - lo) / 2;
+      if (cells[mid] < b) lo = mid + 1; else hi = mid;
+    }
+    range_pos[v] = lo;
+  }
   if (tid == 0) {
     gene_ptr[0] = 0;
     gene_ptr[1] = n_pos;
@@ -252,7 +269,7 @@ NB_API int32_t nb_opt_pml_cuda_noalloc(const double* design, const double* offse
     uint64_t items = n_pos;
     if (k + uint64_t{1} > items) items = k + uint64_t{1};
     if (n_requests > items) items = n_requests;
-    if (static_cast<uint64_t>(kWarps) + 1 > items) items = kWarps + 1;
+    if (static_cast<uint64_t>(kRanges) + 1 > items) items = kRanges + 1;
     uint64_t blocks = (items + kStageThreads - 1) / kStageThreads;
     const uint64_t max_blocks = static_cast<uint64_t>(slot.sms) * 8;
     if (blocks > max_blocks) blocks = max_blocks;
@@ -277,6 +294,8 @@ NB_API int32_t nb_opt_pml_cuda_noalloc(const double* design, const double* offse
     data.runs = reinterpret_cast<const uint64_t*>(base + L.runs);
     data.totals = subject_total;
     data.warp_cells = reinterpret_cast<const uint32_t*>(base + L.warp_cells);
+    data.range_cells = reinterpret_cast<const uint32_t*>(base + L.range_cells);
+    data.range_pos = reinterpret_cast<const uint64_t*>(base + L.range_pos);
     data.n_cells = static_cast<int32_t>(n_cells);
     data.n_subjects = static_cast<int32_t>(k);
     data.n_coef = static_cast<int32_t>(n_beta);
@@ -286,7 +305,7 @@ NB_API int32_t nb_opt_pml_cuda_noalloc(const double* design, const double* offse
     ctl.max_backtrack = kPmlMaxBacktrack;
     FitResult* results = reinterpret_cast<FitResult*>(base + L.results);
     const int launched = launch_fit(data, ctl, reinterpret_cast<const FitRequest*>(base + L.requests), results,
-                                    header, header + 1, per_sm * slot.sms, st);
+                                    header, header + 1, per_sm * slot.sms, 1, st);
     check(static_cast<cudaError_t>(launched), "fit kernel launch");
     unpack_noalloc<<<(n_requests + kStageThreads - 1) / kStageThreads, kStageThreads, 0, st>>>(
         results, n_requests, n_beta, beta_out, information_out, scalars_out, ints_out);

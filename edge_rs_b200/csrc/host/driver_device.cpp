@@ -111,6 +111,19 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
   std::vector<uint32_t> wcells(device::kWarps + 1);
   for (int w = 0; w <= device::kWarps; ++w)
     wcells[w] = static_cast<uint32_t>(sh.n_cells * static_cast<size_t>(w) / device::kWarps);
+  // the sweep's fixed cell ranges and, per gene, the first positive entry at
+  // or after each range boundary (absolute positions)
+  constexpr int R = device::kRanges;
+  std::vector<uint32_t> rcells(R + 1);
+  for (int v = 0; v <= R; ++v) rcells[v] = static_cast<uint32_t>(sh.n_cells * static_cast<size_t>(v) / R);
+  std::vector<uint64_t> rpos(G * (R + 1));
+  for (size_t g = 0; g < G; ++g) {
+    const GeneCounts& gc = genes[g];
+    for (int v = 0; v <= R; ++v) {
+      auto it = std::lower_bound(gc.cells.begin(), gc.cells.end(), rcells[v]);
+      rpos[g * (R + 1) + v] = gene_ptr[g] + static_cast<uint64_t>(it - gc.cells.begin());
+    }
+  }
 
   data_.design = device_copy(sh.design.data(), sh.design.size(), &owned_);
   data_.log_offset = device_copy(sh.log_offset.data(), sh.log_offset.size(), &owned_);
@@ -121,9 +134,11 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
   data_.runs = device_copy(runs.data(), runs.size(), &owned_);
   data_.totals = device_copy(totals.data(), totals.size(), &owned_);
   data_.warp_cells = device_copy(wcells.data(), wcells.size(), &owned_);
+  data_.range_cells = device_copy(rcells.data(), rcells.size(), &owned_);
+  data_.range_pos = device_copy(rpos.data(), rpos.size(), &owned_);
   h2d_bytes_ = (sh.design.size() + sh.log_offset.size() + counts.size() + totals.size()) * sizeof(double) +
-               (fid.size() + cells.size() + wcells.size()) * sizeof(uint32_t) +
-               (gene_ptr.size() + runs.size()) * sizeof(uint64_t);
+               (fid.size() + cells.size() + wcells.size() + rcells.size()) * sizeof(uint32_t) +
+               (gene_ptr.size() + runs.size() + rpos.size()) * sizeof(uint64_t);
   data_.n_cells = static_cast<int32_t>(sh.n_cells);
   data_.n_subjects = K;
   data_.n_coef = sh.n_coef;
@@ -139,6 +154,8 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
     fail(NB_ERR_UNSUPPORTED, "the fit kernel cannot be resident with " + std::to_string(K) +
                                  " subjects and " + std::to_string(sh.n_coef) + " columns");
   grid_ = per_sm * sms;
+  for (int c = 2; c <= device::kMaxCluster; c *= 2)
+    max_clusters_[c] = device::fit_max_clusters(K, sh.n_coef, c);
   for (Lane& lane : lanes_) {
     cuda_check(cudaStreamCreateWithFlags(&lane.stream, cudaStreamNonBlocking), "cudaStreamCreate");
     cuda_check(cudaEventCreate(&lane.ev0), "event");
@@ -156,7 +173,7 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
 
 void DeviceFitter::reset_counters() {
   device_ms_ = 0.0;
-  launches_ = requests_ = sweeps_ = cell_visits_ = h2d_bytes_ = d2h_bytes_ = 0;
+  launches_ = requests_ = sweeps_ = cell_visits_ = slot_cycles_ = h2d_bytes_ = d2h_bytes_ = 0;
 }
 
 void DeviceFitter::begin_step() {
@@ -281,9 +298,20 @@ void DeviceFitter::submit(int lane_index, const std::vector<device::FitRequest>&
                              lane.stream),
              "count copy");
   cuda_check(cudaEventRecord(lane.ev0, lane.stream), "event");
-  const int grid = static_cast<int>(std::min<size_t>(grid_, n));
+  // Spread each request over a cluster of CTAs when the requests in flight
+  // leave SM slots idle: the largest power of two (up to kMaxCluster) with
+  // requests x cluster within the resident CTA slots.
+  size_t in_flight = n;
+  for (const Lane& other : lanes_)
+    if (&other != &lane) in_flight += other.pending;
+  int cluster = 1;
+  while (cluster < device::kMaxCluster && in_flight * static_cast<size_t>(cluster) * 2 <= static_cast<size_t>(grid_) &&
+         max_clusters_[cluster * 2] > 0)
+    cluster *= 2;
+  int grid = static_cast<int>(std::min<size_t>(grid_, n));
+  if (cluster > 1) grid = static_cast<int>(std::min<size_t>(max_clusters_[cluster], n)) * cluster;
   cuda_check(static_cast<cudaError_t>(device::launch_fit(data_, ctl_, lane.d_req, lane.d_res, lane.d_counter,
-                                                          lane.d_counter + 1, grid, lane.stream)),
+                                                          lane.d_counter + 1, grid, cluster, lane.stream)),
              "fit kernel launch");
   cuda_check(cudaEventRecord(lane.ev1, lane.stream), "event");
   cuda_check(cudaMemcpyAsync(lane.h_res, lane.d_res, n * sizeof(device::FitResult), cudaMemcpyDeviceToHost,
@@ -307,6 +335,7 @@ const device::FitResult* DeviceFitter::collect(int lane_index) {
     const uint64_t sw = static_cast<uint64_t>(lane.h_res[i].sweeps);
     sweeps_ += sw;
     cell_visits_ += sw * (n_cells_ + gene_nnz_[lane.h_req[i].gene]);
+    slot_cycles_ += static_cast<uint64_t>(lane.h_res[i].cycles);
   }
   lane.pending = 0;
   return lane.h_res;
@@ -583,6 +612,8 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
     stats->requests = fitter.requests();
     stats->sweeps = fitter.sweeps();
     stats->cell_visits = fitter.cell_visits();
+    stats->fit_slots = static_cast<uint64_t>(fitter.grid());
+    stats->slot_cycles = fitter.slot_cycles();
     stats->gpu_launches = fitter.launches();
     stats->ms_prepare = ss.ms_prepare;
     stats->ms_stage_one = ss.ms_stage_one;

@@ -43,6 +43,8 @@ class DeviceFitter {
   uint64_t requests() const { return requests_; }
   uint64_t sweeps() const { return sweeps_; }
   uint64_t cell_visits() const { return cell_visits_; }
+  uint64_t slot_cycles() const { return slot_cycles_; }
+  int grid() const { return grid_; }
   uint64_t h2d_bytes() const { return h2d_bytes_; }
   uint64_t d2h_bytes() const { return d2h_bytes_; }
   void reset_counters();
@@ -75,6 +77,7 @@ class DeviceFitter {
   device::FitControl ctl_{};
   std::vector<void*> owned_;
   int grid_ = 0;
+  int max_clusters_[device::kMaxCluster + 1] = {};  // resident clusters per cluster size
   // stage-one buffers
   int32_t* h_pheader_ = nullptr;
   int32_t* d_pcounter_ = nullptr;
@@ -86,7 +89,7 @@ class DeviceFitter {
   size_t pcapacity_ = 0;
   int pgrid_ = 0;
   double device_ms_ = 0.0;
-  uint64_t launches_ = 0, requests_ = 0, sweeps_ = 0, cell_visits_ = 0;
+  uint64_t launches_ = 0, requests_ = 0, sweeps_ = 0, cell_visits_ = 0, slot_cycles_ = 0;
   uint64_t h2d_bytes_ = 0, d2h_bytes_ = 0;
 };
 

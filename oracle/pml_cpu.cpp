@@ -105,7 +105,7 @@ void fold(double* acc, const double* x, int nb, double dd, double p) {
 // at a count of zero, then a sparse part adding what the positive counts
 // change.
 void sweep(const PmlData& d, const std::vector<double>& beta, const std::vector<double>& log_w,
-           double gamma, const Penalty& pen, const std::vector<size_t>& run, Sweep& out) {
+           double gamma, const Penalty& pen, Sweep& out) {
   const int nb = d.n_beta, k = d.k, T = nb * (nb + 1) / 2, nv = 5 + 2 * nb + T;
   auto dense = [&](double* acc, size_t r, int s) {
     double eta = eta_of(d, beta, r);
@@ -128,7 +128,7 @@ void sweep(const PmlData& d, const std::vector<double>& beta, const std::vector<
     double u = e * inv;
     fold(acc, d.design + c * nb, nb, y * (1.0 - u), (y * u) * inv);
   };
-  std::vector<double> tot = tree_sums(d, run, nv, dense, sparse);
+  std::vector<double> tot = range_sums(d, nv, dense, sparse);
   std::vector<double> llv(k);
   for (int s = 0; s < k; ++s) {
     const double* S = &tot[static_cast<size_t>(s) * nv];
@@ -244,7 +244,7 @@ double determinant(std::vector<double> a, int n) {
 
 // Higher-order Laplace terms at the final iterate (pml.rs:1828-1919).
 double laplace_correction(const PmlData& d, const std::vector<double>& beta, const std::vector<double>& log_w,
-                          const std::vector<size_t>& run, const std::vector<double>& w_cur, double gamma,
+                          const std::vector<double>& w_cur, double gamma,
                           double lambda, int ord) {
   const bool high = ord > 2;
   auto terms = [&](double e, double scale, double* acc) {
@@ -262,7 +262,7 @@ double laplace_correction(const PmlData& d, const std::vector<double>& beta, con
   auto sparse = [&](double* acc, size_t i, int s) {
     terms(nebula::nb_exp_tab(eta_of(d, beta, d.cells[i]) + log_w[s], &nebula::kNbTables), d.counts[i], acc);
   };
-  std::vector<double> tot = tree_sums(d, run, 4, dense, sparse);
+  std::vector<double> tot = range_sums(d, 4, dense, sparse);
   double third_acc = 0, fourth_acc = 0, fifth_acc = 0;
   for (int s = 0; s < d.k; ++s) {
     const double* S = &tot[static_cast<size_t>(s) * 4];
@@ -358,14 +358,13 @@ bool opt_pml(const PmlData& d, const double* beta_init, const double* log_w_init
   std::vector<double> beta(beta_init, beta_init + nb);
   std::vector<double> log_w(k, 0.0);
   if (log_w_init) log_w.assign(log_w_init, log_w_init + k);
-  std::vector<size_t> run = positive_runs(d);
   Sweep cur, trial;
   cur.init(nb, k);
   trial.init(nb, k);
   std::vector<double> vw_step(k, 0), vb2(nb * nb, 0), step_beta(nb), step_log_w(k), dwvw(k);
   std::vector<double> damp_beta(nb), damp_log_w(k), new_beta(nb), new_log_w(k);
   int sweeps = 0;
-  sweep(d, beta, log_w, gamma, pen, run, cur);
+  sweep(d, beta, log_w, gamma, pen, cur);
   ++sweeps;
   double ll = cur.ll, ll_prev = 0.0, likdif = 0.0;
   int step = 0, backtracks = 0;
@@ -399,7 +398,7 @@ bool opt_pml(const PmlData& d, const double* beta_init, const double* log_w_init
     for (int j = 0; j < nb; ++j) new_beta[j] = beta[j] + step_beta[j];
     for (int s = 0; s < k; ++s) new_log_w[s] = log_w[s] + step_log_w[s];
     ll_prev = ll;
-    sweep(d, new_beta, new_log_w, gamma, pen, run, trial);
+    sweep(d, new_beta, new_log_w, gamma, pen, trial);
     ++sweeps;
     ll = trial.ll;
     likdif = ll - ll_prev;
@@ -439,7 +438,7 @@ bool opt_pml(const PmlData& d, const double* beta_init, const double* log_w_init
           new_log_w[s] = log_w[s] - min_step;
         }
       }
-      sweep(d, new_beta, new_log_w, gamma, pen, run, trial);
+      sweep(d, new_beta, new_log_w, gamma, pen, trial);
       ++sweeps;
       ll = trial.ll;
       likdif = ll - ll_prev;
@@ -453,7 +452,7 @@ bool opt_pml(const PmlData& d, const double* beta_init, const double* log_w_init
   if (params.reml) log_det += nebula::nb_log(std::fabs(determinant(vb2, nb)));
   double second = 0.0;
   if (prior == Prior::Gamma && params.ord > 1) {
-    second = laplace_correction(d, beta, log_w, run, cur.w, gamma, pen.lambda, params.ord);
+    second = laplace_correction(d, beta, log_w, cur.w, gamma, pen.lambda, params.ord);
     ++sweeps;
   }
   out->beta = beta;
@@ -477,7 +476,7 @@ double pml_objective_gradient(const PmlData& d, const double* beta, const double
   std::vector<double> b(beta, beta + nb), lw(log_w, log_w + k);
   Sweep cur;
   cur.init(nb, k);
-  sweep(d, b, lw, gamma, pen, positive_runs(d), cur);
+  sweep(d, b, lw, gamma, pen, cur);
   for (int j = 0; j < nb; ++j) gradient[j] = -cur.db[j];
   for (int s = 0; s < k; ++s) gradient[nb + s] = -cur.dw[s];
   return -cur.ll;

@@ -1,5 +1,6 @@
-// ORACLE — test infrastructure only. The summation tree the CPU oracle shares
-// with the CUDA kernels (pml_fit.cu, ptmg_eval.cu), restated on the CPU.
+// ORACLE — test infrastructure only. The summation trees the CPU oracle shares
+// with the CUDA kernels, restated on the CPU: tree_sums for stage one's cell
+// passes (ptmg_eval.cu), range_sums for the inner fit's sweep (pml_fit.cu).
 #pragma once
 
 #include <algorithm>
@@ -10,8 +11,8 @@
 
 namespace oracle {
 
-// The summation tree both this oracle and the CUDA kernel use for a sweep's
-// per-subject sums, so that the two agree bit for bit. Dense part: the cells
+// The summation tree of stage one's per-subject sums, so that the oracle and
+// the CUDA kernel agree bit for bit. Dense part: the cells
 // are cut into kWarps equal contiguous ranges; within a range each subject
 // piece is summed by kLanes strided partial sums (lane l takes cells
 // c0 + l, c0 + l + kLanes, ...), which are then combined by the butterfly
@@ -91,5 +92,61 @@ std::vector<double> tree_sums(const PmlData& d, const std::vector<size_t>& run, 
   return total;
 }
 
+// The fit kernel's tree (pml_fit.cu). The cells are cut into kRanges equal
+// contiguous ranges (range v = [N v / kRanges, N (v + 1) / kRanges)). Within a
+// range, each subject segment is summed by kLanes strided partials, first
+// over the segment's cells (dense: lane l takes cells c0 + l, c0 + l + kLanes,
+// ...) and then, continuing the same partials, over the positive entries
+// whose cells fall in the segment (sparse: lane l takes entries p0 + l,
+// p0 + l + kLanes, ...); the partials are butterflied as above into the
+// segment's piece. A subject's total is 0 + the pieces of the non-empty
+// ranges that meet it, in range order. The tree does not depend on how many
+// warps or CTAs share the ranges.
+constexpr int kRanges = 64;
+
+inline size_t range_start(const PmlData& d, int v) { return d.n_cells * static_cast<size_t>(v) / kRanges; }
+
+template <typename Dense, typename Sparse>
+std::vector<double> range_sums(const PmlData& d, int nv, Dense cell, Sparse pos) {
+  const int k = d.k;
+  std::vector<double> pieces(static_cast<size_t>(k + kRanges) * nv, 0.0);
+  Tree tree(nv);
+  auto first_entry = [&](size_t c) {
+    return static_cast<size_t>(std::lower_bound(d.cells, d.cells + d.n_pos, c,
+                                                [](uint32_t x, size_t v) { return x < v; }) -
+                               d.cells);
+  };
+  for (int v = 0; v < kRanges; ++v) {
+    const size_t a = range_start(d, v), b = range_start(d, v + 1);
+    if (a >= b) continue;
+    int s = subject_of(d, a);
+    size_t pa = first_entry(a);
+    for (size_t c0 = a; c0 < b; ++s) {
+      const size_t s_end = std::min<size_t>(b, d.subject_start[s + 1]);
+      const size_t p_end = first_entry(s_end);
+      tree.clear();
+      for (int l = 0; l < kLanes; ++l)
+        for (size_t r = c0 + l; r < s_end; r += kLanes) cell(tree.lane(l), r, s);
+      for (int l = 0; l < kLanes; ++l)
+        for (size_t i = pa + l; i < p_end; i += kLanes) pos(tree.lane(l), i, s);
+      tree.reduce(&pieces[static_cast<size_t>(s + v) * nv]);
+      pa = p_end;
+      c0 = s_end;
+    }
+  }
+  std::vector<double> total(static_cast<size_t>(k) * nv);
+  for (int s = 0; s < k; ++s) {
+    for (int x = 0; x < nv; ++x) {
+      double t = 0.0;
+      for (int v = 0; v < kRanges; ++v) {
+        const size_t a = range_start(d, v), b = range_start(d, v + 1);
+        if (a < b && a < d.subject_start[s + 1] && b > d.subject_start[s])
+          t += pieces[static_cast<size_t>(s + v) * nv + x];
+      }
+      total[static_cast<size_t>(s) * nv + x] = t;
+    }
+  }
+  return total;
+}
 
 }  // namespace oracle

@@ -101,3 +101,30 @@ def test_device_rejects_variance_outside_the_domain(synthetic):
     res = opt_pml_batch(v["design"], v["offset"], nb, v["counts"], v["cells"], v["subject_start"],
                         v["subject_total"], np.zeros(nb), [0.0, 0.2], [1.0, 0.0])
     assert [r["status"] for r in res] == [1, 1]
+
+
+@pytest.mark.parametrize("n_requests", [1, 60, 100, 200])
+def test_device_results_do_not_depend_on_the_batch(synthetic, n_requests):
+    """Batches of 1, 60, 100 and 200 requests run with 8, 4, 2 and 1 CTAs per
+    request (thread-block clusters sharing each sweep, or none); the summation
+    tree is fixed, so every copy of a point gives the same bits, equal to the
+    oracle's."""
+    work = synthetic["c1"]
+    nb = work["n_coef"]
+    v = gene_view(work, 1)
+    beta0 = np.zeros(nb)
+    beta0[0] = np.log(max(v["counts"].sum() / v["offset"].size, 1e-3))
+    pts = [POINTS[q % 4] for q in range(n_requests)]
+    dev = opt_pml_batch(v["design"], v["offset"], nb, v["counts"], v["cells"], v["subject_start"],
+                        v["subject_total"], beta0, [p[0] for p in pts], [p[1] for p in pts], ord=[p[2] for p in pts])
+    for q in range(min(n_requests, 4)):
+        s, c, o = POINTS[q]
+        ref = of.opt_pml(v["design"], v["offset"], nb, v["counts"], v["cells"], v["subject_start"],
+                         v["subject_total"], beta0, s, c, ord=o)
+        for key in ("log_likelihood", "log_det", "second_order"):
+            assert dev[q][key] == ref[key], (q, key)
+        assert np.array_equal(dev[q]["beta"], ref["beta"])
+    for q in range(4, n_requests):
+        for key in ("log_likelihood", "log_likelihood_prev", "log_det", "second_order", "iterations"):
+            assert dev[q][key] == dev[q % 4][key], (q, key)
+        assert np.array_equal(dev[q]["information"], dev[q % 4]["information"])
