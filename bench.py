@@ -58,6 +58,7 @@ def parse():
     ap.add_argument("--config", default="c1")
     ap.add_argument("--genes", type=int, default=None)
     ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--lanes", type=int, default=0, help="stage-two batches in flight (0: the library default)")
     ap.add_argument("--cpu-genes", type=int, default=32, help="gene sample of the CPU baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -180,7 +181,7 @@ def ours_arm(args, world, rank, local, dist):
     work = workloads.make(args.config, seed=1000 + rank, n_genes=args.genes)
     params = NebulaParams(method="HL")
     flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > 126 MB L2
-    session = Session(work.csr, work.subject, work.design, work.n_coef, work.offset, params)
+    session = Session(work.csr, work.subject, work.design, work.n_coef, work.offset, params, lanes=args.lanes)
     for _ in range(args.warmup):
         session.fit()
     sampler = ClockSampler(local)
@@ -224,7 +225,8 @@ def ours_arm(args, world, rank, local, dist):
             dist.barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        f2 = nebula_sparse_cuda(work.csr, work.subject, work.design, work.n_coef, work.offset, params)
+        f2 = nebula_sparse_cuda(work.csr, work.subject, work.design, work.n_coef, work.offset, params,
+                                lanes=args.lanes)
         torch.cuda.synchronize()
         el = barrier_max(dist, time.perf_counter() - t0)
         e2e_vals.append(world * len(f2.gene_index) / el)
@@ -262,7 +264,12 @@ def ours_arm(args, world, rank, local, dist):
         "cpu_baseline": cpu,
         "detail": {"rounds_per_step": stats[-1]["rounds"], "requests_per_step": stats[-1]["requests"],
                    "sweeps_per_step": stats[-1]["sweeps"], "cell_visits_per_step": stats[-1]["cell_visits"],
-                   "kernel_ms_per_step": kernel_ms / args.steps, "wall_ms_per_step": 1000.0 * t_wall / args.steps},
+                   "kernel_ms_per_step": kernel_ms / args.steps, "wall_ms_per_step": 1000.0 * t_wall / args.steps,
+                   # share of the fit CTAs' slot-time spent inside requests
+                   "slot_utilisation": stats[-1]["slot_cycles"] / (stats[-1]["fit_slots"] * stats[-1]["ms_step_device"]
+                                                                   * 1e-3 * clocks["sm_mhz"] * 1e6)
+                   if clocks.get("sm_mhz") else None,
+                   "cycles_per_visit_per_cta": stats[-1]["slot_cycles"] / stats[-1]["cell_visits"]},
     }
     print(json.dumps(line), flush=True)
 

@@ -54,7 +54,7 @@ class NbFit(ctypes.Structure):
 class NbOptions(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("warm_start", ctypes.c_int32),
                 ("host_threads", ctypes.c_int32), ("audit_percent", ctypes.c_int32),
-                ("mlp_weights", c_float_p)]
+                ("mlp_weights", c_float_p), ("lanes", ctypes.c_int32)]
 
 
 class NbStats(ctypes.Structure):

@@ -35,7 +35,7 @@ struct alignas(16) FitResult {
   double beta[kMaxCoef];
   double information[kMaxCoef * kMaxCoef];
   int32_t iterations, backtracks, sweeps, status;  // status 0 ok, 1 rejected arguments
-  int64_t cycles;  // SM clock cycles the CTA spent on the request
+  int64_t cycles;  // SM clock cycles the request held its CTAs (summed over the cluster)
   int64_t pad;
 };
 

@@ -30,6 +30,7 @@
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cfloat>
 #include <cstdint>
 
@@ -796,7 +797,7 @@ __global__ void __launch_bounds__(kThreads, (NB <= 4 ? 2 : 1)) fit_kernel(GeneDa
       out->backtracks = static_cast<int32_t>(sm.sc[kBacktracks]);
       out->sweeps = static_cast<int32_t>(sm.sc[kSweeps]);
       out->status = 0;
-      out->cycles = clock64() - t_start;
+      out->cycles = (clock64() - t_start) * cl.size;  // every CTA of the cluster was busy
     }
   }
 }
@@ -811,8 +812,20 @@ size_t smem_for(int K) {
 // static shared memory.
 template <int NB>
 cudaError_t configure_nb(size_t smem) {
-  return cudaFuncSetAttribute(fit_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              static_cast<int>(smem));
+  // the attribute only grows: the largest size set so far, per device
+  static std::atomic<int> configured[64];
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const bool cached = dev >= 0 && dev < 64;
+  if (cached && configured[dev].load() >= static_cast<int>(smem)) return cudaSuccess;
+  e = cudaFuncSetAttribute(fit_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (e == cudaSuccess && cached) {
+    int seen = configured[dev].load();
+    while (seen < static_cast<int>(smem) && !configured[dev].compare_exchange_weak(seen, static_cast<int>(smem))) {
+    }
+  }
+  return e;
 }
 
 template <int NB>

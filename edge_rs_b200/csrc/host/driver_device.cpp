@@ -78,7 +78,8 @@ T* device_copy(const T* host, size_t n, std::vector<void*>* owned) {
 // ---------------------------------------------------------------------------
 // Resident device copy of one call's inputs, and the per-round launch.
 
-DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& genes, int device) {
+DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& genes, int device, int lanes)
+    : lanes_(static_cast<size_t>(std::max(1, std::min(lanes, kMaxLanes)))) {
   const Shared& sh = prep.shared;
   if (device >= 0) cuda_check(cudaSetDevice(device), "cudaSetDevice");
   cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -341,6 +342,13 @@ const device::FitResult* DeviceFitter::collect(int lane_index) {
   return lane.h_res;
 }
 
+bool DeviceFitter::ready(int lane_index) {
+  const cudaError_t e = cudaStreamQuery(lanes_[lane_index].stream);
+  if (e == cudaErrorNotReady) return false;
+  cuda_check(e, "fit kernel");
+  return true;
+}
+
 const device::FitResult* DeviceFitter::run(const std::vector<device::FitRequest>& reqs) {
   submit(0, reqs);
   return collect(0);
@@ -393,7 +401,8 @@ std::unique_ptr<Session> create_session(const nb_csr* counts, const uint64_t* su
                [&](size_t g) { ss->genes[g] = positive_indices(ss->prep.counts, ss->prep.kept[g]); });
   ss->ms_prepare = ms_since(t0);
   auto t2 = Clock::now();
-  ss->fitter = std::make_unique<DeviceFitter>(ss->prep, ss->genes, ss->opt.device);
+  const int lanes = ss->opt.lanes > 0 ? ss->opt.lanes : DeviceFitter::kDefaultLanes;
+  ss->fitter = std::make_unique<DeviceFitter>(ss->prep, ss->genes, ss->opt.device, lanes);
   ss->ms_upload = ms_since(t2);
   // stage one (nebula.rs:812-901): every gene's projected Newton in lockstep,
   // one batched launch of marginal-likelihood cell passes per round
@@ -492,10 +501,10 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
   // while one lane's batch runs on the device the host steps another lane's
   // searches, and the lanes' kernels share the SMs. A gene's sequence of
   // evaluations does not depend on which batch carries it.
-  constexpr int L = DeviceFitter::kLanes;
-  std::vector<size_t> lane_active[L];
-  std::vector<device::FitRequest> batch[L];
-  std::vector<Slot> slots[L];
+  const int L = fitter.lanes();
+  std::vector<std::vector<size_t>> lane_active(L);
+  std::vector<std::vector<device::FitRequest>> batch(L);
+  std::vector<std::vector<Slot>> slots(L);
   for (size_t i = 0; i < active.size(); ++i) lane_active[i % L].push_back(active[i]);
   auto build = [&](int l) {
     batch[l].clear();
@@ -548,27 +557,37 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
     }
     lane_active[l].swap(still);
   };
+  // Lanes are served in the order their batches finish, so one slow batch
+  // (a search whose point needs many Newton steps) holds up no other lane.
   uint64_t rounds = 0;
-  int order[L];
-  int head = 0, count = 0;
+  std::vector<int> in_flight;
   for (int l = 0; l < L; ++l) {
     if (lane_active[l].empty()) continue;
     build(l);
     fitter.submit(l, batch[l]);
-    order[(head + count++) % L] = l;
+    in_flight.push_back(l);
   }
-  while (count > 0) {
-    const int l = order[head];
-    head = (head + 1) % L;
-    --count;
-    const device::FitResult* res = fitter.collect(l);
-    ++rounds;
-    absorb(l, res);
-    if (!lane_active[l].empty()) {
-      build(l);
-      fitter.submit(l, batch[l]);
-      order[(head + count++) % L] = l;
+  while (!in_flight.empty()) {
+    bool progressed = false;
+    for (size_t i = 0; i < in_flight.size();) {
+      const int l = in_flight[i];
+      if (!fitter.ready(l)) {
+        ++i;
+        continue;
+      }
+      progressed = true;
+      const device::FitResult* res = fitter.collect(l);
+      ++rounds;
+      absorb(l, res);
+      if (!lane_active[l].empty()) {
+        build(l);
+        fitter.submit(l, batch[l]);
+        ++i;
+      } else {
+        in_flight.erase(in_flight.begin() + static_cast<std::ptrdiff_t>(i));
+      }
     }
+    if (!progressed) std::this_thread::yield();
   }
   const double ms_stage_two = ms_since(t2);
 

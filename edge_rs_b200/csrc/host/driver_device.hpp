@@ -20,9 +20,10 @@ namespace nebula {
 // leaves idle) while the host prepares the next batch of another lane.
 class DeviceFitter {
  public:
-  static constexpr int kLanes = 4;
+  static constexpr int kDefaultLanes = 8;
+  static constexpr int kMaxLanes = 64;
 
-  DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& genes, int device);
+  DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& genes, int device, int lanes = 1);
   ~DeviceFitter();
   DeviceFitter(const DeviceFitter&) = delete;
   DeviceFitter& operator=(const DeviceFitter&) = delete;
@@ -34,6 +35,8 @@ class DeviceFitter {
   // and returns its results, valid until the lane's next submit().
   void submit(int lane, const std::vector<device::FitRequest>& reqs);
   const device::FitResult* collect(int lane);
+  // True once the lane's batch has finished (collect() will not wait).
+  bool ready(int lane);
   // One batch of stage-one evaluations: per request (2 + W) * K doubles,
   // valid until the next call.
   const double* run_ptmg(const std::vector<device::PtmgRequest>& reqs);
@@ -45,6 +48,7 @@ class DeviceFitter {
   uint64_t cell_visits() const { return cell_visits_; }
   uint64_t slot_cycles() const { return slot_cycles_; }
   int grid() const { return grid_; }
+  int lanes() const { return static_cast<int>(lanes_.size()); }
   uint64_t h2d_bytes() const { return h2d_bytes_; }
   uint64_t d2h_bytes() const { return d2h_bytes_; }
   void reset_counters();
@@ -70,7 +74,7 @@ class DeviceFitter {
   void reserve(Lane& lane, size_t n);
   cudaStream_t stream_ = nullptr;
   cudaEvent_t step0_ = nullptr, step1_ = nullptr;
-  Lane lanes_[kLanes];
+  std::vector<Lane> lanes_;
   std::vector<uint64_t> gene_nnz_;
   size_t n_cells_ = 0;
   device::GeneData data_{};
