@@ -75,6 +75,33 @@ int launch_fit(const GeneData& data, const FitControl& ctl, const FitRequest* re
                FitResult* results, const int32_t* n_requests, int32_t* counter, int grid,
                int cluster, void* stream);
 
+// Streaming mode: one persistent launch serves requests the host posts while
+// it runs. Ticket t's request is ring[t & mask] in device memory; the host
+// copies it there and then, by a later copy on the same stream, seq[t & mask]
+// = t. A cluster takes the next ticket off `taken`, polls seq[t & mask]
+// (backing off, at most idle_ns by the global timer), runs the fit, writes
+// the result into results[t & mask] (host memory mapped into the device's
+// address space) and then done[t & mask] = t + 1. *stop != 0 tells clusters
+// waiting on a ticket nobody will post to exit; a wait that runs out sets
+// *status = 1 and exits too. Nothing else waits.
+struct FitQueue {
+  const FitRequest* ring;
+  const long long* seq;
+  const int* stop;
+  unsigned long long* taken;
+  FitResult* results;
+  long long* done;
+  int* status;
+  long long mask;
+  long long idle_ns;
+};
+
+int launch_fit_queue(const GeneData& data, const FitControl& ctl, const FitQueue& queue, int grid, int cluster,
+                     void* stream);
+
+// Clusters of `cluster` CTAs the streaming kernel can keep resident at once.
+int fit_queue_max_clusters(int n_subjects, int n_coef, int cluster);
+
 // CTAs per SM the fit kernel can keep resident for this shape.
 int fit_blocks_per_sm(int n_subjects, int n_coef);
 

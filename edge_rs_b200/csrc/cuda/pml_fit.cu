@@ -529,16 +529,236 @@ __device__ double determinant(double* a) {
   return det;
 }
 
+// One inner fit (optimise, pml.rs:1614-1800) by the calling cluster: every
+// CTA of the cluster runs it in step (each sweep shared over the cluster's
+// CTAs) and rank 0 writes the result to `out`.
 template <int NB>
-__global__ void __launch_bounds__(kThreads, (NB <= 4 ? 2 : 1)) fit_kernel(GeneData d, FitControl ctl,
-                                                       const FitRequest* __restrict__ requests,
-                                                       FitResult* __restrict__ results,
-                                                       const int32_t* __restrict__ n_requests,
-                                                       int32_t* __restrict__ counter) {
-  extern __shared__ __align__(16) double smem_raw[];
-  Smem<NB> sm;
-  const int K = d.n_subjects;
-  sm.carve(smem_raw, K);
+__device__ void fit_one(const GeneData& d, const FitControl& ctl, Smem<NB>& sm, const FitRequest& req,
+                        FitResult* out, const Cluster& cl, int& parity, long long t_start) {
+  const int K = sm.K;
+  const int tid = threadIdx.x;
+  const int gene = req.gene;
+
+  // gamma_penalty (pml.rs:432-441) and the argument checks of optimise
+  const double exps = nb_exp(req.subject);
+  const bool bad = !(isfinite(exps) && exps > 1.0) || !(isfinite(req.cell) && req.cell > 0.0);
+  if (bad) {
+    if (tid == 0 && cl.rank == 0) {
+      out->status = 1;
+      out->iterations = 0;
+      out->sweeps = 0;
+      out->cycles = 0;
+    }
+    return;
+  }
+  if (tid == 0) {
+    sm.sc[kAlpha] = 1.0 / (exps - 1.0);
+    sm.sc[kLambda] = 1.0 / (sqrt(exps) * (exps - 1.0));
+    sm.sc[kGamma] = req.cell;
+    sm.sc[kSweeps] = 0.0;
+  }
+  if (tid < NB) sm.beta[tid] = req.beta[tid];
+  for (int s = tid; s < K; s += blockDim.x) sm.log_w[s] = 0.0;
+  for (int i = tid; i <= kRanges; i += blockDim.x)
+    sm.rpos[i] = d.range_pos[static_cast<size_t>(gene) * (kRanges + 1) + i];
+  for (int i = tid; i <= K; i += blockDim.x) sm.runs[i] = d.runs[static_cast<size_t>(gene) * (K + 1) + i];
+  __syncthreads();
+
+  int cur = 0;  // index of the current sweep buffer (every thread tracks it identically)
+  sweep<NB>(d, sm, gene, sm.beta, sm.log_w, SweepView<NB>(sm.sw[cur], K), parity, cl);
+  if (tid == 0) {
+    sm.sc[kLl] = *SweepView<NB>(sm.sw[cur], K).ll;
+    sm.sc[kLlPrev] = 0.0;
+    sm.sc[kLikdif] = 0.0;
+    sm.sc[kStep] = 0.0;
+    sm.sc[kBacktracks] = 0.0;
+  }
+  __syncthreads();
+
+  for (;;) {
+    const double step = sm.sc[kStep];
+    const bool go = step == 0.0 || (sm.sc[kLikdif] > ctl.eps && step < static_cast<double>(ctl.max_iter));
+    __syncthreads();
+    if (!go) break;
+    SweepView<NB> c(sm.sw[cur], K);
+    SweepView<NB> tr(sm.sw[cur ^ 1], K);
+    if (tid == 0) sm.sc[kStep] = step + 1.0;
+    // Schur complement of the random-effect block and the step (pml.rs:1660-1710)
+    for (int s = tid; s < K; s += blockDim.x) {
+      sm.vw_step[s] = c.vw[s];
+      sm.dwvw[s] = c.dw[s] / c.vw[s];
+      sm.damp_log_w[s] = 1.0;
+    }
+    if (tid < NB) sm.damp_beta[tid] = 1.0;
+    __syncthreads();
+    if (tid < Dims<NB>::T) {
+      int a = 0, rem = tid;
+      while (rem >= NB - a) {
+        rem -= NB - a;
+        ++a;
+      }
+      const int b = a + rem;
+      double acc = 0.0;
+      for (int s = 0; s < K; ++s) acc += c.vwb[s * NB + a] * c.vwb[s * NB + b] / c.vw[s];
+      const double v = c.vb[a * NB + b] - acc;
+      sm.vb2[a * NB + b] = v;
+      sm.vb2[b * NB + a] = v;
+      sm.factor[a * NB + b] = v;
+      sm.factor[b * NB + a] = v;
+    } else if (tid >= 64 && tid < 64 + NB) {
+      const int j = tid - 64;
+      double acc = 0.0;
+      for (int s = 0; s < K; ++s) acc += c.vwb[s * NB + j] * sm.dwvw[s];
+      sm.step_beta[j] = c.db[j] - acc;
+    }
+    __syncthreads();
+    if (tid == 0) ldlt_solve<NB>(sm.factor, sm.step_beta);
+    __syncthreads();
+    for (int s = tid; s < K; s += blockDim.x) {
+      double acc = 0.0;
+#pragma unroll
+      for (int j = 0; j < NB; ++j) acc += c.vwb[s * NB + j] * sm.step_beta[j];
+      sm.step_log_w[s] = sm.dwvw[s] - acc / c.vw[s];
+      sm.new_log_w[s] = sm.log_w[s] + sm.step_log_w[s];
+    }
+    if (tid < NB) sm.new_beta[tid] = sm.beta[tid] + sm.step_beta[tid];
+    if (tid == 0) sm.sc[kLlPrev] = sm.sc[kLl];
+    __syncthreads();
+    sweep<NB>(d, sm, gene, sm.new_beta, sm.new_log_w, tr, parity, cl);
+    if (tid == 0) {
+      sm.sc[kLl] = *tr.ll;
+      sm.sc[kLikdif] = sm.sc[kLl] - sm.sc[kLlPrev];
+      sm.sc[kBacktracks] = 0.0;
+      sm.sc[kMinStep] = kStepCutoff;
+      sm.sc[kStop] = 0.0;
+    }
+    __syncthreads();
+    // backtracking (pml.rs:1716-1760)
+    for (;;) {
+      const double ll = sm.sc[kLl];
+      const bool again = sm.sc[kLikdif] < 0.0 || isinf(ll);
+      __syncthreads();
+      if (!again) break;
+      if (tid == 0) {
+        const double bt = sm.sc[kBacktracks] + 1.0;
+        sm.sc[kBacktracks] = bt;
+        sm.sc[kMinStep] = sm.sc[kMinStep] / 2.0;
+        if (bt > static_cast<double>(ctl.max_backtrack)) {
+          sm.sc[kLikdif] = 0.0;
+          sm.sc[kLl] = sm.sc[kLlPrev];
+          double gb = 0.0, gw = 0.0;
+          for (int j = 0; j < NB; ++j) gb = fmax(gb, fabs(c.db[j]));
+          for (int s = 0; s < K; ++s) gw = fmax(gw, fabs(c.dw[s]));
+          if (gb > kGradientTolerance || gw > kGradientTolerance) sm.sc[kBacktracks] = bt + 1.0;
+          sm.sc[kStop] = 1.0;
+        }
+      }
+      __syncthreads();
+      if (sm.sc[kStop] != 0.0) break;
+      const double min_step = sm.sc[kMinStep];
+      if (tid < NB) {
+        const double dd = sm.step_beta[tid];
+        if (dd < kStepCutoff && dd > -kStepCutoff) {
+          sm.damp_beta[tid] /= 2.0;
+          sm.new_beta[tid] = sm.beta[tid] + dd * sm.damp_beta[tid];
+        } else if (dd > 0.0) {
+          sm.new_beta[tid] = sm.beta[tid] + min_step;
+        } else {
+          sm.new_beta[tid] = sm.beta[tid] - min_step;
+        }
+      }
+      for (int s = tid; s < K; s += blockDim.x) {
+        const double dd = sm.step_log_w[s];
+        if (dd < kStepCutoff && dd > -kStepCutoff) {
+          sm.damp_log_w[s] /= 2.0;
+          sm.new_log_w[s] = sm.log_w[s] + dd * sm.damp_log_w[s];
+        } else if (dd > 0.0) {
+          sm.new_log_w[s] = sm.log_w[s] + min_step;
+        } else {
+          sm.new_log_w[s] = sm.log_w[s] - min_step;
+        }
+      }
+      __syncthreads();
+      sweep<NB>(d, sm, gene, sm.new_beta, sm.new_log_w, tr, parity, cl);
+      if (tid == 0) {
+        sm.sc[kLl] = *tr.ll;
+        sm.sc[kLikdif] = sm.sc[kLl] - sm.sc[kLlPrev];
+      }
+      __syncthreads();
+    }
+    // accept the trial point as the new iterate
+    if (tid < NB) sm.beta[tid] = sm.new_beta[tid];
+    for (int s = tid; s < K; s += blockDim.x) sm.log_w[s] = sm.new_log_w[s];
+    cur ^= 1;
+    __syncthreads();
+  }
+
+  // log-determinant from the previous iterate's vw (pml.rs:1767-1777)
+  if (tid == 0) {
+    double log_det = 0.0;
+    for (int s = 0; s < K; ++s) log_det += nb_log(fabs(sm.vw_step[s]));
+    if (req.reml) {
+      for (int i = 0; i < NB * NB; ++i) sm.factor[i] = sm.vb2[i];
+      log_det += nb_log(fabs(determinant<NB>(sm.factor)));
+    }
+    sm.sc[kLogDet] = log_det;
+    sm.sc[kSecond] = 0.0;
+  }
+  __syncthreads();
+  // higher-order Laplace correction at the final iterate (pml.rs:1828-1919)
+  if (req.ord > 1) {
+    SweepView<NB> c(sm.sw[cur], K);
+    sweep_sums<NB, 1>(d, sm, sm.beta, sm.log_w, sm.sc[kGamma], parity, cl);
+    parity ^= 1;
+    if (tid == 0) {
+      const double gamma = sm.sc[kGamma], lambda = sm.sc[kLambda];
+      const bool high = req.ord > 2;
+      double third_acc = 0.0, fourth_acc = 0.0, fifth_acc = 0.0;
+      for (int s = 0; s < K; ++s) {
+        const double* S = sm.totals + s * Dims<NB>::NS;
+        const double prior = lambda * c.w[s];
+        const double vw = gamma * S[0] + prior;
+        const double third = gamma * S[1] + prior;
+        third_acc += third * third / (vw * vw * vw);
+        if (high) {
+          const double fourth = gamma * S[2] + prior;
+          const double fifth = gamma * S[3] + prior;
+          const double vs = vw * vw;
+          fourth_acc += fourth / vs;
+          fifth_acc += fifth * third / (vs * vs);
+        }
+      }
+      double second = 5.0 * third_acc / 24.0;
+      if (high) {
+        second -= fourth_acc / 8.0;
+        second += 7.0 * fifth_acc / 48.0;
+      }
+      sm.sc[kSecond] = second;
+      sm.sc[kSweeps] += 1.0;
+    }
+    __syncthreads();
+  }
+  if (cl.rank != 0) return;  // rank 0 of the cluster writes the result
+  if (tid < NB) out->beta[tid] = sm.beta[tid];
+  for (int i = tid; i < NB * NB; i += blockDim.x) out->information[i] = sm.vb2[i];
+  if (tid == 0) {
+    out->log_likelihood = sm.sc[kLl];
+    out->log_likelihood_prev = sm.sc[kLlPrev];
+    out->log_det = sm.sc[kLogDet];
+    out->second_order = sm.sc[kSecond];
+    out->iterations = static_cast<int32_t>(sm.sc[kStep]);
+    out->backtracks = static_cast<int32_t>(sm.sc[kBacktracks]);
+    out->sweeps = static_cast<int32_t>(sm.sc[kSweeps]);
+    out->status = 0;
+    out->cycles = (clock64() - t_start) * cl.size;  // every CTA of the cluster was busy
+  }
+}
+
+// Per-CTA set-up shared by both kernels: tables, subject boundaries, the
+// cell ranges and the ranges meeting each subject, the cluster coordinates.
+template <int NB>
+__device__ Cluster setup_cta(const GeneData& d, Smem<NB>& sm) {
+  const int K = sm.K;
   const int tid = threadIdx.x;
   nb_load_tables(sm.tab);
   for (int i = tid; i <= K; i += blockDim.x) sm.fid[i] = d.fid[i];
@@ -555,11 +775,25 @@ __global__ void __launch_bounds__(kThreads, (NB <= 4 ? 2 : 1)) fit_kernel(GeneDa
     sm.vhi[s] = hi;
   }
   Cluster cl;
-  {
-    cg::cluster_group cluster = cg::this_cluster();
-    cl.rank = static_cast<int>(cluster.block_rank());
-    cl.size = static_cast<int>(cluster.num_blocks());
-  }
+  cg::cluster_group cluster = cg::this_cluster();
+  cl.rank = static_cast<int>(cluster.block_rank());
+  cl.size = static_cast<int>(cluster.num_blocks());
+  return cl;
+}
+
+// Batch mode: *n_requests requests in device memory, taken off an atomic
+// counter one per cluster.
+template <int NB>
+__global__ void __launch_bounds__(kThreads, (NB <= 4 ? 2 : 1)) fit_kernel(GeneData d, FitControl ctl,
+                                                       const FitRequest* __restrict__ requests,
+                                                       FitResult* __restrict__ results,
+                                                       const int32_t* __restrict__ n_requests,
+                                                       int32_t* __restrict__ counter) {
+  extern __shared__ __align__(16) double smem_raw[];
+  Smem<NB> sm;
+  sm.carve(smem_raw, d.n_subjects);
+  const Cluster cl = setup_cta<NB>(d, sm);
+  const int tid = threadIdx.x;
   __shared__ int next_req;
   const int total = *n_requests;
   int parity = 0;  // sweep parity of the pieces buffers, identical in every thread of the cluster
@@ -582,222 +816,75 @@ __global__ void __launch_bounds__(kThreads, (NB <= 4 ? 2 : 1)) fit_kernel(GeneDa
     const int q = next_req;
     if (q >= total) break;
     const FitRequest req = requests[q];
-    const long long t_start = clock64();
-    const int gene = req.gene;
-    FitResult* out = results + q;
+    fit_one<NB>(d, ctl, sm, req, results + q, cl, parity, clock64());
+  }
+}
 
-    // gamma_penalty (pml.rs:432-441) and the argument checks of optimise
-    const double exps = nb_exp(req.subject);
-    const bool bad = !(isfinite(exps) && exps > 1.0) || !(isfinite(req.cell) && req.cell > 0.0);
-    if (bad) {
-      if (tid == 0 && cl.rank == 0) {
-        out->status = 1;
-        out->iterations = 0;
-        out->sweeps = 0;
-        out->cycles = 0;
-      }
-      continue;
-    }
-    if (tid == 0) {
-      sm.sc[kAlpha] = 1.0 / (exps - 1.0);
-      sm.sc[kLambda] = 1.0 / (sqrt(exps) * (exps - 1.0));
-      sm.sc[kGamma] = req.cell;
-      sm.sc[kSweeps] = 0.0;
-    }
-    if (tid < NB) sm.beta[tid] = req.beta[tid];
-    for (int s = tid; s < K; s += blockDim.x) sm.log_w[s] = 0.0;
-    for (int i = tid; i <= kRanges; i += blockDim.x)
-      sm.rpos[i] = d.range_pos[static_cast<size_t>(gene) * (kRanges + 1) + i];
-    for (int i = tid; i <= K; i += blockDim.x) sm.runs[i] = d.runs[static_cast<size_t>(gene) * (K + 1) + i];
-    __syncthreads();
+__device__ __forceinline__ long long global_ns() {
+  long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
-    int cur = 0;  // index of the current sweep buffer (every thread tracks it identically)
-    sweep<NB>(d, sm, gene, sm.beta, sm.log_w, SweepView<NB>(sm.sw[cur], K), parity, cl);
-    if (tid == 0) {
-      sm.sc[kLl] = *SweepView<NB>(sm.sw[cur], K).ll;
-      sm.sc[kLlPrev] = 0.0;
-      sm.sc[kLikdif] = 0.0;
-      sm.sc[kStep] = 0.0;
-      sm.sc[kBacktracks] = 0.0;
-    }
-    __syncthreads();
+// Streaming mode (FitQueue): one persistent launch for a whole stage.
+template <int NB>
+__global__ void __launch_bounds__(kThreads, (NB <= 4 ? 2 : 1)) fit_queue_kernel(GeneData d, FitControl ctl,
+                                                             FitQueue qu) {
+  extern __shared__ __align__(16) double smem_raw[];
+  Smem<NB> sm;
+  sm.carve(smem_raw, d.n_subjects);
+  const Cluster cl = setup_cta<NB>(d, sm);
+  const int tid = threadIdx.x;
+  __shared__ long long next_ticket;  // the ticket to run, or -1 to exit
+  int parity = 0;
 
-    for (;;) {
-      const double step = sm.sc[kStep];
-      const bool go = step == 0.0 || (sm.sc[kLikdif] > ctl.eps && step < static_cast<double>(ctl.max_iter));
-      __syncthreads();
-      if (!go) break;
-      SweepView<NB> c(sm.sw[cur], K);
-      SweepView<NB> tr(sm.sw[cur ^ 1], K);
-      if (tid == 0) sm.sc[kStep] = step + 1.0;
-      // Schur complement of the random-effect block and the step (pml.rs:1660-1710)
-      for (int s = tid; s < K; s += blockDim.x) {
-        sm.vw_step[s] = c.vw[s];
-        sm.dwvw[s] = c.dw[s] / c.vw[s];
-        sm.damp_log_w[s] = 1.0;
-      }
-      if (tid < NB) sm.damp_beta[tid] = 1.0;
-      __syncthreads();
-      if (tid < Dims<NB>::T) {
-        int a = 0, rem = tid;
-        while (rem >= NB - a) {
-          rem -= NB - a;
-          ++a;
-        }
-        const int b = a + rem;
-        double acc = 0.0;
-        for (int s = 0; s < K; ++s) acc += c.vwb[s * NB + a] * c.vwb[s * NB + b] / c.vw[s];
-        const double v = c.vb[a * NB + b] - acc;
-        sm.vb2[a * NB + b] = v;
-        sm.vb2[b * NB + a] = v;
-        sm.factor[a * NB + b] = v;
-        sm.factor[b * NB + a] = v;
-      } else if (tid >= 64 && tid < 64 + NB) {
-        const int j = tid - 64;
-        double acc = 0.0;
-        for (int s = 0; s < K; ++s) acc += c.vwb[s * NB + j] * sm.dwvw[s];
-        sm.step_beta[j] = c.db[j] - acc;
-      }
-      __syncthreads();
-      if (tid == 0) ldlt_solve<NB>(sm.factor, sm.step_beta);
-      __syncthreads();
-      for (int s = tid; s < K; s += blockDim.x) {
-        double acc = 0.0;
-#pragma unroll
-        for (int j = 0; j < NB; ++j) acc += c.vwb[s * NB + j] * sm.step_beta[j];
-        sm.step_log_w[s] = sm.dwvw[s] - acc / c.vw[s];
-        sm.new_log_w[s] = sm.log_w[s] + sm.step_log_w[s];
-      }
-      if (tid < NB) sm.new_beta[tid] = sm.beta[tid] + sm.step_beta[tid];
-      if (tid == 0) sm.sc[kLlPrev] = sm.sc[kLl];
-      __syncthreads();
-      sweep<NB>(d, sm, gene, sm.new_beta, sm.new_log_w, tr, parity, cl);
-      if (tid == 0) {
-        sm.sc[kLl] = *tr.ll;
-        sm.sc[kLikdif] = sm.sc[kLl] - sm.sc[kLlPrev];
-        sm.sc[kBacktracks] = 0.0;
-        sm.sc[kMinStep] = kStepCutoff;
-        sm.sc[kStop] = 0.0;
-      }
-      __syncthreads();
-      // backtracking (pml.rs:1716-1760)
+  for (;;) {
+    cluster_barrier(cl);
+    if (cl.rank == 0 && tid == 0) {
+      const long long t = static_cast<long long>(atomicAdd(qu.taken, 1ull));
+      const volatile long long* seq = qu.seq + (t & qu.mask);
+      const volatile int* stop = qu.stop;
+      const long long t0 = global_ns();
+      unsigned int pause = 128;
+      long long got = -1;
       for (;;) {
-        const double ll = sm.sc[kLl];
-        const bool again = sm.sc[kLikdif] < 0.0 || isinf(ll);
-        __syncthreads();
-        if (!again) break;
-        if (tid == 0) {
-          const double bt = sm.sc[kBacktracks] + 1.0;
-          sm.sc[kBacktracks] = bt;
-          sm.sc[kMinStep] = sm.sc[kMinStep] / 2.0;
-          if (bt > static_cast<double>(ctl.max_backtrack)) {
-            sm.sc[kLikdif] = 0.0;
-            sm.sc[kLl] = sm.sc[kLlPrev];
-            double gb = 0.0, gw = 0.0;
-            for (int j = 0; j < NB; ++j) gb = fmax(gb, fabs(c.db[j]));
-            for (int s = 0; s < K; ++s) gw = fmax(gw, fabs(c.dw[s]));
-            if (gb > kGradientTolerance || gw > kGradientTolerance) sm.sc[kBacktracks] = bt + 1.0;
-            sm.sc[kStop] = 1.0;
-          }
+        if (*seq == t) {
+          got = t;
+          break;
         }
-        __syncthreads();
-        if (sm.sc[kStop] != 0.0) break;
-        const double min_step = sm.sc[kMinStep];
-        if (tid < NB) {
-          const double dd = sm.step_beta[tid];
-          if (dd < kStepCutoff && dd > -kStepCutoff) {
-            sm.damp_beta[tid] /= 2.0;
-            sm.new_beta[tid] = sm.beta[tid] + dd * sm.damp_beta[tid];
-          } else if (dd > 0.0) {
-            sm.new_beta[tid] = sm.beta[tid] + min_step;
-          } else {
-            sm.new_beta[tid] = sm.beta[tid] - min_step;
-          }
+        if (*stop != 0) break;
+        if (global_ns() - t0 > qu.idle_ns) {
+          atomicExch(qu.status, 1);
+          break;
         }
-        for (int s = tid; s < K; s += blockDim.x) {
-          const double dd = sm.step_log_w[s];
-          if (dd < kStepCutoff && dd > -kStepCutoff) {
-            sm.damp_log_w[s] /= 2.0;
-            sm.new_log_w[s] = sm.log_w[s] + dd * sm.damp_log_w[s];
-          } else if (dd > 0.0) {
-            sm.new_log_w[s] = sm.log_w[s] + min_step;
-          } else {
-            sm.new_log_w[s] = sm.log_w[s] - min_step;
-          }
-        }
-        __syncthreads();
-        sweep<NB>(d, sm, gene, sm.new_beta, sm.new_log_w, tr, parity, cl);
-        if (tid == 0) {
-          sm.sc[kLl] = *tr.ll;
-          sm.sc[kLikdif] = sm.sc[kLl] - sm.sc[kLlPrev];
-        }
-        __syncthreads();
+        __nanosleep(pause);
+        if (pause < 2048) pause *= 2;
       }
-      // accept the trial point as the new iterate
-      if (tid < NB) sm.beta[tid] = sm.new_beta[tid];
-      for (int s = tid; s < K; s += blockDim.x) sm.log_w[s] = sm.new_log_w[s];
-      cur ^= 1;
+      if (cl.size == 1) {
+        next_ticket = got;
+      } else {
+        cg::cluster_group cluster = cg::this_cluster();
+        for (int r = 0; r < cl.size; ++r) *cluster.map_shared_rank(&next_ticket, r) = got;
+      }
+    }
+    cluster_barrier(cl);
+    const long long t = next_ticket;
+    if (t < 0) break;
+    // the request, read past L1: the host's copy landed in L2 before the
+    // sequence number this cluster saw
+    FitRequest req;
+    {
+      const int4* src = reinterpret_cast<const int4*>(qu.ring + (t & qu.mask));
+      int4* dst = reinterpret_cast<int4*>(&req);
+#pragma unroll
+      for (int i = 0; i < static_cast<int>(sizeof(FitRequest) / 16); ++i) dst[i] = __ldcg(src + i);
+    }
+    fit_one<NB>(d, ctl, sm, req, qu.results + (t & qu.mask), cl, parity, clock64());
+    if (cl.rank == 0) {
+      // every thread's result writes reach host memory before the flag
+      __threadfence_system();
       __syncthreads();
-    }
-
-    // log-determinant from the previous iterate's vw (pml.rs:1767-1777)
-    if (tid == 0) {
-      double log_det = 0.0;
-      for (int s = 0; s < K; ++s) log_det += nb_log(fabs(sm.vw_step[s]));
-      if (req.reml) {
-        for (int i = 0; i < NB * NB; ++i) sm.factor[i] = sm.vb2[i];
-        log_det += nb_log(fabs(determinant<NB>(sm.factor)));
-      }
-      sm.sc[kLogDet] = log_det;
-      sm.sc[kSecond] = 0.0;
-    }
-    __syncthreads();
-    // higher-order Laplace correction at the final iterate (pml.rs:1828-1919)
-    if (req.ord > 1) {
-      SweepView<NB> c(sm.sw[cur], K);
-      sweep_sums<NB, 1>(d, sm, sm.beta, sm.log_w, sm.sc[kGamma], parity, cl);
-      parity ^= 1;
-      if (tid == 0) {
-        const double gamma = sm.sc[kGamma], lambda = sm.sc[kLambda];
-        const bool high = req.ord > 2;
-        double third_acc = 0.0, fourth_acc = 0.0, fifth_acc = 0.0;
-        for (int s = 0; s < K; ++s) {
-          const double* S = sm.totals + s * Dims<NB>::NS;
-          const double prior = lambda * c.w[s];
-          const double vw = gamma * S[0] + prior;
-          const double third = gamma * S[1] + prior;
-          third_acc += third * third / (vw * vw * vw);
-          if (high) {
-            const double fourth = gamma * S[2] + prior;
-            const double fifth = gamma * S[3] + prior;
-            const double vs = vw * vw;
-            fourth_acc += fourth / vs;
-            fifth_acc += fifth * third / (vs * vs);
-          }
-        }
-        double second = 5.0 * third_acc / 24.0;
-        if (high) {
-          second -= fourth_acc / 8.0;
-          second += 7.0 * fifth_acc / 48.0;
-        }
-        sm.sc[kSecond] = second;
-        sm.sc[kSweeps] += 1.0;
-      }
-      __syncthreads();
-    }
-    if (cl.rank != 0) continue;  // rank 0 of the cluster writes the result
-    if (tid < NB) out->beta[tid] = sm.beta[tid];
-    for (int i = tid; i < NB * NB; i += blockDim.x) out->information[i] = sm.vb2[i];
-    if (tid == 0) {
-      out->log_likelihood = sm.sc[kLl];
-      out->log_likelihood_prev = sm.sc[kLlPrev];
-      out->log_det = sm.sc[kLogDet];
-      out->second_order = sm.sc[kSecond];
-      out->iterations = static_cast<int32_t>(sm.sc[kStep]);
-      out->backtracks = static_cast<int32_t>(sm.sc[kBacktracks]);
-      out->sweeps = static_cast<int32_t>(sm.sc[kSweeps]);
-      out->status = 0;
-      out->cycles = (clock64() - t_start) * cl.size;  // every CTA of the cluster was busy
+      if (tid == 0) reinterpret_cast<volatile long long*>(qu.done)[t & qu.mask] = t + 1;
     }
   }
 }
@@ -810,6 +897,29 @@ size_t smem_for(int K) {
 // Opts the kernel into the dynamic shared memory one CTA needs; the
 // attribute may not exceed the per-block opt-in limit less the kernel's
 // static shared memory.
+template <int NB>
+cudaError_t configure_kernel(const void* kernel, size_t smem, std::atomic<int>* configured) {
+  // the attribute only grows: the largest size set so far, per device
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const bool cached = dev >= 0 && dev < 64;
+  if (cached && configured[dev].load() >= static_cast<int>(smem)) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (e == cudaSuccess && cached) {
+    int seen = configured[dev].load();
+    while (seen < static_cast<int>(smem) && !configured[dev].compare_exchange_weak(seen, static_cast<int>(smem))) {
+    }
+  }
+  return e;
+}
+
+template <int NB>
+cudaError_t configure_queue_nb(size_t smem) {
+  static std::atomic<int> configured[64];
+  return configure_kernel<NB>(reinterpret_cast<const void*>(fit_queue_kernel<NB>), smem, configured);
+}
+
 template <int NB>
 cudaError_t configure_nb(size_t smem) {
   // the attribute only grows: the largest size set so far, per device
@@ -852,6 +962,29 @@ int launch_nb(const GeneData& d, const FitControl& ctl, const FitRequest* req, F
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   return cudaLaunchKernelEx(&cfg, fit_kernel<NB>, d, ctl, req, res, n_req, counter);
+}
+
+template <int NB>
+int launch_queue_nb(const GeneData& d, const FitControl& ctl, const FitQueue& qu, int grid, int cluster,
+                    cudaStream_t stream) {
+  const size_t smem = Smem<NB>::bytes(d.n_subjects);
+  cudaError_t e = configure_queue_nb<NB>(smem);
+  if (e != cudaSuccess) return e;
+  if (cluster < 1 || cluster > kMaxCluster || (cluster & (cluster - 1)) != 0 || grid % cluster != 0)
+    return cudaErrorInvalidValue;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid, 1, 1);
+  cfg.blockDim = dim3(kThreads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, fit_queue_kernel<NB>, d, ctl, qu);
 }
 
 template <int NB>
@@ -914,6 +1047,40 @@ int fit_blocks_per_sm(int n_subjects, int n_coef) {
   }
 }
 
+template <int NB>
+int queue_clusters_nb(int K, int cluster) {
+  const size_t smem = Smem<NB>::bytes(K);
+  if (configure_queue_nb<NB>(smem) != cudaSuccess) return 0;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(cluster, 1, 1);
+  cfg.blockDim = dim3(kThreads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, fit_queue_kernel<NB>, &cfg) != cudaSuccess) return 0;
+  return n;
+}
+
+int fit_queue_max_clusters(int n_subjects, int n_coef, int cluster) {
+  switch (n_coef) {
+    case 1: return queue_clusters_nb<1>(n_subjects, cluster);
+    case 2: return queue_clusters_nb<2>(n_subjects, cluster);
+    case 3: return queue_clusters_nb<3>(n_subjects, cluster);
+    case 4: return queue_clusters_nb<4>(n_subjects, cluster);
+    case 5: return queue_clusters_nb<5>(n_subjects, cluster);
+    case 6: return queue_clusters_nb<6>(n_subjects, cluster);
+    case 7: return queue_clusters_nb<7>(n_subjects, cluster);
+    case 8: return queue_clusters_nb<8>(n_subjects, cluster);
+    default: return 0;
+  }
+}
+
 int fit_max_clusters(int n_subjects, int n_coef, int cluster) {
   switch (n_coef) {
     case 1: return clusters_nb<1>(n_subjects, cluster);
@@ -925,6 +1092,22 @@ int fit_max_clusters(int n_subjects, int n_coef, int cluster) {
     case 7: return clusters_nb<7>(n_subjects, cluster);
     case 8: return clusters_nb<8>(n_subjects, cluster);
     default: return 0;
+  }
+}
+
+int launch_fit_queue(const GeneData& d, const FitControl& ctl, const FitQueue& qu, int grid, int cluster,
+                     void* stream) {
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  switch (d.n_coef) {
+    case 1: return launch_queue_nb<1>(d, ctl, qu, grid, cluster, s);
+    case 2: return launch_queue_nb<2>(d, ctl, qu, grid, cluster, s);
+    case 3: return launch_queue_nb<3>(d, ctl, qu, grid, cluster, s);
+    case 4: return launch_queue_nb<4>(d, ctl, qu, grid, cluster, s);
+    case 5: return launch_queue_nb<5>(d, ctl, qu, grid, cluster, s);
+    case 6: return launch_queue_nb<6>(d, ctl, qu, grid, cluster, s);
+    case 7: return launch_queue_nb<7>(d, ctl, qu, grid, cluster, s);
+    case 8: return launch_queue_nb<8>(d, ctl, qu, grid, cluster, s);
+    default: return cudaErrorInvalidValue;
   }
 }
 

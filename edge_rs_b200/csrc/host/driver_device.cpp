@@ -157,6 +157,8 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
   grid_ = per_sm * sms;
   for (int c = 2; c <= device::kMaxCluster; c *= 2)
     max_clusters_[c] = device::fit_max_clusters(K, sh.n_coef, c);
+  for (int c = 1; c <= device::kMaxCluster; c *= 2)
+    queue_clusters_[c] = device::fit_queue_max_clusters(K, sh.n_coef, c);
   for (Lane& lane : lanes_) {
     cuda_check(cudaStreamCreateWithFlags(&lane.stream, cudaStreamNonBlocking), "cudaStreamCreate");
     cuda_check(cudaEventCreate(&lane.ev0), "event");
@@ -245,6 +247,19 @@ const double* DeviceFitter::run_ptmg(const std::vector<device::PtmgRequest>& req
 }
 
 DeviceFitter::~DeviceFitter() {
+  queue_abort();
+  for (cudaStream_t st : q_.posters)
+    if (st) cudaStreamSynchronize(st);
+  if (q_.h_ring) cudaFreeHost(q_.h_ring);
+  if (q_.h_seq) cudaFreeHost(q_.h_seq);
+  if (q_.h_one) cudaFreeHost(q_.h_one);
+  if (q_.h_results) cudaFreeHost(q_.h_results);
+  if (q_.h_done) cudaFreeHost(q_.h_done);
+  if (q_.ev0) cudaEventDestroy(q_.ev0);
+  if (q_.ev1) cudaEventDestroy(q_.ev1);
+  if (q_.ready) cudaEventDestroy(q_.ready);
+  for (cudaStream_t st : q_.posters)
+    if (st) cudaStreamDestroy(st);
   if (d_preq_) cudaFree(d_preq_);
   if (d_pres_) cudaFree(d_pres_);
   if (h_preq_) cudaFreeHost(h_preq_);
@@ -340,6 +355,205 @@ const device::FitResult* DeviceFitter::collect(int lane_index) {
   }
   lane.pending = 0;
   return lane.h_res;
+}
+
+// ---------------------------------------------------------------------------
+// Streaming mode.
+
+namespace {
+constexpr size_t kQueueCapacity = 16384;      // tickets in the ring (a power of two)
+constexpr long long kQueueIdleNs = 30000000000LL;  // longest wait of a cluster for work: 30 s
+}  // namespace
+
+int DeviceFitter::cluster_for(size_t requests) const {
+  int cluster = 1;
+  while (cluster < device::kMaxCluster && requests * static_cast<size_t>(cluster) * 2 <= static_cast<size_t>(grid_) &&
+         queue_clusters_[cluster * 2] > 0)
+    cluster *= 2;
+  return cluster;
+}
+
+void DeviceFitter::queue_start(int cluster) {
+  if (q_.running) fail(NB_ERR_GPU, "the work queue is already running");
+  if (!q_.d_ring) {
+    const size_t cap = kQueueCapacity;
+    q_.capacity = cap;
+    cuda_check(cudaEventCreate(&q_.ev0), "event");
+    cuda_check(cudaEventCreate(&q_.ev1), "event");
+    cuda_check(cudaEventCreateWithFlags(&q_.ready, cudaEventDisableTiming), "event");
+    for (cudaStream_t& st : q_.posters)
+      cuda_check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
+    cuda_check(cudaMalloc(reinterpret_cast<void**>(&q_.d_ring), cap * sizeof(device::FitRequest)), "cudaMalloc");
+    owned_.push_back(q_.d_ring);
+    cuda_check(cudaMalloc(reinterpret_cast<void**>(&q_.d_seq), cap * sizeof(long long)), "cudaMalloc");
+    owned_.push_back(q_.d_seq);
+    cuda_check(cudaMalloc(reinterpret_cast<void**>(&q_.d_stop), sizeof(int)), "cudaMalloc");
+    owned_.push_back(q_.d_stop);
+    cuda_check(cudaMalloc(reinterpret_cast<void**>(&q_.d_taken), sizeof(unsigned long long)), "cudaMalloc");
+    owned_.push_back(q_.d_taken);
+    cuda_check(cudaMalloc(reinterpret_cast<void**>(&q_.d_status), sizeof(int)), "cudaMalloc");
+    owned_.push_back(q_.d_status);
+    cuda_check(cudaMallocHost(reinterpret_cast<void**>(&q_.h_ring), cap * sizeof(device::FitRequest)),
+               "cudaMallocHost");
+    cuda_check(cudaMallocHost(reinterpret_cast<void**>(&q_.h_seq), cap * sizeof(long long)), "cudaMallocHost");
+    cuda_check(cudaMallocHost(reinterpret_cast<void**>(&q_.h_one), sizeof(int)), "cudaMallocHost");
+    *q_.h_one = 1;
+    cuda_check(cudaHostAlloc(reinterpret_cast<void**>(&q_.h_results), cap * sizeof(device::FitResult),
+                             cudaHostAllocMapped),
+               "cudaHostAlloc");
+    cuda_check(cudaHostAlloc(reinterpret_cast<void**>(&q_.h_done), cap * sizeof(long long), cudaHostAllocMapped),
+               "cudaHostAlloc");
+  }
+  if (cluster < 1 || cluster > device::kMaxCluster || queue_clusters_[cluster] <= 0)
+    fail(NB_ERR_GPU, "no resident cluster of " + std::to_string(cluster) + " fit CTAs");
+  // tickets restart at zero: no stale sequence number or done flag may match one
+  std::memset(q_.h_done, 0, q_.capacity * sizeof(long long));
+  q_.next.store(0);
+  cuda_check(cudaMemsetAsync(q_.d_seq, 0xff, q_.capacity * sizeof(long long), stream_), "memset");
+  cuda_check(cudaMemsetAsync(q_.d_stop, 0, sizeof(int), stream_), "memset");
+  cuda_check(cudaMemsetAsync(q_.d_taken, 0, sizeof(unsigned long long), stream_), "memset");
+  cuda_check(cudaMemsetAsync(q_.d_status, 0, sizeof(int), stream_), "memset");
+  // posts follow the resets
+  cuda_check(cudaEventRecord(q_.ready, stream_), "event");
+  for (cudaStream_t st : q_.posters) cuda_check(cudaStreamWaitEvent(st, q_.ready, 0), "stream wait");
+  device::FitQueue fq{};
+  fq.ring = q_.d_ring;
+  fq.seq = q_.d_seq;
+  fq.stop = q_.d_stop;
+  fq.taken = q_.d_taken;
+  void* dev_ptr = nullptr;
+  cuda_check(cudaHostGetDevicePointer(&dev_ptr, q_.h_results, 0), "mapped results");
+  fq.results = static_cast<device::FitResult*>(dev_ptr);
+  cuda_check(cudaHostGetDevicePointer(&dev_ptr, q_.h_done, 0), "mapped flags");
+  fq.done = static_cast<long long*>(dev_ptr);
+  fq.status = q_.d_status;
+  fq.mask = static_cast<long long>(q_.capacity - 1);
+  fq.idle_ns = kQueueIdleNs;
+  const int grid = queue_clusters_[cluster] * cluster;
+  cuda_check(cudaEventRecord(q_.ev0, stream_), "event");
+  cuda_check(static_cast<cudaError_t>(device::launch_fit_queue(data_, ctl_, fq, grid, cluster, stream_)),
+             "fit queue kernel launch");
+  cuda_check(cudaEventRecord(q_.ev1, stream_), "event");
+  q_.running = true;
+  ++launches_;
+}
+
+void DeviceFitter::copy_range(void* dst, const void* src, size_t elem, long long first, size_t n, cudaStream_t s) {
+  const long long mask = static_cast<long long>(q_.capacity - 1);
+  size_t copied = 0;
+  while (copied < n) {
+    const size_t slot = static_cast<size_t>((first + static_cast<long long>(copied)) & mask);
+    const size_t len = std::min(n - copied, q_.capacity - slot);
+    cuda_check(cudaMemcpyAsync(static_cast<char*>(dst) + slot * elem, static_cast<const char*>(src) + slot * elem,
+                               len * elem, cudaMemcpyHostToDevice, s),
+               "queue copy");
+    copied += len;
+  }
+}
+
+long long DeviceFitter::queue_post(const device::FitRequest* reqs, size_t n, int poster, Tally* tally) {
+  if (n == 0) return q_.next.load();
+  if (n > q_.capacity / 2) fail(NB_ERR_GPU, "too many requests in one post");
+  std::lock_guard<std::mutex> lock(q_.post_mu);
+  const long long first = q_.next.fetch_add(static_cast<long long>(n));
+  const long long cap = static_cast<long long>(q_.capacity);
+  const long long mask = cap - 1;
+  for (size_t i = 0; i < n; ++i) {
+    const long long t = first + static_cast<long long>(i);
+    if (t >= cap && !queue_done(t - cap)) {
+      // the slot still holds an unfinished request: wait for it (bounded)
+      auto t0 = Clock::now();
+      while (!queue_done(t - cap)) {
+        if (!queue_running()) queue_failure("ended with work pending");
+        if (ms_since(t0) > 60000.0) queue_failure("made no progress for 60 s");
+        std::this_thread::yield();
+      }
+    }
+    q_.h_ring[t & mask] = reqs[i];
+    q_.h_seq[t & mask] = t;
+  }
+  // the requests, then (later on the same stream) their sequence numbers.
+  // Every post goes through one stream, one at a time (the lock above):
+  // copies from several streams into neighbouring ring slots lost updates.
+  (void)poster;
+  cudaStream_t st = q_.posters[0];
+  copy_range(q_.d_ring, q_.h_ring, sizeof(device::FitRequest), first, n, st);
+  copy_range(q_.d_seq, q_.h_seq, sizeof(long long), first, n, st);
+  tally->h2d += n * (sizeof(device::FitRequest) + sizeof(long long));
+  return first;
+}
+
+bool DeviceFitter::queue_done(long long ticket) const {
+  long long& flag = q_.h_done[ticket & static_cast<long long>(q_.capacity - 1)];
+  return std::atomic_ref<long long>(flag).load(std::memory_order_acquire) == ticket + 1;
+}
+
+const device::FitResult& DeviceFitter::queue_result(long long ticket) const {
+  return q_.h_results[ticket & static_cast<long long>(q_.capacity - 1)];
+}
+
+void DeviceFitter::queue_account(long long ticket, int gene, Tally* tally) const {
+  const device::FitResult& r = queue_result(ticket);
+  ++tally->requests;
+  tally->d2h += sizeof(device::FitResult) + sizeof(long long);
+  if (r.status != 0) return;
+  const uint64_t sw = static_cast<uint64_t>(r.sweeps);
+  tally->sweeps += sw;
+  tally->cell_visits += sw * (n_cells_ + gene_nnz_[static_cast<size_t>(gene)]);
+  tally->slot_cycles += static_cast<uint64_t>(r.cycles);
+}
+
+void DeviceFitter::add_tally(const Tally& t) {
+  requests_ += t.requests;
+  sweeps_ += t.sweeps;
+  cell_visits_ += t.cell_visits;
+  slot_cycles_ += t.slot_cycles;
+  h2d_bytes_ += t.h2d;
+  d2h_bytes_ += t.d2h;
+}
+
+bool DeviceFitter::queue_running() {
+  const cudaError_t e = cudaEventQuery(q_.ev1);
+  if (e == cudaErrorNotReady) return true;
+  cuda_check(e, "fit queue kernel");
+  return false;
+}
+
+void DeviceFitter::queue_stop_impl(bool check) {
+  if (!q_.running) return;
+  q_.running = false;
+  const cudaError_t e1 = cudaMemcpyAsync(q_.d_stop, q_.h_one, sizeof(int), cudaMemcpyHostToDevice, q_.posters[0]);
+  const cudaError_t e2 = cudaEventSynchronize(q_.ev1);
+  int status = 0;
+  const cudaError_t e3 = cudaMemcpy(&status, q_.d_status, sizeof(int), cudaMemcpyDeviceToHost);
+  for (cudaStream_t st : q_.posters) cudaStreamSynchronize(st);
+  if (!check) return;
+  cuda_check(e1, "stop copy");
+  cuda_check(e2, "fit queue kernel");
+  cuda_check(e3, "queue status");
+  float ms = 0.0f;
+  cuda_check(cudaEventElapsedTime(&ms, q_.ev0, q_.ev1), "event time");
+  device_ms_ += ms;
+  if (status != 0) fail(NB_ERR_GPU, "a fit cluster waited more than 30 s for work");
+}
+
+void DeviceFitter::queue_stop() { queue_stop_impl(true); }
+
+void DeviceFitter::queue_failure(const char* what) {
+  int status = -1;
+  cudaMemcpy(&status, q_.d_status, sizeof(int), cudaMemcpyDeviceToHost);
+  unsigned long long taken = 0;
+  cudaMemcpy(&taken, q_.d_taken, sizeof(taken), cudaMemcpyDeviceToHost);
+  fail(NB_ERR_GPU, std::string("the fit queue kernel ") + what + " (tickets posted " +
+                       std::to_string(q_.next.load()) + ", taken " + std::to_string(taken) +
+                       (status == 1 ? ", a cluster waited more than 30 s for work)" : ")"));
+}
+
+void DeviceFitter::queue_abort() noexcept {
+  try {
+    queue_stop_impl(false);
+  } catch (...) {
+  }
 }
 
 bool DeviceFitter::ready(int lane_index) {
@@ -470,133 +684,60 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
   DeviceFitter& fitter = *ss.fitter;
   fitter.reset_counters();
   fitter.begin_step();
-  // stage two: every search in lockstep, one launch per round
+  // Stages two and three through one persistent launch: every gene's search
+  // runs at its own pace. When all of a gene's pending points have come
+  // back, the host steps its search and posts the next points, or, once the
+  // search is done, the gene's final fit (nebula.rs:948-967). No gene waits
+  // for another, and a gene's sequence of evaluations is that of the
+  // reference's search. The genes are dealt to host worker threads, each of
+  // which builds its genes' searches and steps them.
   auto t2 = Clock::now();
   std::vector<GeneTask> tasks(G);
-  std::vector<size_t> active;
-  for (size_t g = 0; g < G; ++g) {
-    GeneTask& t = tasks[g];
-    const GenePlan& plan = ss.plans[g];
-    if (plan.refit == Refit::None) continue;
-    std::optional<double> fixed_cell;
-    std::vector<double> start;
-    if (plan.refit == Refit::Both) {
-      start = {plan.sigma, plan.gamma};
-    } else {
-      start = {plan.sigma};
-      fixed_cell = plan.gamma;
-    }
-    std::vector<double> lower, upper;
-    variance_bounds(sh.params, fixed_cell.has_value(), &lower, &upper);
-    t.search = std::make_unique<StageTwoSearch>(start, lower, upper, plan.ord);
-    t.objective = VarianceObjective::make(sh, ss.genes[g], fixed_cell);
-    active.push_back(g);
-  }
   struct Slot {
     double subject, cell;
-    int request;  // index into the batch, -1 when the point is outside the domain
+    int ticket;  // index into the gene's tickets, -1 when the point is outside the domain
   };
-  // The genes are dealt round-robin onto the fitter's lanes. Each lane's
-  // searches advance in lockstep, one batch per round; the lanes leapfrog, so
-  // while one lane's batch runs on the device the host steps another lane's
-  // searches, and the lanes' kernels share the SMs. A gene's sequence of
-  // evaluations does not depend on which batch carries it.
-  const int L = fitter.lanes();
-  std::vector<std::vector<size_t>> lane_active(L);
-  std::vector<std::vector<device::FitRequest>> batch(L);
-  std::vector<std::vector<Slot>> slots(L);
-  for (size_t i = 0; i < active.size(); ++i) lane_active[i % L].push_back(active[i]);
-  auto build = [&](int l) {
-    batch[l].clear();
-    slots[l].clear();
-    for (size_t g : lane_active[l]) {
-      GeneTask& t = tasks[g];
-      const auto& points = t.search->ask();
-      for (size_t p = 0; p < points.size(); ++p) {
-        double subject = 0.0, cell = 0.0;
-        std::vector<double> beta;
-        Slot slot{0.0, 0.0, -1};
-        if (t.objective.request(points[p], ss.plans[g].beta_start, &subject, &cell, &beta)) {
-          device::FitRequest r{};
-          r.gene = static_cast<int32_t>(g);
-          r.ord = t.search->order();
-          r.reml = sh.params.reml ? 1 : 0;
-          r.subject = subject;
-          r.cell = cell;
-          for (int j = 0; j < sh.n_coef; ++j) r.beta[j] = beta[j];
-          slot = Slot{subject, cell, static_cast<int>(batch[l].size())};
-          batch[l].push_back(r);
-        }
-        slots[l].push_back(slot);
-      }
-    }
+  struct Flight {
+    std::vector<long long> tickets;
+    std::vector<Slot> slots;
+    bool final_fit = false;
   };
-  auto absorb = [&](int l, const device::FitResult* res) {
-    std::vector<double> values;
-    size_t si = 0;
-    std::vector<size_t> still;
-    for (size_t g : lane_active[l]) {
-      GeneTask& t = tasks[g];
-      const size_t n_points = t.search->ask().size();
-      values.assign(n_points, std::numeric_limits<double>::infinity());
-      for (size_t p = 0; p < n_points; ++p, ++si) {
-        const Slot& s = slots[l][si];
-        if (s.request < 0) continue;
-        const device::FitResult& r = res[s.request];
-        if (r.status != 0) continue;
-        InnerFit fit{r.log_likelihood, r.log_likelihood_prev, r.log_det, r.second_order};
-        values[p] = t.objective.assemble(s.subject, s.cell, fit, t.objective.tail(s.cell));
-      }
-      t.search->tell(values);
-      if (t.search->done()) {
-        t.refit = t.search->result();
-        t.search.reset();
-      } else {
-        still.push_back(g);
-      }
-    }
-    lane_active[l].swap(still);
-  };
-  // Lanes are served in the order their batches finish, so one slow batch
-  // (a search whose point needs many Newton steps) holds up no other lane.
-  uint64_t rounds = 0;
-  std::vector<int> in_flight;
-  for (int l = 0; l < L; ++l) {
-    if (lane_active[l].empty()) continue;
-    build(l);
-    fitter.submit(l, batch[l]);
-    in_flight.push_back(l);
-  }
-  while (!in_flight.empty()) {
-    bool progressed = false;
-    for (size_t i = 0; i < in_flight.size();) {
-      const int l = in_flight[i];
-      if (!fitter.ready(l)) {
-        ++i;
-        continue;
-      }
-      progressed = true;
-      const device::FitResult* res = fitter.collect(l);
-      ++rounds;
-      absorb(l, res);
-      if (!lane_active[l].empty()) {
-        build(l);
-        fitter.submit(l, batch[l]);
-        ++i;
-      } else {
-        in_flight.erase(in_flight.begin() + static_cast<std::ptrdiff_t>(i));
-      }
-    }
-    if (!progressed) std::this_thread::yield();
-  }
-  const double ms_stage_two = ms_since(t2);
-
-  // stage three: one final fit per gene at order one (nebula.rs:948-967)
-  auto t3 = Clock::now();
+  std::vector<Flight> flight(G);
   std::vector<double> sigma(G), gamma(G);
   std::vector<int> conv(G);
-  std::vector<device::FitRequest> final_batch;
-  for (size_t g = 0; g < G; ++g) {
+  std::vector<FinalFit> finals(G);
+  // a worker's requests of one pass, posted together; owners[k] = (gene,
+  // index of the gene's ticket) for outbox[k]
+  struct Outbox {
+    std::vector<device::FitRequest> reqs;
+    std::vector<std::pair<size_t, size_t>> owners;
+  };
+  auto plan_points = [&](size_t g, Outbox* box) {
+    GeneTask& t = tasks[g];
+    Flight& f = flight[g];
+    f.slots.clear();
+    f.tickets.clear();
+    for (const auto& point : t.search->ask()) {
+      double subject = 0.0, cell = 0.0;
+      std::vector<double> beta;
+      Slot slot{0.0, 0.0, -1};
+      if (t.objective.request(point, ss.plans[g].beta_start, &subject, &cell, &beta)) {
+        device::FitRequest r{};
+        r.gene = static_cast<int32_t>(g);
+        r.ord = t.search->order();
+        r.reml = sh.params.reml ? 1 : 0;
+        r.subject = subject;
+        r.cell = cell;
+        for (int j = 0; j < sh.n_coef; ++j) r.beta[j] = beta[j];
+        slot = Slot{subject, cell, static_cast<int>(f.tickets.size())};
+        box->owners.emplace_back(g, f.tickets.size());
+        box->reqs.push_back(r);
+        f.tickets.push_back(-1);
+      }
+      f.slots.push_back(slot);
+    }
+  };
+  auto plan_final = [&](size_t g, Outbox* box) {
     apply_refit(ss.plans[g], tasks[g].refit, &sigma[g], &gamma[g], &conv[g]);
     device::FitRequest r{};
     r.gene = static_cast<int32_t>(g);
@@ -606,23 +747,149 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
     r.cell = gamma[g];
     for (int j = 0; j < sh.n_coef; ++j) r.beta[j] = ss.plans[g].beta_start[j];
     r.beta[sh.intercept] -= sigma[g] / 2.0;
-    final_batch.push_back(r);
+    Flight& f = flight[g];
+    f.final_fit = true;
+    f.tickets.assign(1, -1);
+    box->owners.emplace_back(g, 0);
+    box->reqs.push_back(r);
+  };
+  auto post = [&](Outbox* box, int poster, DeviceFitter::Tally* tally) {
+    if (box->reqs.empty()) return;
+    const long long first = fitter.queue_post(box->reqs.data(), box->reqs.size(), poster, tally);
+    for (size_t k = 0; k < box->owners.size(); ++k)
+      flight[box->owners[k].first].tickets[box->owners[k].second] = first + static_cast<long long>(k);
+    box->reqs.clear();
+    box->owners.clear();
+  };
+  const int hw = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
+  const int workers = std::max(1, std::min<int>({ss.opt.host_threads > 0 ? ss.opt.host_threads : hw, 8,
+                                                 static_cast<int>(std::max<size_t>(G, 1))}));
+  std::vector<DeviceFitter::Tally> tallies(workers);
+  std::vector<uint64_t> steps(workers, 0);
+  std::atomic<bool> abort{false};
+  std::mutex err_mu;
+  std::optional<NbError> first_err;
+  auto worker = [&](int w) {
+    try {
+      DeviceFitter::Tally* tally = &tallies[w];
+      Outbox box;
+      std::vector<size_t> waiting;
+      for (size_t g = static_cast<size_t>(w); g < G; g += static_cast<size_t>(workers)) {
+        GeneTask& t = tasks[g];
+        const GenePlan& plan = ss.plans[g];
+        if (plan.refit != Refit::None) {
+          std::optional<double> fixed_cell;
+          std::vector<double> start;
+          if (plan.refit == Refit::Both) {
+            start = {plan.sigma, plan.gamma};
+          } else {
+            start = {plan.sigma};
+            fixed_cell = plan.gamma;
+          }
+          std::vector<double> lower, upper;
+          variance_bounds(sh.params, fixed_cell.has_value(), &lower, &upper);
+          t.search = std::make_unique<StageTwoSearch>(start, lower, upper, plan.ord);
+          t.objective = VarianceObjective::make(sh, ss.genes[g], fixed_cell);
+          plan_points(g, &box);
+        } else {
+          plan_final(g, &box);
+        }
+        waiting.push_back(g);
+        if (box.reqs.size() >= 64) post(&box, w, tally);
+      }
+      post(&box, w, tally);
+      auto last_progress = Clock::now();
+      while (!waiting.empty() && !abort.load(std::memory_order_relaxed)) {
+        bool progressed = false;
+        for (size_t i = 0; i < waiting.size();) {
+          const size_t g = waiting[i];
+          Flight& f = flight[g];
+          bool ready = true;
+          for (size_t k = f.tickets.size(); k > 0 && ready; --k) ready = fitter.queue_done(f.tickets[k - 1]);
+          if (!ready) {
+            ++i;
+            continue;
+          }
+          progressed = true;
+          ++steps[w];
+          if (f.final_fit) {
+            fitter.queue_account(f.tickets[0], static_cast<int>(g), tally);
+            const device::FitResult& r = fitter.queue_result(f.tickets[0]);
+            if (r.status != 0) fail(NB_ERR_INVALID_ARGUMENT, "opt_pml rejected the final variance components");
+            FinalFit& ff = finals[g];
+            ff.beta.assign(r.beta, r.beta + sh.n_coef);
+            ff.information.resize(static_cast<size_t>(sh.n_coef) * sh.n_coef);
+            for (int a = 0; a < sh.n_coef; ++a)
+              for (int b = 0; b < sh.n_coef; ++b)
+                ff.information[a * sh.n_coef + b] = r.information[a * sh.n_coef + b];
+            ff.log_likelihood = r.log_likelihood;
+            ff.iterations = r.iterations;
+            ff.backtracks = r.backtracks;
+            waiting[i] = waiting.back();
+            waiting.pop_back();
+            continue;
+          }
+          GeneTask& t = tasks[g];
+          std::vector<double> values(f.slots.size(), std::numeric_limits<double>::infinity());
+          for (size_t p = 0; p < f.slots.size(); ++p) {
+            const Slot& sl = f.slots[p];
+            if (sl.ticket < 0) continue;
+            const long long ticket = f.tickets[static_cast<size_t>(sl.ticket)];
+            fitter.queue_account(ticket, static_cast<int>(g), tally);
+            const device::FitResult& r = fitter.queue_result(ticket);
+            if (r.status != 0) continue;
+            InnerFit fit{r.log_likelihood, r.log_likelihood_prev, r.log_det, r.second_order};
+            values[p] = t.objective.assemble(sl.subject, sl.cell, fit, t.objective.tail(sl.cell));
+          }
+          t.search->tell(values);
+          if (t.search->done()) {
+            t.refit = t.search->result();
+            t.search.reset();
+            plan_final(g, &box);
+          } else {
+            plan_points(g, &box);
+          }
+          ++i;
+        }
+        post(&box, w, tally);
+        if (progressed) {
+          last_progress = Clock::now();
+        } else {
+          if (!fitter.queue_running()) fitter.queue_failure("ended with work pending");
+          if (ms_since(last_progress) > 60000.0) fitter.queue_failure("made no progress for 60 s");
+          std::this_thread::yield();
+        }
+      }
+    } catch (const NbError& e) {
+      std::lock_guard<std::mutex> lock(err_mu);
+      if (!first_err) first_err = e;
+      abort.store(true);
+    } catch (const std::exception& e) {
+      std::lock_guard<std::mutex> lock(err_mu);
+      if (!first_err) first_err = NbError{NB_ERR_GPU, e.what()};
+      abort.store(true);
+    }
+  };
+  {
+    struct QueueGuard {
+      DeviceFitter& f;
+      ~QueueGuard() { f.queue_abort(); }
+    } guard{fitter};
+    fitter.queue_start(fitter.cluster_for(G));
+    std::vector<std::thread> pool;
+    for (int w = 1; w < workers; ++w) pool.emplace_back(worker, w);
+    worker(0);
+    for (auto& th : pool) th.join();
+    if (first_err) throw *first_err;
+    fitter.queue_stop();
   }
-  const device::FitResult* res = fitter.run(final_batch);
+  for (const auto& tl : tallies) fitter.add_tally(tl);
+  uint64_t rounds = 0;
+  for (uint64_t n : steps) rounds += n;
+  const double ms_stage_two = ms_since(t2);
+  auto t3 = Clock::now();
   std::vector<GeneOutcome> outcomes(G);
-  for (size_t g = 0; g < G; ++g) {
-    const device::FitResult& r = res[g];
-    if (r.status != 0) fail(NB_ERR_INVALID_ARGUMENT, "opt_pml rejected the final variance components");
-    FinalFit ff;
-    ff.beta.assign(r.beta, r.beta + sh.n_coef);
-    ff.information.resize(static_cast<size_t>(sh.n_coef) * sh.n_coef);
-    for (int a = 0; a < sh.n_coef; ++a)
-      for (int b = 0; b < sh.n_coef; ++b) ff.information[a * sh.n_coef + b] = r.information[a * sh.n_coef + b];
-    ff.log_likelihood = r.log_likelihood;
-    ff.iterations = r.iterations;
-    ff.backtracks = r.backtracks;
-    outcomes[g] = finish_gene(sh, sigma[g], gamma[g], conv[g], ff);
-  }
+  for (size_t g = 0; g < G; ++g) outcomes[g] = finish_gene(sh, sigma[g], gamma[g], conv[g], finals[g]);
   const double ms_stage_three = ms_since(t3);
   const double ms_step = fitter.end_step();
   assemble_fit(sh, outcomes, ss.prep.kept, out);

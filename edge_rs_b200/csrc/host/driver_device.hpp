@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
+#include <mutex>
 #include <vector>
 
 #include "../cuda/pml_device.cuh"
@@ -37,6 +39,33 @@ class DeviceFitter {
   const device::FitResult* collect(int lane);
   // True once the lane's batch has finished (collect() will not wait).
   bool ready(int lane);
+
+  // Streaming mode: one persistent launch serves requests posted while it
+  // runs (device::FitQueue). queue_start launches it with `cluster` CTAs per
+  // request; queue_post (safe from several host threads, each with its own
+  // `poster` index below kMaxPosters) copies a batch of requests into the
+  // device ring on the poster's stream and returns the first one's ticket;
+  // queue_done / queue_result read a ticket's result from host memory the
+  // kernel writes; queue_stop tells idle clusters to exit, waits for the
+  // kernel and reports a timed-out wait as NB_ERR_GPU.
+  static constexpr int kMaxPosters = 8;
+  struct Tally {
+    uint64_t requests = 0, sweeps = 0, cell_visits = 0, slot_cycles = 0, h2d = 0, d2h = 0;
+  };
+  void queue_start(int cluster);
+  long long queue_post(const device::FitRequest* reqs, size_t n, int poster, Tally* tally);
+  bool queue_done(long long ticket) const;
+  const device::FitResult& queue_result(long long ticket) const;
+  void queue_account(long long ticket, int gene, Tally* tally) const;
+  void add_tally(const Tally& t);
+  bool queue_running();
+  void queue_stop();
+  // queue_stop without throwing, for unwinding
+  void queue_abort() noexcept;
+  // Throws NB_ERR_GPU describing the queue's state.
+  [[noreturn]] void queue_failure(const char* what);
+  // CTAs per request for a stage with `requests` requests in flight.
+  int cluster_for(size_t requests) const;
   // One batch of stage-one evaluations: per request (2 + W) * K doubles,
   // valid until the next call.
   const double* run_ptmg(const std::vector<device::PtmgRequest>& reqs);
@@ -72,6 +101,28 @@ class DeviceFitter {
     size_t pending = 0;  // requests of the batch in flight
   };
   void reserve(Lane& lane, size_t n);
+  struct Queue {
+    size_t capacity = 0;  // a power of two
+    device::FitRequest* d_ring = nullptr;
+    long long* d_seq = nullptr;
+    int* d_stop = nullptr;
+    unsigned long long* d_taken = nullptr;
+    int* d_status = nullptr;
+    device::FitRequest* h_ring = nullptr;    // pinned staging, slot for slot
+    long long* h_seq = nullptr;              // pinned staging, slot for slot
+    int* h_one = nullptr;                    // pinned: 1
+    device::FitResult* h_results = nullptr;  // mapped
+    long long* h_done = nullptr;             // mapped
+    cudaStream_t posters[kMaxPosters] = {};
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ready = nullptr;
+    std::atomic<long long> next{0};
+    std::mutex post_mu;
+    bool running = false;
+  };
+  void copy_range(void* dst, const void* src, size_t elem, long long first, size_t n, cudaStream_t s);
+  void queue_stop_impl(bool check);
+  Queue q_;
+  int queue_clusters_[device::kMaxCluster + 1] = {};
   cudaStream_t stream_ = nullptr;
   cudaEvent_t step0_ = nullptr, step1_ = nullptr;
   std::vector<Lane> lanes_;
