@@ -9,7 +9,7 @@ A step fits every gene of the workload:
   resident in HBM (nb_session_fit), device time from CUDA events recorded on the
   library's launching stream around the step; L2 is flushed between steps.
 - `e2e`: the drop-in nebula_sparse_cuda call from host buffers (validation,
-  stage one on host threads, upload, stages two and three, download).
+  upload, stage one, stages two and three, download).
 - `roofline`: the fit kernel against the measured FP64 FMA peak of this GPU
   (its work is FP64 arithmetic; neither HBM nor the tensor cores bound it).
 - `cpu_baseline`: the FP64 CPU oracle (the reference's nebula_sparse restated)
@@ -58,7 +58,7 @@ def parse():
     ap.add_argument("--config", default="c1")
     ap.add_argument("--genes", type=int, default=None)
     ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--lanes", type=int, default=0, help="stage-two batches in flight (0: the library default)")
+    ap.add_argument("--cluster", type=int, default=0, help="CTAs per inner fit (0: the library's choice)")
     ap.add_argument("--cpu-genes", type=int, default=32, help="gene sample of the CPU baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -181,7 +181,7 @@ def ours_arm(args, world, rank, local, dist):
     work = workloads.make(args.config, seed=1000 + rank, n_genes=args.genes)
     params = NebulaParams(method="HL")
     flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > 126 MB L2
-    session = Session(work.csr, work.subject, work.design, work.n_coef, work.offset, params, lanes=args.lanes)
+    session = Session(work.csr, work.subject, work.design, work.n_coef, work.offset, params, cluster=args.cluster)
     for _ in range(args.warmup):
         session.fit()
     sampler = ClockSampler(local)
@@ -207,8 +207,8 @@ def ours_arm(args, world, rank, local, dist):
     visits = float(np.sum([s["cell_visits"] for s in stats]))
     kernel_ms = float(np.sum([s["ms_device"] for s in stats]))
     fp64_peak = measure_fp64_tflops(5)
-    # the fit kernel is the whole step and its launches overlap across the
-    # fitter's lanes, so its FLOP are divided by the step's device time
+    # the fit kernel is the whole step (one persistent launch serves stages
+    # two and three), so its FLOP are divided by the step's device time
     achieved = visits * flops_per_visit(work.n_coef) / (float(np.sum(step_ms)) / 1000.0) / 1e12
     traffic = None
     if os.path.exists(PROFILE_SUMMARY):
@@ -226,7 +226,7 @@ def ours_arm(args, world, rank, local, dist):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         f2 = nebula_sparse_cuda(work.csr, work.subject, work.design, work.n_coef, work.offset, params,
-                                lanes=args.lanes)
+                                cluster=args.cluster)
         torch.cuda.synchronize()
         el = barrier_max(dist, time.perf_counter() - t0)
         e2e_vals.append(world * len(f2.gene_index) / el)
@@ -253,7 +253,7 @@ def ours_arm(args, world, rank, local, dist):
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                      "frac": achieved / fp64_peak if fp64_peak > 0 else None, "traffic": traffic,
                      "kernel": "fit_kernel", "flops_per_visit": flops_per_visit(work.n_coef),
-                     "time": "device time of the step (CUDA events; the kernel's launches overlap)",
+                     "time": "device time of the step (CUDA events around the persistent launch)",
                      "peak_source": "measured on this GPU: FP64 FMA chains (nb_measure_fp64_tflops)"},
         "e2e": {"value": float(np.mean(e2e_vals)) if e2e_vals else None, "unit": "genes/s",
                 "h2d_bytes_per_step": int(h2d),
@@ -269,7 +269,8 @@ def ours_arm(args, world, rank, local, dist):
                    "slot_utilisation": stats[-1]["slot_cycles"] / (stats[-1]["fit_slots"] * stats[-1]["ms_step_device"]
                                                                    * 1e-3 * clocks["sm_mhz"] * 1e6)
                    if clocks.get("sm_mhz") else None,
-                   "cycles_per_visit_per_cta": stats[-1]["slot_cycles"] / stats[-1]["cell_visits"]},
+                   "cycles_per_visit_per_cta": stats[-1]["slot_cycles"] / stats[-1]["cell_visits"],
+                   "ctas_per_fit": stats[-1]["cluster"]},
     }
     print(json.dumps(line), flush=True)
 

@@ -54,7 +54,7 @@ class NbFit(ctypes.Structure):
 class NbOptions(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("warm_start", ctypes.c_int32),
                 ("host_threads", ctypes.c_int32), ("audit_percent", ctypes.c_int32),
-                ("mlp_weights", c_float_p), ("lanes", ctypes.c_int32)]
+                ("mlp_weights", c_float_p), ("cluster", ctypes.c_int32)]
 
 
 class NbStats(ctypes.Structure):
@@ -66,7 +66,8 @@ class NbStats(ctypes.Structure):
                 ("ms_device", ctypes.c_double), ("ms_step_device", ctypes.c_double),
                 ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64),
                 ("audited", ctypes.c_uint64), ("refit_cold", ctypes.c_uint64),
-                ("fit_slots", ctypes.c_uint64), ("slot_cycles", ctypes.c_uint64)]
+                ("fit_slots", ctypes.c_uint64), ("slot_cycles", ctypes.c_uint64),
+                ("cluster", ctypes.c_uint64)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

@@ -121,11 +121,11 @@ def call_nebula(fn, counts, subject_id, design, n_coef, offset, params, extra_ar
 
 
 def nebula_sparse_cuda(counts, subject_id, design, n_coef, offset=None, params: Optional[NebulaParams] = None,
-                       warm_start=False, device=-1, host_threads=0, audit_percent=5, lanes=0):
+                       warm_start=False, device=-1, host_threads=0, audit_percent=5, cluster=0):
     """Fits NEBULA per gene with every inner penalised fit on the GPU."""
     lib = _ffi.product_library()
     opts = _ffi.NbOptions(int(device), int(bool(warm_start)), int(host_threads), int(audit_percent), None,
-                          int(lanes))
+                          int(cluster))
     return call_nebula(lib.nebula_sparse_cuda_ex, counts, subject_id, design, n_coef, offset, params,
                        options=opts, want_stats=True)
 
@@ -169,7 +169,7 @@ class Session:
     three on the resident copy."""
 
     def __init__(self, counts, subject_id, design, n_coef, offset=None, params: Optional[NebulaParams] = None,
-                 warm_start=False, device=-1, host_threads=0, audit_percent=5, lanes=0):
+                 warm_start=False, device=-1, host_threads=0, audit_percent=5, cluster=0):
         self._lib = _ffi.product_library()
         self._keep = []
         csr = _as_csr(counts)
@@ -180,7 +180,7 @@ class Session:
         self.n_coef = int(n_coef)
         p = (params or NebulaParams()).to_c()
         opts = _ffi.NbOptions(int(device), int(bool(warm_start)), int(host_threads), int(audit_percent), None,
-                              int(lanes))
+                              int(cluster))
         self._keep = [csr, subject, design, off, p, opts]
         handle = ctypes.c_void_p()
         err = ctypes.create_string_buffer(512)

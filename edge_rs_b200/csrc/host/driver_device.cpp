@@ -366,9 +366,15 @@ constexpr long long kQueueIdleNs = 30000000000LL;  // longest wait of a cluster 
 }  // namespace
 
 int DeviceFitter::cluster_for(size_t requests) const {
+  // Spread each fit over more CTAs while (a) the fits in flight times the
+  // cluster stay within about four times the resident CTA slots, so the
+  // searches that finish last still find the SMs busy, and (b) each CTA keeps
+  // at least ~40,000 cells per sweep, so a sweep's fixed costs (the cluster
+  // barrier, the combine, the Newton step every CTA repeats) stay small.
   int cluster = 1;
-  while (cluster < device::kMaxCluster && requests * static_cast<size_t>(cluster) * 2 <= static_cast<size_t>(grid_) &&
-         queue_clusters_[cluster * 2] > 0)
+  while (cluster < device::kMaxCluster && queue_clusters_[cluster * 2] > 0 &&
+         requests * static_cast<size_t>(cluster) * 2 <= 4 * static_cast<size_t>(grid_) &&
+         n_cells_ >= static_cast<size_t>(cluster) * 2 * 40000)
     cluster *= 2;
   return cluster;
 }
@@ -595,7 +601,39 @@ struct Session {
   std::unique_ptr<DeviceFitter> fitter;
   nb_options opt{};
   double ms_prepare = 0.0, ms_stage_one = 0.0, ms_upload = 0.0;
+  // autotuning of the CTAs per fit: the first calls of a session try the
+  // candidates in turn (the results do not depend on the choice) and later
+  // calls take the fastest
+  std::vector<int> tune_candidates;
+  std::vector<double> tune_ms;
+  int tuned = 0;
 };
+
+int choose_cluster(Session& ss, size_t G) {
+  const int forced = ss.opt.cluster;
+  if (forced == 1 || forced == 2 || forced == 4 || forced == 8) return forced;
+  if (ss.tuned > 0) return ss.tuned;
+  if (ss.tune_candidates.empty()) {
+    const int guess = ss.fitter->cluster_for(G);
+    for (int c : {guess, guess * 2, guess / 2})
+      if (c >= 1 && c <= device::kMaxCluster &&
+          std::find(ss.tune_candidates.begin(), ss.tune_candidates.end(), c) == ss.tune_candidates.end())
+        ss.tune_candidates.push_back(c);
+  }
+  return ss.tune_candidates[ss.tune_ms.size()];
+}
+
+void record_cluster(Session& ss, int cluster, double ms) {
+  if (ss.tuned > 0 || ss.tune_candidates.empty() || ss.opt.cluster != 0) return;
+  if (ss.tune_candidates[ss.tune_ms.size()] != cluster) return;
+  ss.tune_ms.push_back(ms);
+  if (ss.tune_ms.size() == ss.tune_candidates.size()) {
+    size_t best = 0;
+    for (size_t i = 1; i < ss.tune_ms.size(); ++i)
+      if (ss.tune_ms[i] < ss.tune_ms[best]) best = i;
+    ss.tuned = ss.tune_candidates[best];
+  }
+}
 
 std::unique_ptr<Session> create_session(const nb_csr* counts, const uint64_t* subject_id, const double* design,
                                         uint32_t n_coef, const double* offset, const nb_params* params,
@@ -615,8 +653,7 @@ std::unique_ptr<Session> create_session(const nb_csr* counts, const uint64_t* su
                [&](size_t g) { ss->genes[g] = positive_indices(ss->prep.counts, ss->prep.kept[g]); });
   ss->ms_prepare = ms_since(t0);
   auto t2 = Clock::now();
-  const int lanes = ss->opt.lanes > 0 ? ss->opt.lanes : DeviceFitter::kDefaultLanes;
-  ss->fitter = std::make_unique<DeviceFitter>(ss->prep, ss->genes, ss->opt.device, lanes);
+  ss->fitter = std::make_unique<DeviceFitter>(ss->prep, ss->genes, ss->opt.device);
   ss->ms_upload = ms_since(t2);
   // stage one (nebula.rs:812-901): every gene's projected Newton in lockstep,
   // one batched launch of marginal-likelihood cell passes per round
@@ -764,6 +801,7 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
   const int hw = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
   const int workers = std::max(1, std::min<int>({ss.opt.host_threads > 0 ? ss.opt.host_threads : hw, 8,
                                                  static_cast<int>(std::max<size_t>(G, 1))}));
+  const int cluster = choose_cluster(ss, G);
   std::vector<DeviceFitter::Tally> tallies(workers);
   std::vector<uint64_t> steps(workers, 0);
   std::atomic<bool> abort{false};
@@ -875,7 +913,7 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
       DeviceFitter& f;
       ~QueueGuard() { f.queue_abort(); }
     } guard{fitter};
-    fitter.queue_start(fitter.cluster_for(G));
+    fitter.queue_start(cluster);
     std::vector<std::thread> pool;
     for (int w = 1; w < workers; ++w) pool.emplace_back(worker, w);
     worker(0);
@@ -892,6 +930,7 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
   for (size_t g = 0; g < G; ++g) outcomes[g] = finish_gene(sh, sigma[g], gamma[g], conv[g], finals[g]);
   const double ms_stage_three = ms_since(t3);
   const double ms_step = fitter.end_step();
+  record_cluster(ss, cluster, ms_step);
   assemble_fit(sh, outcomes, ss.prep.kept, out);
   if (stats) {
     stats->rounds = rounds;
@@ -900,6 +939,7 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
     stats->cell_visits = fitter.cell_visits();
     stats->fit_slots = static_cast<uint64_t>(fitter.grid());
     stats->slot_cycles = fitter.slot_cycles();
+    stats->cluster = static_cast<uint64_t>(cluster);
     stats->gpu_launches = fitter.launches();
     stats->ms_prepare = ss.ms_prepare;
     stats->ms_stage_one = ss.ms_stage_one;

@@ -102,7 +102,8 @@ typedef struct nb_options {
   int32_t host_threads;  /* stage-one host threads; 0 = all cores */
   int32_t audit_percent; /* warm start only: share of genes refit cold */
   const float* mlp_weights; /* warm start only: nb_mlp_* layout; NULL = built-in */
-  int32_t lanes;         /* stage-two batches in flight at once (1-64); 0 = 8 */
+  int32_t cluster;       /* CTAs sharing each inner fit in stages two and three
+                            (1, 2, 4 or 8); 0 = chosen per call */
 } nb_options;
 
 /* Counters of one call (timings in milliseconds of host wall clock, device
@@ -121,6 +122,7 @@ typedef struct nb_stats {
   uint64_t audited, refit_cold;
   uint64_t fit_slots;       /* fit-kernel CTAs resident at once (per lane) */
   uint64_t slot_cycles;     /* SM clock cycles the fit CTAs spent on requests */
+  uint64_t cluster;         /* CTAs that shared each fit in stages two and three */
 } nb_stats;
 
 void nb_params_default(nb_params* params);
