@@ -61,6 +61,9 @@ def parse():
     ap.add_argument("--cluster", type=int, default=0, help="CTAs per inner fit (0: the library's choice)")
     ap.add_argument("--cpu-genes", type=int, default=32, help="gene sample of the CPU baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fit-batch", type=int, default=0,
+                    help="instead of the bench: time launches of the fit kernel in batch mode, this many inner fits "
+                         "of the workload's first gene per launch (the profiling workload)")
     return ap.parse_args()
 
 
@@ -275,8 +278,43 @@ def ours_arm(args, world, rank, local, dist):
     print(json.dumps(line), flush=True)
 
 
+def fit_batch(args):
+    """R inner fits of one c1-shaped gene per launch through nb_opt_pml_cuda:
+    the per-fit code of the persistent launch (fit_one) in the batch kernel,
+    a bounded single launch for the profiler. Prints one JSON line."""
+    from edge_rs_b200.api import opt_pml_cuda
+    work = workloads.make(args.config, seed=1000, n_genes=1)
+    lo, hi = int(work.indptr[0]), int(work.indptr[1])
+    cells, counts = work.indices[lo:hi], work.data[lo:hi]
+    keep = counts > 0
+    cells, counts = cells[keep], counts[keep]
+    fid = np.concatenate([[0], np.cumsum(work.truth["sizes"])]).astype(np.uint64)
+    subj = np.searchsorted(fid, cells, side="right") - 1
+    total = np.bincount(subj, weights=counts, minlength=fid.size - 1)
+    design = work.design.astype(np.float64)
+    log_off = np.log(work.offset)
+    beta0 = np.zeros(work.n_coef)
+    beta0[0] = np.log(max(counts.sum() / work.n_cells, 1e-3)) - float(np.mean(log_off))
+    rng = np.random.default_rng(0)
+    r = args.fit_batch
+    sigma = rng.uniform(0.05, 1.5, r)
+    gamma = np.exp(rng.uniform(np.log(0.5), np.log(10.0), r))
+    times, sweeps = [], 0
+    for _ in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        out = opt_pml_cuda(design, log_off, counts, cells, fid, total, beta0, sigma, gamma)
+        times.append(time.perf_counter() - t0)
+        sweeps = int(out["sweeps"].sum())
+    ms = 1000.0 * float(np.median(times[args.warmup:]))
+    print(json.dumps({"mode": "fit-batch", "requests": r, "n_cells": int(work.n_cells), "nnz": int(cells.size),
+                      "sweeps_per_launch": sweeps, "ms_per_call": ms}), flush=True)
+
+
 def main():
     args = parse()
+    if args.fit_batch > 0:
+        fit_batch(args)
+        return
     if args.impl == "reference":  # rank 0 alone times the CPU path; other ranks exit
         reference_arm(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), None)
         return

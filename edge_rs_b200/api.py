@@ -210,6 +210,47 @@ class Session:
         self.close()
 
 
+def opt_pml_cuda(design, offset, counts, cells, subject_start, subject_total, beta_init, subject, cell, ord=None,
+                 reml=False, eps=1e-6):
+    """A batch of inner fits of one gene on the GPU (nb_opt_pml_cuda; the
+    reference's opt_pml, src/sc/pml.rs:468-508, once per (subject, cell)
+    point). `design` is used as given (n_cells x n_beta), `offset` holds log
+    offsets, `counts`/`cells` the positive entries in cell order,
+    `subject_start` the k + 1 subject boundaries. Returns a dict of arrays:
+    beta (n x n_beta), information (n x n_beta^2), log_likelihood,
+    log_likelihood_prev, log_det, second_order, status, iterations,
+    backtracks, sweeps."""
+    lib = _ffi.product_library()
+    design = np.ascontiguousarray(design, np.float64)
+    offset = np.ascontiguousarray(offset, np.float64)
+    n_cells = offset.size
+    n_beta = design.size // n_cells
+    counts = np.ascontiguousarray(counts, np.float64)
+    cells = np.ascontiguousarray(cells, np.uint32)
+    ss = np.ascontiguousarray(subject_start, np.uint64)
+    tot = np.ascontiguousarray(subject_total, np.float64)
+    subject = np.atleast_1d(np.asarray(subject, np.float64))
+    n = subject.size
+    cell = np.ascontiguousarray(np.broadcast_to(np.asarray(cell, np.float64), (n,)))
+    b0 = np.ascontiguousarray(np.broadcast_to(np.asarray(beta_init, np.float64), (n, n_beta)))
+    ordv = np.ascontiguousarray(np.broadcast_to(np.asarray(1 if ord is None else ord, np.int32), (n,)))
+    beta = np.zeros((n, n_beta))
+    info = np.zeros((n, n_beta * n_beta))
+    sc = np.zeros((n, 4))
+    ints = np.zeros((n, 4), np.int32)
+    err = ctypes.create_string_buffer(256)
+    p = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    rc = lib.nb_opt_pml_cuda(p(design), p(offset), ctypes.c_uint64(n_cells), ctypes.c_uint32(n_beta), p(counts),
+                             p(cells), ctypes.c_uint64(counts.size), p(ss), ctypes.c_uint32(ss.size - 1), p(tot),
+                             ctypes.c_uint32(n), p(b0), p(subject), p(cell), p(ordv), ctypes.c_int32(int(reml)),
+                             ctypes.c_double(eps), p(beta), p(info), p(sc), p(ints), err, ctypes.c_size_t(len(err)))
+    if rc != 0:
+        raise NebulaError(rc, err.value.decode(errors="replace"))
+    return dict(beta=beta, information=info, log_likelihood=sc[:, 0], log_likelihood_prev=sc[:, 1],
+                log_det=sc[:, 2], second_order=sc[:, 3], status=ints[:, 0], iterations=ints[:, 1],
+                backtracks=ints[:, 2], sweeps=ints[:, 3])
+
+
 def measure_fp64_tflops(repeats=5):
     """Measured FP64 FMA throughput of the current device (TFLOP/s)."""
     return float(_ffi.product_library().nb_measure_fp64_tflops(int(repeats)))
