@@ -58,6 +58,17 @@ struct Dims {
 };
 constexpr int kLaplaceSums = 4;
 
+// Asynchronous 8-byte copy global -> shared (cp.async), and its group fences.
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
@@ -71,6 +82,7 @@ struct Smem {
   NbTableData* tab;      // exp/log tables (nbmath.hpp)
   double* pieces[2];     // (K + kRanges) x NS each: one sweep's (subject, range) pieces, by sweep parity
   double* totals;        // K x NS, per-subject totals after the combine
+  double* stage;         // kWarps x kStageDoubles: each lane's next two design rows and offsets
   double* sw[2];         // two sweeps: w K, dw K, vw K, vwb K*NB, db NB, vb NB*NB, ll 1
   double* beta;          // NB
   double* log_w;         // K
@@ -93,10 +105,12 @@ struct Smem {
   int32_t* vlo;          // K: first range meeting each subject
   int32_t* vhi;          // K: last range meeting each subject
 
+  // two buffers x two cells x (NB design values + the offset) x 32 lanes
+  static constexpr int kStageDoubles = 2 * 2 * (NB + 1) * 32;
   __host__ __device__ static size_t sweep_doubles(int K) { return 3 * K + K * NB + NB + NB * NB + 1; }
   __host__ __device__ static size_t doubles(int K) {
-    return (size_t)kNbTableDoubles + (size_t)(3 * K + 2 * kRanges) * Dims<NB>::NS + 2 * sweep_doubles(K) +
-           4 * NB + 7 * K + 2 * NB * NB + 16 + (kRanges + 1) + (K + 1);
+    return (size_t)kNbTableDoubles + (size_t)kWarps * kStageDoubles + (size_t)(3 * K + 2 * kRanges) * Dims<NB>::NS +
+           2 * sweep_doubles(K) + 4 * NB + 7 * K + 2 * NB * NB + 16 + (kRanges + 1) + (K + 1);
   }
   __host__ __device__ static size_t bytes(int K) {
     return doubles(K) * 8 + (size_t)(K + 1 + kRanges + 1 + 2 * K) * 4 + 16;
@@ -107,6 +121,8 @@ struct Smem {
     double* p = base;
     tab = reinterpret_cast<NbTableData*>(p);
     p += kNbTableDoubles;
+    stage = p;
+    p += kWarps * kStageDoubles;
     pieces[0] = p;
     p += (K + kRanges) * Dims<NB>::NS;
     pieces[1] = p;
@@ -291,15 +307,48 @@ __device__ void sweep_sums(const GeneData& d, Smem<NB>& sm, const double* beta_s
       for (int x = 0; x < NV; ++x) acc[x] = 0.0;
       // dense: two cells (r and r + 32) per iteration; their exp/log/division
       // chains interleave, and each accumulator still takes cell r before
-      // cell r + 32, the order of the lane's sequential sum
+      // cell r + 32, the order of the lane's sequential sum. Each lane copies
+      // its next iteration's two design rows and offsets into shared memory
+      // (cp.async, double-buffered) while it computes the current ones, and
+      // reads only what it copied itself.
+      double* stg = sm.stage + warp * Smem<NB>::kStageDoubles;
+      auto prefetch = [&](int r, int buf) {
+        double* dst = stg + buf * 2 * (NB + 1) * 32 + lane;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          const int c = r + 32 * k;
+          if (c < s_end) {
+            const double* row = d.design + static_cast<size_t>(c) * NB;
+#pragma unroll
+            for (int j = 0; j < NB; ++j) cp_async8(dst + (k * (NB + 1) + j) * 32, row + j);
+            cp_async8(dst + (k * (NB + 1) + NB) * 32, d.log_offset + c);
+          }
+        }
+        cp_async_commit();
+      };
+      int buf = 0;
+      prefetch(c0 + lane, 0);
       for (int r = c0 + lane; r < s_end; r += 64) {
+        prefetch(r + 64, buf ^ 1);
+        cp_async_wait<1>();
         const bool has_b = r + 32 < s_end;
-        const int rb = has_b ? r + 32 : r;
+        const double* src = stg + buf * 2 * (NB + 1) * 32 + lane;
         double xa[NB], xb[NB];
-        load_row<NB>(d.design, r, xa);
-        load_row<NB>(d.design, rb, xb);
-        const double ea = nb_exp_tab(linear_eta<NB>(xa, beta, __ldg(d.log_offset + r)) + lw, tab);
-        const double eb = nb_exp_tab(linear_eta<NB>(xb, beta, __ldg(d.log_offset + rb)) + lw, tab);
+#pragma unroll
+        for (int j = 0; j < NB; ++j) xa[j] = src[j * 32];
+        const double offa = src[NB * 32];
+        double offb = offa;
+        if (has_b) {
+#pragma unroll
+          for (int j = 0; j < NB; ++j) xb[j] = src[((NB + 1) + j) * 32];
+          offb = src[(2 * NB + 1) * 32];
+        } else {
+#pragma unroll
+          for (int j = 0; j < NB; ++j) xb[j] = xa[j];
+        }
+        buf ^= 1;
+        const double ea = nb_exp_tab(linear_eta<NB>(xa, beta, offa) + lw, tab);
+        const double eb = nb_exp_tab(linear_eta<NB>(xb, beta, offb) + lw, tab);
         const double ta = ea + gamma, tb = eb + gamma;
         if (MODE == 0) {
           const double la = nb_log_tab(ta, tab), lb = nb_log_tab(tb, tab);
@@ -316,6 +365,7 @@ __device__ void sweep_sums(const GeneData& d, Smem<NB>& sm, const double* beta_s
           if (has_b) laplace_terms(acc, eb, tb, gamma, gamma);
         }
       }
+      cp_async_wait<0>();
       // sparse: the segment's positive entries, into the same partials
       for (uint64_t p = pa + lane; p < p_end; p += 64) {
         const bool has_b = p + 32 < p_end;
