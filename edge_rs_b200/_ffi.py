@@ -54,7 +54,8 @@ class NbFit(ctypes.Structure):
 class NbOptions(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("warm_start", ctypes.c_int32),
                 ("host_threads", ctypes.c_int32), ("audit_percent", ctypes.c_int32),
-                ("mlp_weights", c_float_p), ("cluster", ctypes.c_int32)]
+                ("mlp_weights", c_float_p), ("cluster", ctypes.c_int32),
+                ("warm_points", ctypes.POINTER(ctypes.c_double)), ("evaluations", ctypes.POINTER(ctypes.c_int32))]
 
 
 class NbStats(ctypes.Structure):
@@ -102,7 +103,22 @@ PRODUCT_SIGNATURES = {
                                           ctypes.POINTER(ctypes.c_uint32)]),
     "nb_bobyqa_free": (None, [ctypes.c_void_p]),
     "nb_measure_fp64_tflops": (ctypes.c_double, [ctypes.c_int]),
+    "nb_mlp_init": (None, [ctypes.c_uint64, c_float_p]),
+    "nb_mlp_builtin": (None, [c_float_p]),
+    "nb_mlp_predict_cuda": (ctypes.c_int32, [c_float_p, c_float_p, ctypes.c_uint64, c_float_p, ctypes.c_char_p,
+                                             ctypes.c_size_t]),
+    "nb_mlp_gradient_cuda": (ctypes.c_int32, [c_float_p, c_float_p, c_float_p, ctypes.c_uint64, c_float_p,
+                                              c_double_p, ctypes.c_char_p, ctypes.c_size_t]),
+    "nb_mlp_train_cuda": (ctypes.c_int32, [c_float_p, c_float_p, ctypes.c_uint64, ctypes.c_int32, ctypes.c_int32,
+                                           ctypes.c_float, ctypes.c_uint64, c_float_p, c_double_p, ctypes.c_char_p,
+                                           ctypes.c_size_t]),
+    "nb_session_features": (ctypes.c_int32, [ctypes.c_void_p, c_float_p, c_double_p, c_u64_p, ctypes.c_char_p,
+                                             ctypes.c_size_t]),
 }
+
+MLP_FEATURES = 12
+MLP_OUTPUTS = 3
+MLP_PARAMS = 5211
 
 
 def declare(lib, signatures):

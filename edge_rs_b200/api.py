@@ -59,6 +59,7 @@ class NebulaFit:
     gene_index: np.ndarray
     n_coef: int
     stats: dict = field(default_factory=dict)
+    evaluations: Optional[np.ndarray] = None  # stage-two objective evaluations per gene
 
 
 def _as_csr(counts):
@@ -120,14 +121,44 @@ def call_nebula(fn, counts, subject_id, design, n_coef, offset, params, extra_ar
     return fit_from_arrays(out, n_coef, stats.as_dict() if want_stats else None)
 
 
+def _options(device, warm_start, host_threads, audit_percent, cluster, n_genes, warm_points=None,
+             mlp_weights=None):
+    """An NbOptions plus the arrays it points into (kept alive by the caller)."""
+    evaluations = np.zeros(max(int(n_genes), 1), np.int32)
+    wp = None if warm_points is None else np.ascontiguousarray(warm_points, np.float64).reshape(-1, 2)
+    mw = None if mlp_weights is None else np.ascontiguousarray(mlp_weights, np.float32)
+    if mw is not None and mw.size != _ffi.MLP_PARAMS:
+        raise NebulaError(2, f"mlp_weights has {mw.size} values, expected {_ffi.MLP_PARAMS}")
+    if wp is not None and wp.shape[0] != n_genes:
+        raise NebulaError(2, f"warm_points has {wp.shape[0]} rows, expected {n_genes}")
+    mode = int(warm_start)
+    opts = _ffi.NbOptions(int(device), mode, int(host_threads), int(audit_percent),
+                          _ffi.ptr(mw, ctypes.c_float), int(cluster), _ffi.ptr(wp, ctypes.c_double),
+                          _ffi.ptr(evaluations, ctypes.c_int32))
+    return opts, [evaluations, wp, mw]
+
+
 def nebula_sparse_cuda(counts, subject_id, design, n_coef, offset=None, params: Optional[NebulaParams] = None,
-                       warm_start=False, device=-1, host_threads=0, audit_percent=5, cluster=0):
-    """Fits NEBULA per gene with every inner penalised fit on the GPU."""
+                       warm_start=False, device=-1, host_threads=0, audit_percent=5, cluster=0, warm_points=None,
+                       mlp_weights=None):
+    """Fits NEBULA per gene with every inner penalised fit on the GPU.
+
+    warm_start: False/0 plain (the reference's method). Otherwise every
+    inner fit after a gene's first search step starts from the gene's
+    previous iterate, and the search starts from: True/1 the warm-start
+    network's prediction (`mlp_weights`, or the built-in network); 2
+    `warm_points` (n_genes x (sigma, gamma)); 3 stage one's estimate.
+    audit_percent of the searched genes also run plain and keep that
+    result when its objective is better.
+    """
     lib = _ffi.product_library()
-    opts = _ffi.NbOptions(int(device), int(bool(warm_start)), int(host_threads), int(audit_percent), None,
-                          int(cluster))
-    return call_nebula(lib.nebula_sparse_cuda_ex, counts, subject_id, design, n_coef, offset, params,
-                       options=opts, want_stats=True)
+    n_genes = int(_as_csr(counts).struct.n_genes)
+    opts, keep = _options(device, warm_start, host_threads, audit_percent, cluster, n_genes, warm_points,
+                          mlp_weights)
+    fit = call_nebula(lib.nebula_sparse_cuda_ex, counts, subject_id, design, n_coef, offset, params,
+                      options=opts, want_stats=True)
+    fit.evaluations = keep[0][: len(fit.gene_index)].copy()
+    return fit
 
 
 @dataclass
@@ -169,7 +200,8 @@ class Session:
     three on the resident copy."""
 
     def __init__(self, counts, subject_id, design, n_coef, offset=None, params: Optional[NebulaParams] = None,
-                 warm_start=False, device=-1, host_threads=0, audit_percent=5, cluster=0):
+                 warm_start=False, device=-1, host_threads=0, audit_percent=5, cluster=0, warm_points=None,
+                 mlp_weights=None):
         self._lib = _ffi.product_library()
         self._keep = []
         csr = _as_csr(counts)
@@ -179,9 +211,10 @@ class Session:
         self.n_genes = int(csr.struct.n_genes)
         self.n_coef = int(n_coef)
         p = (params or NebulaParams()).to_c()
-        opts = _ffi.NbOptions(int(device), int(bool(warm_start)), int(host_threads), int(audit_percent), None,
-                              int(cluster))
-        self._keep = [csr, subject, design, off, p, opts]
+        opts, arrays = _options(device, warm_start, host_threads, audit_percent, cluster, self.n_genes,
+                                warm_points, mlp_weights)
+        self._evaluations = arrays[0]
+        self._keep = [csr, subject, design, off, p, opts, arrays]
         handle = ctypes.c_void_p()
         err = ctypes.create_string_buffer(512)
         rc = self._lib.nb_session_create(ctypes.byref(csr.struct), _ffi.ptr(subject, ctypes.c_uint64),
@@ -199,7 +232,22 @@ class Session:
         rc = self._lib.nb_session_fit(self._handle, ctypes.byref(out.struct), ctypes.byref(stats), err, len(err))
         if rc != 0:
             raise NebulaError(rc, err.value.decode(errors="replace"))
-        return fit_from_arrays(out, self.n_coef, stats.as_dict())
+        fit = fit_from_arrays(out, self.n_coef, stats.as_dict())
+        fit.evaluations = self._evaluations[: len(fit.gene_index)].copy()
+        return fit
+
+    def features(self):
+        """The kept genes' warm-start features (n_kept x 12) and stage one's
+        (sigma, gamma) (n_kept x 2)."""
+        n = ctypes.c_uint64(0)
+        err = ctypes.create_string_buffer(256)
+        feats = np.zeros((self.n_genes, _ffi.MLP_FEATURES), np.float32)
+        s1 = np.zeros((self.n_genes, 2))
+        rc = self._lib.nb_session_features(self._handle, _ffi.ptr(feats, ctypes.c_float), _ffi.ptr(s1, ctypes.c_double),
+                                           ctypes.byref(n), err, len(err))
+        if rc != 0:
+            raise NebulaError(rc, err.value.decode(errors="replace"))
+        return feats[: n.value].copy(), s1[: n.value].copy()
 
     def close(self):
         if getattr(self, "_handle", None):
@@ -249,6 +297,65 @@ def opt_pml_cuda(design, offset, counts, cells, subject_start, subject_total, be
     return dict(beta=beta, information=info, log_likelihood=sc[:, 0], log_likelihood_prev=sc[:, 1],
                 log_det=sc[:, 2], second_order=sc[:, 3], status=ints[:, 0], iterations=ints[:, 1],
                 backtracks=ints[:, 2], sweeps=ints[:, 3])
+
+
+def _check(rc, err):
+    if rc != 0:
+        raise NebulaError(rc, err.value.decode(errors="replace"))
+
+
+def mlp_init(seed=0):
+    """Initial warm-start network parameters (NB_MLP_PARAMS float32)."""
+    p = np.zeros(_ffi.MLP_PARAMS, np.float32)
+    _ffi.product_library().nb_mlp_init(ctypes.c_uint64(seed), _ffi.ptr(p, ctypes.c_float))
+    return p
+
+
+def mlp_builtin():
+    """The built-in warm-start network's parameters."""
+    p = np.zeros(_ffi.MLP_PARAMS, np.float32)
+    _ffi.product_library().nb_mlp_builtin(_ffi.ptr(p, ctypes.c_float))
+    return p
+
+
+def mlp_predict(params, features):
+    """The network's outputs (n x 3) on the GPU."""
+    p = np.ascontiguousarray(params, np.float32)
+    x = np.ascontiguousarray(features, np.float32).reshape(-1, _ffi.MLP_FEATURES)
+    out = np.zeros((x.shape[0], _ffi.MLP_OUTPUTS), np.float32)
+    err = ctypes.create_string_buffer(256)
+    _check(_ffi.product_library().nb_mlp_predict_cuda(_ffi.ptr(p, ctypes.c_float), _ffi.ptr(x, ctypes.c_float),
+                                                      x.shape[0], _ffi.ptr(out, ctypes.c_float), err, len(err)), err)
+    return out
+
+
+def mlp_gradient(params, features, targets):
+    """(loss, gradient) of the network on the GPU."""
+    p = np.ascontiguousarray(params, np.float32)
+    x = np.ascontiguousarray(features, np.float32).reshape(-1, _ffi.MLP_FEATURES)
+    t = np.ascontiguousarray(targets, np.float32).reshape(-1, _ffi.MLP_OUTPUTS)
+    g = np.zeros(_ffi.MLP_PARAMS, np.float32)
+    loss = ctypes.c_double(0.0)
+    err = ctypes.create_string_buffer(256)
+    _check(_ffi.product_library().nb_mlp_gradient_cuda(_ffi.ptr(p, ctypes.c_float), _ffi.ptr(x, ctypes.c_float),
+                                                       _ffi.ptr(t, ctypes.c_float), x.shape[0],
+                                                       _ffi.ptr(g, ctypes.c_float), ctypes.byref(loss), err,
+                                                       len(err)), err)
+    return loss.value, g
+
+
+def mlp_train(features, targets, params, epochs=200, batch=512, lr=1e-3, seed=0):
+    """Trains a copy of `params` with Adam on the GPU; returns (params, per-epoch mean batch loss)."""
+    p = np.array(params, np.float32, copy=True)
+    x = np.ascontiguousarray(features, np.float32).reshape(-1, _ffi.MLP_FEATURES)
+    t = np.ascontiguousarray(targets, np.float32).reshape(-1, _ffi.MLP_OUTPUTS)
+    losses = np.zeros(int(epochs))
+    err = ctypes.create_string_buffer(256)
+    _check(_ffi.product_library().nb_mlp_train_cuda(_ffi.ptr(x, ctypes.c_float), _ffi.ptr(t, ctypes.c_float),
+                                                    x.shape[0], int(epochs), int(batch), ctypes.c_float(lr),
+                                                    ctypes.c_uint64(seed), _ffi.ptr(p, ctypes.c_float),
+                                                    _ffi.ptr(losses, ctypes.c_double), err, len(err)), err)
+    return p, losses
 
 
 def measure_fp64_tflops(repeats=5):

@@ -23,7 +23,7 @@ struct alignas(16) FitRequest {
   int32_t gene;       // row of the resident CSR (kept genes, in kept order)
   int32_t ord;        // Laplace order (1, 2 or 3)
   int32_t reml;       // add log|det(information)| to the log-determinant
-  int32_t pad;
+  int32_t flags;      // warm inner starts (kWarm*); 0 = the reference's cold start
   double subject;     // nebula's sigma[0] = log(1 + sigma^2)
   double cell;        // NB size gamma
   double beta[kMaxCoef];  // starting fixed effects (log_w starts at zero)
@@ -39,6 +39,13 @@ struct alignas(16) FitResult {
   int64_t pad;
 };
 
+// FitRequest.flags: start the Newton loop from the gene's stored (beta,
+// log_w) in buffer 1 - kWarmBuffer instead of (beta, 0); store the final
+// (beta, log_w) into buffer kWarmBuffer.
+constexpr int32_t kWarmRead = 1;
+constexpr int32_t kWarmWrite = 2;
+constexpr int32_t kWarmBuffer = 4;
+
 // Resident per-call data, device pointers.
 struct GeneData {
   const double* design;      // n_cells x n_coef, centred, row-major
@@ -52,6 +59,7 @@ struct GeneData {
   const uint32_t* warp_cells;  // kWarps + 1 boundaries of stage one's warp ranges
   const uint32_t* range_cells; // kRanges + 1 boundaries of the sweep's cell ranges
   const uint64_t* range_pos;   // n_genes x (kRanges + 1): first positive entry at or after each boundary
+  double* warm_state;          // n_genes x 2 x (n_coef + n_subjects), or null
   int32_t n_cells;
   int32_t n_subjects;
   int32_t n_coef;

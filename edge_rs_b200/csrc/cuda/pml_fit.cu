@@ -607,8 +607,15 @@ __device__ void fit_one(const GeneData& d, const FitControl& ctl, Smem<NB>& sm, 
     sm.sc[kGamma] = req.cell;
     sm.sc[kSweeps] = 0.0;
   }
-  if (tid < NB) sm.beta[tid] = req.beta[tid];
-  for (int s = tid; s < K; s += blockDim.x) sm.log_w[s] = 0.0;
+  // warm inner start: the gene's stored iterate (read past L1; another
+  // cluster wrote it in an earlier step of the gene's search)
+  const size_t warm_stride = static_cast<size_t>(NB + K);
+  const bool warm_read = d.warm_state && (req.flags & kWarmRead);
+  const double* warm_src =
+      warm_read ? d.warm_state + (static_cast<size_t>(gene) * 2 + ((req.flags & kWarmBuffer) ? 0 : 1)) * warm_stride
+                : nullptr;
+  if (tid < NB) sm.beta[tid] = warm_read ? __ldcg(warm_src + tid) : req.beta[tid];
+  for (int s = tid; s < K; s += blockDim.x) sm.log_w[s] = warm_read ? __ldcg(warm_src + NB + s) : 0.0;
   for (int i = tid; i <= kRanges; i += blockDim.x)
     sm.rpos[i] = d.range_pos[static_cast<size_t>(gene) * (kRanges + 1) + i];
   for (int i = tid; i <= K; i += blockDim.x) sm.runs[i] = d.runs[static_cast<size_t>(gene) * (K + 1) + i];
@@ -627,7 +634,11 @@ __device__ void fit_one(const GeneData& d, const FitControl& ctl, Smem<NB>& sm, 
 
   for (;;) {
     const double step = sm.sc[kStep];
-    const bool go = step == 0.0 || (sm.sc[kLikdif] > ctl.eps && step < static_cast<double>(ctl.max_iter));
+    // A warm-started fit takes at least two Newton steps: the log-determinant
+    // comes from the previous iterate's vw (pml.rs:1767-1777), which after a
+    // single step would still be the stored start.
+    const double min_steps = warm_read ? 2.0 : 1.0;
+    const bool go = step < min_steps || (sm.sc[kLikdif] > ctl.eps && step < static_cast<double>(ctl.max_iter));
     __syncthreads();
     if (!go) break;
     SweepView<NB> c(sm.sw[cur], K);
@@ -789,6 +800,11 @@ __device__ void fit_one(const GeneData& d, const FitControl& ctl, Smem<NB>& sm, 
     __syncthreads();
   }
   if (cl.rank != 0) return;  // rank 0 of the cluster writes the result
+  if (d.warm_state && (req.flags & kWarmWrite)) {
+    double* dst = d.warm_state + (static_cast<size_t>(gene) * 2 + ((req.flags & kWarmBuffer) ? 1 : 0)) * warm_stride;
+    if (tid < NB) __stcg(dst + tid, sm.beta[tid]);
+    for (int s = tid; s < K; s += blockDim.x) __stcg(dst + NB + s, sm.log_w[s]);
+  }
   if (tid < NB) out->beta[tid] = sm.beta[tid];
   for (int i = tid; i < NB * NB; i += blockDim.x) out->information[i] = sm.vb2[i];
   if (tid == 0) {

@@ -11,7 +11,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
+#include <cmath>
 #include <chrono>
 #include <cstring>
 #include <limits>
@@ -25,6 +27,7 @@
 #include "export.hpp"
 #include "search.hpp"
 #include "stage_one.hpp"
+#include "warm_start.hpp"
 
 namespace nebula {
 namespace {
@@ -143,6 +146,14 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
   data_.n_cells = static_cast<int32_t>(sh.n_cells);
   data_.n_subjects = K;
   data_.n_coef = sh.n_coef;
+  {
+    // per gene two (beta, log_w) slots for warm inner starts
+    double* warm = nullptr;
+    const size_t doubles = std::max<size_t>(G, 1) * 2 * static_cast<size_t>(sh.n_coef + K);
+    cuda_check(cudaMalloc(reinterpret_cast<void**>(&warm), doubles * sizeof(double)), "cudaMalloc");
+    owned_.push_back(warm);
+    data_.warm_state = warm;
+  }
   ctl_.eps = sh.params.eps;
   ctl_.max_iter = kPmlMaxIter;
   ctl_.max_backtrack = kPmlMaxBacktrack;
@@ -714,6 +725,48 @@ std::unique_ptr<Session> create_session(const nb_csr* counts, const uint64_t* su
   return ss;
 }
 
+// Starts of the warm-started searches: the caller's points (warm_start 2) or
+// the network's prediction from the genes' features (warm_start 1), with the
+// network's log evaluation budget; a non-finite or non-positive start falls
+// back to stage one's.
+void warm_starts(Session& ss, std::vector<std::array<double, 2>>* point, std::vector<double>* budget) {
+  const Shared& sh = ss.prep.shared;
+  const size_t G = ss.genes.size();
+  const int K = sh.n_subjects;
+  for (size_t g = 0; g < G; ++g) (*point)[g] = {ss.plans[g].sigma, ss.plans[g].gamma};
+  auto accept = [&](size_t g, double sigma, double gamma) {
+    if (std::isfinite(sigma) && sigma > 0.0) (*point)[g][0] = sigma;
+    if (std::isfinite(gamma) && gamma > 0.0) (*point)[g][1] = gamma;
+  };
+  if (ss.opt.warm_start == 3) return;  // stage one's starts, warm inner fits only
+  if (ss.opt.warm_start == 2) {
+    if (!ss.opt.warm_points) fail(NB_ERR_INVALID_ARGUMENT, "warm_start 2 needs warm_points");
+    for (size_t g = 0; g < G; ++g) {
+      const size_t in = ss.prep.kept[g];
+      accept(g, ss.opt.warm_points[2 * in], ss.opt.warm_points[2 * in + 1]);
+    }
+    return;
+  }
+  std::vector<float> features(G * mlp::kIn), y(G * mlp::kOut);
+  parallel_for(G, ss.opt.host_threads, [&](size_t g) {
+    warm_features(sh, ss.genes[g], &ss.prep.totals[ss.prep.kept[g] * K], ss.plans[g], &features[g * mlp::kIn]);
+  });
+  const float* params = ss.opt.mlp_weights ? ss.opt.mlp_weights : builtin_mlp_params();
+  char err[256] = {};
+  const int32_t rc = nb_mlp_predict_cuda(params, features.data(), G, y.data(), err, sizeof(err));
+  if (rc != NB_OK) fail(rc, std::string("warm-start network: ") + err);
+  // Corrections smaller than about twice the network's held-out error
+  // (log-ratio 0.07) are dropped: stage one's start is then as good.
+  constexpr double kGate = 0.07;
+  auto gate = [&](double d) { return std::fabs(d) > kGate ? std::clamp(d, -10.0, 10.0) : 0.0; };
+  for (size_t g = 0; g < G; ++g) {
+    const double d0 = gate(static_cast<double>(y[g * mlp::kOut + 0]));
+    const double d1 = gate(static_cast<double>(y[g * mlp::kOut + 1]));
+    accept(g, ss.plans[g].sigma * std::exp(d0), ss.plans[g].gamma * std::exp(d1));
+    (*budget)[g] = y[g * mlp::kOut + 2];
+  }
+}
+
 // Stages two and three on the resident data, into `out`.
 void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
   const Shared& sh = ss.prep.shared;
@@ -729,7 +782,34 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
   // reference's search. The genes are dealt to host worker threads, each of
   // which builds its genes' searches and steps them.
   auto t2 = Clock::now();
-  std::vector<GeneTask> tasks(G);
+  // Warm start (nb_options.warm_start): each search starts from a predicted
+  // or given point; an audit sample of the genes also runs cold (a twin task
+  // G + a for gene audit_of[a]) and keeps the cold result where the warm
+  // search's best objective is worse.
+  const int warm = (ss.opt.warm_start >= 1 && ss.opt.warm_start <= 3) ? ss.opt.warm_start : 0;
+  std::vector<std::array<double, 2>> warm_point(G);
+  std::vector<double> budget(G, 0.0);
+  if (warm) warm_starts(ss, &warm_point, &budget);
+  std::vector<size_t> audit_of;
+  std::vector<long long> twin(G, -1);
+  if (warm) {
+    const uint32_t share = static_cast<uint32_t>(std::clamp(ss.opt.audit_percent, 0, 100));
+    for (size_t g = 0; g < G; ++g) {
+      const uint32_t h = static_cast<uint32_t>((static_cast<uint64_t>(g) * 2654435761ULL) >> 7) % 100u;
+      if (ss.plans[g].refit != Refit::None && h < share) {
+        twin[g] = static_cast<long long>(G + audit_of.size());
+        audit_of.push_back(g);
+      }
+    }
+  }
+  const size_t T = G + audit_of.size();
+  auto gene_of = [&](size_t v) { return v < G ? v : audit_of[v - G]; };
+  std::vector<GeneTask> tasks(T);
+  std::vector<int> evaluations(G, 0);
+  std::vector<char> warm_done(G, 0), cold_done(G, 0), parked(T, 0);
+  std::vector<double> warm_best(G), cold_best(G);
+  std::vector<std::optional<std::optional<std::pair<std::vector<double>, bool>>>> cold_refit(G);
+  std::atomic<uint64_t> refit_cold{0};
   struct Slot {
     double subject, cell;
     int ticket;  // index into the gene's tickets, -1 when the point is outside the domain
@@ -738,8 +818,16 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
     std::vector<long long> tickets;
     std::vector<Slot> slots;
     bool final_fit = false;
+    int anchor = -1;  // warm start: index of the ticket whose iterate is stored
   };
-  std::vector<Flight> flight(G);
+  // Warm inner starts (warm mode, searched genes, not the audit twins): the
+  // first point of each step of a gene's search stores its final (beta,
+  // log_w) in slot (step & 1); every point of the next step starts its
+  // Newton loop there instead of at (beta_start, 0). A step reads only the
+  // slot the previous step wrote, so concurrent points never race.
+  std::vector<int> wstep(G, 0);
+  std::vector<std::array<char, 2>> wvalid(G, std::array<char, 2>{0, 0});
+  std::vector<Flight> flight(T);
   std::vector<double> sigma(G), gamma(G);
   std::vector<int> conv(G);
   std::vector<FinalFit> finals(G);
@@ -749,11 +837,16 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
     std::vector<device::FitRequest> reqs;
     std::vector<std::pair<size_t, size_t>> owners;
   };
-  auto plan_points = [&](size_t g, Outbox* box) {
-    GeneTask& t = tasks[g];
-    Flight& f = flight[g];
+  auto plan_points = [&](size_t v, Outbox* box) {
+    const size_t g = gene_of(v);
+    GeneTask& t = tasks[v];
+    Flight& f = flight[v];
     f.slots.clear();
     f.tickets.clear();
+    f.anchor = -1;
+    const bool inner_warm = warm && v < G;
+    const int wb = wstep[g] & 1;
+    const bool can_read = inner_warm && wvalid[g][1 - wb];
     for (const auto& point : t.search->ask()) {
       double subject = 0.0, cell = 0.0;
       std::vector<double> beta;
@@ -766,8 +859,15 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
         r.subject = subject;
         r.cell = cell;
         for (int j = 0; j < sh.n_coef; ++j) r.beta[j] = beta[j];
+        if (inner_warm) {
+          r.flags = (wb ? device::kWarmBuffer : 0) | (can_read ? device::kWarmRead : 0);
+          if (f.anchor < 0) {
+            r.flags |= device::kWarmWrite;
+            f.anchor = static_cast<int>(f.tickets.size());
+          }
+        }
         slot = Slot{subject, cell, static_cast<int>(f.tickets.size())};
-        box->owners.emplace_back(g, f.tickets.size());
+        box->owners.emplace_back(v, f.tickets.size());
         box->reqs.push_back(r);
         f.tickets.push_back(-1);
       }
@@ -812,27 +912,38 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
       DeviceFitter::Tally* tally = &tallies[w];
       Outbox box;
       std::vector<size_t> waiting;
-      for (size_t g = static_cast<size_t>(w); g < G; g += static_cast<size_t>(workers)) {
-        GeneTask& t = tasks[g];
+      std::vector<size_t> mine;
+      for (size_t g = static_cast<size_t>(w); g < G; g += static_cast<size_t>(workers)) mine.push_back(g);
+      if (warm == 1)  // the searches predicted to take longest first
+        std::stable_sort(mine.begin(), mine.end(), [&](size_t a, size_t b) { return budget[a] > budget[b]; });
+      auto start_search = [&](size_t v, bool use_warm) {
+        const size_t g = gene_of(v);
         const GenePlan& plan = ss.plans[g];
-        if (plan.refit != Refit::None) {
-          std::optional<double> fixed_cell;
-          std::vector<double> start;
-          if (plan.refit == Refit::Both) {
-            start = {plan.sigma, plan.gamma};
-          } else {
-            start = {plan.sigma};
-            fixed_cell = plan.gamma;
-          }
-          std::vector<double> lower, upper;
-          variance_bounds(sh.params, fixed_cell.has_value(), &lower, &upper);
-          t.search = std::make_unique<StageTwoSearch>(start, lower, upper, plan.ord);
-          t.objective = VarianceObjective::make(sh, ss.genes[g], fixed_cell);
-          plan_points(g, &box);
+        std::optional<double> fixed_cell;
+        std::vector<double> start;
+        if (plan.refit == Refit::Both) {
+          start = {plan.sigma, plan.gamma};
+          if (use_warm) start = {warm_point[g][0], warm_point[g][1]};
+        } else {
+          start = {use_warm ? warm_point[g][0] : plan.sigma};
+          fixed_cell = plan.gamma;
+        }
+        std::vector<double> lower, upper;
+        variance_bounds(sh.params, fixed_cell.has_value(), &lower, &upper);
+        for (size_t d = 0; d < start.size(); ++d) start[d] = std::clamp(start[d], lower[d], upper[d]);
+        tasks[v].search = std::make_unique<StageTwoSearch>(start, lower, upper, plan.ord);
+        tasks[v].objective = VarianceObjective::make(sh, ss.genes[g], fixed_cell);
+        plan_points(v, &box);
+        waiting.push_back(v);
+      };
+      for (size_t g : mine) {
+        if (ss.plans[g].refit != Refit::None) {
+          start_search(g, warm != 0);
+          if (twin[g] >= 0) start_search(static_cast<size_t>(twin[g]), false);
         } else {
           plan_final(g, &box);
+          waiting.push_back(g);
         }
-        waiting.push_back(g);
         if (box.reqs.size() >= 64) post(&box, w, tally);
       }
       post(&box, w, tally);
@@ -841,6 +952,10 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
         bool progressed = false;
         for (size_t i = 0; i < waiting.size();) {
           const size_t g = waiting[i];
+          if (parked[g]) {
+            ++i;
+            continue;
+          }
           Flight& f = flight[g];
           bool ready = true;
           for (size_t k = f.tickets.size(); k > 0 && ready; --k) ready = fitter.queue_done(f.tickets[k - 1]);
@@ -868,22 +983,57 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
             continue;
           }
           GeneTask& t = tasks[g];
+          const size_t gene = gene_of(g);
           std::vector<double> values(f.slots.size(), std::numeric_limits<double>::infinity());
           for (size_t p = 0; p < f.slots.size(); ++p) {
             const Slot& sl = f.slots[p];
             if (sl.ticket < 0) continue;
             const long long ticket = f.tickets[static_cast<size_t>(sl.ticket)];
-            fitter.queue_account(ticket, static_cast<int>(g), tally);
+            fitter.queue_account(ticket, static_cast<int>(gene), tally);
             const device::FitResult& r = fitter.queue_result(ticket);
             if (r.status != 0) continue;
             InnerFit fit{r.log_likelihood, r.log_likelihood_prev, r.log_det, r.second_order};
             values[p] = t.objective.assemble(sl.subject, sl.cell, fit, t.objective.tail(sl.cell));
           }
+          if (warm && g < G) {
+            const int wb = wstep[g] & 1;
+            wvalid[g][wb] = f.anchor >= 0 && fitter.queue_result(f.tickets[static_cast<size_t>(f.anchor)]).status == 0;
+            ++wstep[g];
+          }
           t.search->tell(values);
           if (t.search->done()) {
             t.refit = t.search->result();
+            const double best = t.search->best_value();
+            if (g < G) evaluations[g] = t.search->evaluations();
             t.search.reset();
-            plan_final(g, &box);
+            // the audit: both searches of a twinned gene must be done
+            auto decide_and_finish = [&](size_t h) {
+              const bool warm_ok = tasks[h].refit.has_value() && tasks[h].refit->has_value();
+              const bool cold_ok = cold_refit[h].has_value() && cold_refit[h]->has_value();
+              if (cold_ok && (!warm_ok || cold_best[h] < warm_best[h] - 1e-9 * std::fabs(cold_best[h]))) {
+                tasks[h].refit = cold_refit[h];
+                refit_cold.fetch_add(1);
+              }
+              parked[h] = 0;
+              plan_final(h, &box);
+            };
+            if (g >= G) {  // a cold twin
+              cold_refit[gene] = t.refit;
+              cold_best[gene] = best;
+              cold_done[gene] = 1;
+              waiting[i] = waiting.back();
+              waiting.pop_back();
+              if (warm_done[gene]) decide_and_finish(gene);
+              continue;
+            }
+            warm_best[g] = best;
+            warm_done[g] = 1;
+            if (twin[g] < 0 || cold_done[g]) {
+              if (twin[g] < 0) plan_final(g, &box);
+              else decide_and_finish(g);
+            } else {
+              parked[g] = 1;  // waits for its cold twin
+            }
           } else {
             plan_points(g, &box);
           }
@@ -928,6 +1078,8 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
   auto t3 = Clock::now();
   std::vector<GeneOutcome> outcomes(G);
   for (size_t g = 0; g < G; ++g) outcomes[g] = finish_gene(sh, sigma[g], gamma[g], conv[g], finals[g]);
+  if (ss.opt.evaluations)
+    for (size_t g = 0; g < G; ++g) ss.opt.evaluations[g] = evaluations[g];
   const double ms_stage_three = ms_since(t3);
   const double ms_step = fitter.end_step();
   record_cluster(ss, cluster, ms_step);
@@ -940,6 +1092,8 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
     stats->fit_slots = static_cast<uint64_t>(fitter.grid());
     stats->slot_cycles = fitter.slot_cycles();
     stats->cluster = static_cast<uint64_t>(cluster);
+    stats->audited = audit_of.size();
+    stats->refit_cold = refit_cold.load();
     stats->gpu_launches = fitter.launches();
     stats->ms_prepare = ss.ms_prepare;
     stats->ms_stage_one = ss.ms_stage_one;
@@ -988,6 +1142,31 @@ NB_API int32_t nb_session_create(const nb_csr* counts, const uint64_t* subject_i
     auto s = std::make_unique<nb_session>();
     s->impl = nebula::create_session(counts, subject_id, design, n_coef, offset_or_null, params_or_null, options);
     *out = s.release();
+    return NB_OK;
+  } catch (const nebula::NbError& e) {
+    nebula::write_err(err, err_len, e.message);
+    return e.code;
+  }
+}
+
+NB_API int32_t nb_session_features(nb_session* session, float* features, double* stage_one, uint64_t* n_kept,
+                                   char* err, size_t err_len) {
+  try {
+    if (!session || !session->impl) nebula::fail(NB_ERR_INVALID_ARGUMENT, "null session");
+    nebula::Session& ss = *session->impl;
+    const nebula::Shared& sh = ss.prep.shared;
+    const size_t G = ss.genes.size();
+    const int K = sh.n_subjects;
+    if (n_kept) *n_kept = G;
+    for (size_t g = 0; g < G; ++g) {
+      if (features)
+        nebula::warm_features(sh, ss.genes[g], &ss.prep.totals[ss.prep.kept[g] * K], ss.plans[g],
+                              features + g * nebula::mlp::kIn);
+      if (stage_one) {
+        stage_one[2 * g] = ss.plans[g].sigma;
+        stage_one[2 * g + 1] = ss.plans[g].gamma;
+      }
+    }
     return NB_OK;
   } catch (const nebula::NbError& e) {
     nebula::write_err(err, err_len, e.message);

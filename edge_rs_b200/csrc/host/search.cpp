@@ -381,8 +381,10 @@ std::optional<std::vector<double>> StageTwoSearch::fit_polish(const std::vector<
 
 void StageTwoSearch::tell(const std::vector<double>& values) {
   evaluations_ += static_cast<int>(values.size());
-  for (double v : values)
+  for (double v : values) {
     if (!std::isfinite(v)) invalid_ = true;
+    else if (v < best_value_) best_value_ = v;
+  }
   switch (stage_) {
     case Stage::Start:
       if (!std::isfinite(values[0])) {

@@ -12,6 +12,7 @@
 
 #include <memory>
 #include <optional>
+#include <limits>
 #include <vector>
 
 #include "bobyqa.hpp"
@@ -40,6 +41,8 @@ class StageTwoSearch {
   // search was abandoned.
   std::optional<std::pair<std::vector<double>, bool>> result() const;
   int evaluations() const { return evaluations_; }
+  // The smallest finite objective value told so far (+inf if none).
+  double best_value() const { return best_value_; }
 
  private:
   enum class Stage { Start, NelderMead, Check, Polish, Bobyqa, Done };
@@ -67,6 +70,7 @@ class StageTwoSearch {
   std::optional<std::pair<std::vector<double>, double>> pinned_;
   bool failed_ = false;
   int evaluations_ = 0;
+  double best_value_ = std::numeric_limits<double>::infinity();
 };
 
 // The profile objective of one gene at one Laplace order

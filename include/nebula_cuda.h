@@ -94,22 +94,45 @@ typedef struct nb_fit {
   uint64_t n_coef;
 } nb_fit;
 
-/* How stage two is started and batched. Zero-initialised = the plain
- * cold-start method the reference runs. */
+/* How stage two is started and run. Zero-initialised = the plain cold-start
+ * method the reference runs, on the current device.
+ *
+ * Warm start (no counterpart in the reference) changes two things, and the
+ * plain optimisers finish every search unchanged:
+ *  - each inner fit of a gene's search after its first step starts its
+ *    Newton loop from the gene's previous iterate (beta, log_w) instead of
+ *    (beta_start, 0), and takes at least two Newton steps;
+ *  - the search itself starts from
+ *      warm_start = 1: the warm-start network's prediction (nb_mlp_predict_cuda)
+ *                      from the gene's summary features, weights
+ *                      `mlp_weights` (NB_MLP_PARAMS floats) or the built-in
+ *                      ones when NULL; genes predicted to need the most
+ *                      evaluations are posted first;
+ *      warm_start = 2: the caller's starts, warm_points[2 * g], [2 * g + 1]
+ *                      for input gene g (e.g. a previous fit);
+ *      warm_start = 3: stage one's estimate, as the plain method.
+ * Results then differ from the plain method's within the search's
+ * tolerance. A deterministic sample of audit_percent % of the searched
+ * genes also runs plain (cold); where the warm search's best objective is
+ * worse than the cold one's by more than 1e-9 relative, the gene keeps the
+ * cold result (refit_cold). */
 typedef struct nb_options {
   int32_t device;        /* CUDA ordinal; -1 = current device */
-  int32_t warm_start;    /* 1: learned warm start + plain finish (see below) */
-  int32_t host_threads;  /* stage-one host threads; 0 = all cores */
-  int32_t audit_percent; /* warm start only: share of genes refit cold */
-  const float* mlp_weights; /* warm start only: nb_mlp_* layout; NULL = built-in */
+  int32_t warm_start;    /* 0 plain, 1 learned, 2 caller's starts, 3 stage one's */
+  int32_t host_threads;  /* host threads; 0 = all cores */
+  int32_t audit_percent; /* warm start only: share of genes also run cold */
+  const float* mlp_weights; /* warm_start 1: NB_MLP_PARAMS floats; NULL = built-in */
   int32_t cluster;       /* CTAs sharing each inner fit in stages two and three
                             (1, 2, 4 or 8); 0 = chosen per call */
+  const double* warm_points; /* warm_start 2: n_genes x 2 starts (sigma, gamma) */
+  int32_t* evaluations;  /* optional out: stage-two objective evaluations per
+                            kept gene (the kept genes' order of nb_fit) */
 } nb_options;
 
 /* Counters of one call (timings in milliseconds of host wall clock, device
  * times from CUDA events on the launching stream). */
 typedef struct nb_stats {
-  uint64_t rounds;          /* batched stage-two launches */
+  uint64_t rounds;          /* search steps the host took in stages two and three */
   uint64_t requests;        /* inner fits run on the device */
   uint64_t sweeps;          /* cell passes run on the device */
   uint64_t cell_visits;     /* dense + sparse cell visits on the device */
@@ -119,8 +142,9 @@ typedef struct nb_stats {
   double ms_step_device;    /* device time from the first stage-two copy to the
                                last stage-three copy, CUDA events */
   uint64_t h2d_bytes, d2h_bytes; /* host<->device bytes the call moved */
-  uint64_t audited, refit_cold;
-  uint64_t fit_slots;       /* fit-kernel CTAs resident at once (per lane) */
+  uint64_t audited, refit_cold; /* warm start: genes also run cold, and those
+                                    that kept the cold result */
+  uint64_t fit_slots;       /* fit-kernel CTAs resident at once */
   uint64_t slot_cycles;     /* SM clock cycles the fit CTAs spent on requests */
   uint64_t cluster;         /* CTAs that shared each fit in stages two and three */
 } nb_stats;
@@ -205,6 +229,44 @@ int32_t nb_opt_pml_cuda_noalloc(const double* design, const double* offset,
                                 double* beta_out, double* information_out,
                                 double* scalars_out, int32_t* ints_out,
                                 void* stream, char* err, size_t err_len);
+
+/* The warm-start network (no counterpart in the reference): 12 summary
+ * features of a gene -> 64 -> 64 -> 3 (GELU), predicting log(final sigma /
+ * stage-one sigma), log(final gamma / stage-one gamma) and log(stage-two
+ * evaluations). Parameters: NB_MLP_PARAMS floats, laid out W1 [64][12],
+ * b1 [64], W2 [64][64], b2 [64], W3 [3][64], b3 [3], input mean [12], input
+ * scale [12] (inputs enter as (x - mean) * scale; the normalisation is not
+ * trained). Loss: mean over samples of sum_o w_o (y_o - t_o)^2 / 2 with
+ * w = (1, 1, 0.25). The kernels are the project's own; gradients are summed
+ * in a fixed order, so results repeat bit for bit. */
+#define NB_MLP_FEATURES 12
+#define NB_MLP_OUTPUTS 3
+#define NB_MLP_PARAMS 5211
+/* Xavier-uniform weights from `seed`, zero biases, identity normalisation. */
+void nb_mlp_init(uint64_t seed, float* params);
+/* The built-in network warm_start = 1 uses when mlp_weights is NULL. */
+void nb_mlp_builtin(float* params);
+/* out: n x NB_MLP_OUTPUTS predictions for n x NB_MLP_FEATURES features. */
+int32_t nb_mlp_predict_cuda(const float* params, const float* features,
+                            uint64_t n, float* out, char* err, size_t err_len);
+/* The loss over n samples (targets n x NB_MLP_OUTPUTS) and its gradient
+ * (NB_MLP_PARAMS floats; zero for the normalisation entries). */
+int32_t nb_mlp_gradient_cuda(const float* params, const float* features,
+                             const float* targets, uint64_t n, float* grad_out,
+                             double* loss_out, char* err, size_t err_len);
+/* Adam (lr, betas 0.9/0.999) on mini-batches of `batch` rows of a fresh
+ * seeded permutation each epoch, from and into `params`; epoch_loss (may
+ * be NULL) receives each epoch's mean batch loss. Each step's four kernels
+ * run as one captured CUDA graph. */
+int32_t nb_mlp_train_cuda(const float* features, const float* targets,
+                          uint64_t n, int32_t epochs, int32_t batch, float lr,
+                          uint64_t seed, float* params, double* epoch_loss,
+                          char* err, size_t err_len);
+/* A session's kept genes: their NB_MLP_FEATURES features (n_kept rows) and
+ * stage one's (sigma, gamma) (n_kept x 2); either may be NULL. */
+int32_t nb_session_features(nb_session* session, float* features,
+                            double* stage_one, uint64_t* n_kept, char* err,
+                            size_t err_len);
 
 /* glm_sc_test (src/sc/test.rs:96-200): Wald test of the contrast c per gene,
  * z = c'beta / sqrt(c'Vc), p = chisq_sf(z^2, 1), BH FDR. log_p_value keeps

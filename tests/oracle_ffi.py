@@ -76,3 +76,22 @@ def nebula_sparse(counts, subject_id, design, n_coef, offset=None, params=None, 
     if rc != 0:
         raise NebulaError(rc, err.value.decode(errors="replace"))
     return fit_from_arrays(out, n_coef), dict(evaluations=int(work[0]), sweeps=int(work[1]), genes=int(work[2]))
+
+
+def mlp_loss_grad(params, features, targets):
+    """The FP64 oracle's loss and gradient of the warm-start network."""
+    p = np.ascontiguousarray(params, np.float32)
+    x = np.ascontiguousarray(features, np.float32).reshape(-1, 12)
+    t = np.ascontiguousarray(targets, np.float32).reshape(-1, 3)
+    g = np.zeros(p.size)
+    loss = ctypes.c_double(0.0)
+    lib().oracle_mlp_loss_grad(_p(p), _p(x), _p(t), ctypes.c_uint64(x.shape[0]), _p(g), ctypes.byref(loss))
+    return loss.value, g
+
+
+def mlp_predict(params, features):
+    p = np.ascontiguousarray(params, np.float32)
+    x = np.ascontiguousarray(features, np.float32).reshape(-1, 12)
+    out = np.zeros((x.shape[0], 3))
+    lib().oracle_mlp_predict(_p(p), _p(x), ctypes.c_uint64(x.shape[0]), _p(out))
+    return out
