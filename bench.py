@@ -293,7 +293,9 @@ def ours_arm(args, world, rank, local, dist):
                      "peak_source": "measured on this GPU: FP64 FMA chains (nb_measure_fp64_tflops)"},
         "e2e": {"value": float(np.mean(e2e_vals)) if e2e_vals else None, "unit": "genes/s",
                 "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h), "ms_stage_one": e2e_stats["ms_stage_one"],
+                "d2h_bytes_per_step": int(d2h), "ms_total": e2e_stats.get("ms_total"),
+                "ms_prepare": e2e_stats.get("ms_prepare"), "ms_upload": e2e_stats.get("ms_upload"),
+                "ms_stage_one": e2e_stats["ms_stage_one"],
                 "ms_stage_two": e2e_stats["ms_stage_two"], "ms_stage_three": e2e_stats["ms_stage_three"]},
         "gpu_launches": launches,
         "clocks": clocks,

@@ -1096,6 +1096,7 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
     stats->refit_cold = refit_cold.load();
     stats->gpu_launches = fitter.launches();
     stats->ms_prepare = ss.ms_prepare;
+    stats->ms_upload = ss.ms_upload;
     stats->ms_stage_one = ss.ms_stage_one;
     stats->ms_stage_two = ms_stage_two;
     stats->ms_stage_three = ms_stage_three;

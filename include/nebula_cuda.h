@@ -147,6 +147,7 @@ typedef struct nb_stats {
   uint64_t fit_slots;       /* fit-kernel CTAs resident at once */
   uint64_t slot_cycles;     /* SM clock cycles the fit CTAs spent on requests */
   uint64_t cluster;         /* CTAs that shared each fit in stages two and three */
+  double ms_upload;         /* host wall time of the device upload */
 } nb_stats;
 
 void nb_params_default(nb_params* params);
