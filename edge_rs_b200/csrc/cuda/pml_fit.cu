@@ -1,21 +1,22 @@
 // Batched penalised NB-gamma inner fit (the reference's opt_pml,
 // src/sc/pml.rs:1614-1800) on sm_100a, FP64 throughout.
 //
-// One persistent CTA per SM slot pulls (gene, sigma, gamma) requests off an
-// atomic work queue and runs the whole Newton loop for each: sweep, Schur
-// complement, pivoted LDL' solve, backtracking, log-determinant and the
-// higher-order Laplace pass.
+// fit_one runs the whole Newton loop of one (gene, sigma, gamma) request:
+// sweep, Schur complement, pivoted LDL' solve, backtracking, log-determinant
+// and the higher-order Laplace pass. Two kernels drive it: fit_kernel (batch:
+// persistent clusters over an atomic counter of a request array) and
+// fit_queue_kernel (one persistent launch per call, fed by the host through
+// a device ring of requests with per-slot sequence numbers). Either runs a
+// request on a cluster of 1, 2, 4 or 8 CTAs that share its sweeps.
 //
 // A sweep (pml.rs:1419-1590) splits each subject into a dense part over every
 // cell at a count of zero and a sparse part over the gene's positive counts.
-// Dense pass: the cells are cut into kWarps contiguous ranges, one per warp;
-// lanes stride a range subject by subject, accumulating the per-subject sums
-// in registers, and each (warp, subject) piece is warp-reduced into its own
-// shared-memory slot (slot index subject + warp is unique because both
-// advance together). Sparse pass: warp w takes the subjects s = w mod kWarps
-// and strides their positive entries. A combine step then sums, per subject
-// and in a fixed order, the slots of the warps that touched it; no atomics,
-// so results are bitwise reproducible run to run.
+// The cells are cut into kRanges fixed ranges; each subject segment of a
+// range is one piece, summed by a warp's lanes over its cells and then its
+// positive entries and butterfly-reduced into a shared-memory slot; a combine
+// step sums each subject's pieces in range order, reading other CTAs' pieces
+// through distributed shared memory. No atomics, and the tree does not depend
+// on the launch shape, so results are bitwise reproducible.
 //
 // The per-request scalars (Newton state, step sizes, loop flags) live in
 // shared memory and are written by thread 0 between barriers, so every
