@@ -91,13 +91,16 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
   std::vector<uint64_t> gene_ptr(G + 1, 0);
   for (size_t g = 0; g < G; ++g) gene_ptr[g + 1] = gene_ptr[g] + genes[g].cells.size();
   const size_t nnz = gene_ptr[G];
-  std::vector<uint32_t> cells(nnz);
-  std::vector<double> counts(nnz), totals(G * K);
+  // the kept genes' entries, concatenated on all host threads (the buffers
+  // are left uninitialised: every element is written once)
+  std::unique_ptr<uint32_t[]> cells(new uint32_t[std::max<size_t>(nnz, 1)]);
+  std::unique_ptr<double[]> counts(new double[std::max<size_t>(nnz, 1)]);
+  std::vector<double> totals(G * K);
   std::vector<uint64_t> runs(G * (K + 1));
-  for (size_t g = 0; g < G; ++g) {
+  parallel_for(G, 0, [&](size_t g) {
     const GeneCounts& gc = genes[g];
-    std::copy(gc.cells.begin(), gc.cells.end(), cells.begin() + gene_ptr[g]);
-    std::copy(gc.counts.begin(), gc.counts.end(), counts.begin() + gene_ptr[g]);
+    std::copy(gc.cells.begin(), gc.cells.end(), cells.get() + gene_ptr[g]);
+    std::copy(gc.counts.begin(), gc.counts.end(), counts.get() + gene_ptr[g]);
     std::copy(prep.totals.begin() + prep.kept[g] * K, prep.totals.begin() + (prep.kept[g] + 1) * K,
               totals.begin() + g * K);
     // positive_runs (pml.rs:1155-1160) as absolute positions
@@ -107,7 +110,7 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
                                  [](uint32_t c, uint64_t v) { return c < v; });
       runs[g * (K + 1) + s] = gene_ptr[g] + static_cast<uint64_t>(it - gc.cells.begin());
     }
-  }
+  });
   gene_nnz_.resize(G);
   for (size_t g = 0; g < G; ++g) gene_nnz_[g] = genes[g].cells.size();
   n_cells_ = sh.n_cells;
@@ -133,15 +136,15 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
   data_.log_offset = device_copy(sh.log_offset.data(), sh.log_offset.size(), &owned_);
   data_.fid = device_copy(fid.data(), fid.size(), &owned_);
   data_.gene_ptr = device_copy(gene_ptr.data(), gene_ptr.size(), &owned_);
-  data_.cells = device_copy(cells.data(), cells.size(), &owned_);
-  data_.counts = device_copy(counts.data(), counts.size(), &owned_);
+  data_.cells = device_copy(cells.get(), nnz, &owned_);
+  data_.counts = device_copy(counts.get(), nnz, &owned_);
   data_.runs = device_copy(runs.data(), runs.size(), &owned_);
   data_.totals = device_copy(totals.data(), totals.size(), &owned_);
   data_.warp_cells = device_copy(wcells.data(), wcells.size(), &owned_);
   data_.range_cells = device_copy(rcells.data(), rcells.size(), &owned_);
   data_.range_pos = device_copy(rpos.data(), rpos.size(), &owned_);
-  h2d_bytes_ = (sh.design.size() + sh.log_offset.size() + counts.size() + totals.size()) * sizeof(double) +
-               (fid.size() + cells.size() + wcells.size() + rcells.size()) * sizeof(uint32_t) +
+  h2d_bytes_ = (sh.design.size() + sh.log_offset.size() + nnz + totals.size()) * sizeof(double) +
+               (fid.size() + nnz + wcells.size() + rcells.size()) * sizeof(uint32_t) +
                (gene_ptr.size() + runs.size() + rpos.size()) * sizeof(uint64_t);
   data_.n_cells = static_cast<int32_t>(sh.n_cells);
   data_.n_subjects = K;
