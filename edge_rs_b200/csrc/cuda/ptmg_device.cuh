@@ -27,5 +27,24 @@ size_t ptmg_scratch_doubles(int n_subjects, int n_coef);  // per CTA
 int launch_ptmg(const GeneData& d, const PtmgRequest* req, double* results, double* scratch,
                 const int32_t* n_requests, int32_t* counter, int grid, void* stream);
 
+// Streaming mode for stage one: the request-ring protocol of FitQueue
+// (pml_device.cuh) with PtmgRequests and results of result_stride doubles
+// each in host-mapped memory; one CTA per request, `grid` CTAs each owning
+// its row of `scratch`.
+struct PtmgQueue {
+  const PtmgRequest* ring;
+  const long long* seq;
+  const int* stop;
+  unsigned long long* taken;
+  double* results;
+  long long result_stride;
+  long long* done;
+  int* status;
+  long long mask;
+  long long idle_ns;
+};
+
+int launch_ptmg_queue(const GeneData& d, const PtmgQueue& queue, double* scratch, int grid, void* stream);
+
 }  // namespace device
 }  // namespace nebula

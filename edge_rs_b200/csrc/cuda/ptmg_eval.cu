@@ -211,6 +211,52 @@ __device__ void tree_pass(const GeneData& d, const uint32_t* fid, const uint32_t
   __syncthreads();
 }
 
+// Shared-memory and scratch views of one stage-one CTA.
+struct PtmgCta {
+  double* ym;        // K
+  double* p1;        // K x 2: cumsumxtb, ylin
+  uint32_t* fid;     // K + 1
+  uint32_t* wcells;  // kWarps + 1
+  double* slots;     // this CTA's scratch rows
+};
+
+template <int NB>
+__device__ PtmgCta ptmg_setup(const GeneData& d, double* smem, double* scratch) {
+  using D = PDims<NB>;
+  const int K = d.n_subjects;
+  PtmgCta c;
+  c.ym = smem;
+  c.p1 = c.ym + K;
+  c.fid = reinterpret_cast<uint32_t*>(c.p1 + 2 * K);
+  c.wcells = c.fid + K + 1;
+  for (int i = threadIdx.x; i <= K; i += blockDim.x) c.fid[i] = d.fid[i];
+  if (threadIdx.x <= kWarps) c.wcells[threadIdx.x] = d.warp_cells[threadIdx.x];
+  c.slots = scratch + static_cast<size_t>(blockIdx.x) * (2 * K + kWarps) * D::W;
+  return c;
+}
+
+// Both passes of one request into `out` ((2 + W) K doubles).
+template <int NB>
+__device__ void ptmg_one(const GeneData& d, const PtmgCta& c, const PtmgRequest& req, double* beta_sm, double* out) {
+  using D = PDims<NB>;
+  const int K = d.n_subjects;
+  const int tid = threadIdx.x;
+  if (tid < NB) beta_sm[tid] = req.beta[tid];
+  __syncthreads();
+  double beta[NB];
+#pragma unroll
+  for (int j = 0; j < NB; ++j) beta[j] = beta_sm[j];
+  tree_pass<NB, 1, 2>(d, c.fid, c.wcells, req.gene, beta, c.ym, req.gamma, c.slots, D::W, c.p1, 2);
+  const double* tot = d.totals + static_cast<size_t>(req.gene) * K;
+  for (int s = tid; s < K; s += blockDim.x) {
+    c.ym[s] = (__ldg(tot + s) + req.alpha) / (c.p1[2 * s] + req.lambda);
+    out[s] = c.p1[2 * s];          // cumsumxtb
+    out[K + s] = c.p1[2 * s + 1];  // ylin
+  }
+  __syncthreads();
+  tree_pass<NB, 2, D::W>(d, c.fid, c.wcells, req.gene, beta, c.ym, req.gamma, c.slots, D::W, out + 2 * K, D::W);
+}
+
 template <int NB>
 __global__ void __launch_bounds__(kThreads, 1) ptmg_kernel(GeneData d, const PtmgRequest* __restrict__ requests,
                                                            double* __restrict__ results,
@@ -219,41 +265,75 @@ __global__ void __launch_bounds__(kThreads, 1) ptmg_kernel(GeneData d, const Ptm
                                                            int32_t* __restrict__ counter) {
   using D = PDims<NB>;
   extern __shared__ __align__(16) double smem[];
-  const int K = d.n_subjects;
-  double* ym = smem;                                        // K
-  double* p1 = ym + K;                                      // K x 2: cumsumxtb, ylin
-  uint32_t* fid = reinterpret_cast<uint32_t*>(p1 + 2 * K);  // K + 1
-  uint32_t* wcells = fid + K + 1;                           // kWarps + 1
+  const PtmgCta c = ptmg_setup<NB>(d, smem, scratch);
   __shared__ int next_req;
   __shared__ double beta_sm[kMaxCoef];
-  const int tid = threadIdx.x;
-  for (int i = tid; i <= K; i += blockDim.x) fid[i] = d.fid[i];
-  if (tid <= kWarps) wcells[tid] = d.warp_cells[tid];
-  double* slots = scratch + static_cast<size_t>(blockIdx.x) * (2 * K + kWarps) * D::W;
   const int total = *n_requests;
-  const size_t out_stride = static_cast<size_t>(2 + D::W) * K;
+  const size_t out_stride = static_cast<size_t>(2 + D::W) * d.n_subjects;
   for (;;) {
     __syncthreads();
-    if (tid == 0) next_req = atomicAdd(counter, 1);
+    if (threadIdx.x == 0) next_req = atomicAdd(counter, 1);
     __syncthreads();
     const int q = next_req;
     if (q >= total) break;
     const PtmgRequest req = requests[q];
-    if (tid < NB) beta_sm[tid] = req.beta[tid];
+    ptmg_one<NB>(d, c, req, beta_sm, results + static_cast<size_t>(q) * out_stride);
+  }
+}
+
+__device__ __forceinline__ long long global_ns() {
+  long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Streaming mode: one persistent launch for stage one, the request-ring
+// protocol of FitQueue (pml_device.cuh) with one CTA per request.
+template <int NB>
+__global__ void __launch_bounds__(kThreads, 1) ptmg_queue_kernel(GeneData d, PtmgQueue qu, double* scratch) {
+  extern __shared__ __align__(16) double smem[];
+  const PtmgCta c = ptmg_setup<NB>(d, smem, scratch);
+  __shared__ long long next_ticket;
+  __shared__ double beta_sm[kMaxCoef];
+  for (;;) {
     __syncthreads();
-    double beta[NB];
-#pragma unroll
-    for (int j = 0; j < NB; ++j) beta[j] = beta_sm[j];
-    double* out = results + static_cast<size_t>(q) * out_stride;
-    tree_pass<NB, 1, 2>(d, fid, wcells, req.gene, beta, ym, req.gamma, slots, D::W, p1, 2);
-    const double* tot = d.totals + static_cast<size_t>(req.gene) * K;
-    for (int s = tid; s < K; s += blockDim.x) {
-      ym[s] = (__ldg(tot + s) + req.alpha) / (p1[2 * s] + req.lambda);
-      out[s] = p1[2 * s];          // cumsumxtb
-      out[K + s] = p1[2 * s + 1];  // ylin
+    if (threadIdx.x == 0) {
+      const long long t = static_cast<long long>(atomicAdd(qu.taken, 1ull));
+      const volatile long long* seq = qu.seq + (t & qu.mask);
+      const volatile int* stop = qu.stop;
+      const long long t0 = global_ns();
+      unsigned int pause = 128;
+      long long got = -1;
+      for (;;) {
+        if (*seq == t) {
+          got = t;
+          break;
+        }
+        if (*stop != 0) break;
+        if (global_ns() - t0 > qu.idle_ns) {
+          atomicExch(qu.status, 1);
+          break;
+        }
+        __nanosleep(pause);
+        if (pause < 2048) pause *= 2;
+      }
+      next_ticket = got;
     }
     __syncthreads();
-    tree_pass<NB, 2, D::W>(d, fid, wcells, req.gene, beta, ym, req.gamma, slots, D::W, out + 2 * K, D::W);
+    const long long t = next_ticket;
+    if (t < 0) break;
+    PtmgRequest req;
+    {
+      const int4* src = reinterpret_cast<const int4*>(qu.ring + (t & qu.mask));
+      int4* dst = reinterpret_cast<int4*>(&req);
+#pragma unroll
+      for (int i = 0; i < static_cast<int>(sizeof(PtmgRequest) / 16); ++i) dst[i] = __ldcg(src + i);
+    }
+    ptmg_one<NB>(d, c, req, beta_sm, qu.results + (t & qu.mask) * qu.result_stride);
+    // every thread's result writes reach host memory before the flag
+    __threadfence_system();
+    __syncthreads();
+    if (threadIdx.x == 0) reinterpret_cast<volatile long long*>(qu.done)[t & qu.mask] = t + 1;
   }
 }
 
@@ -268,7 +348,32 @@ int launch_nb(const GeneData& d, const PtmgRequest* req, double* res, double* sc
   return cudaGetLastError();
 }
 
+template <int NB>
+int launch_queue_nb(const GeneData& d, const PtmgQueue& qu, double* scratch, int grid, cudaStream_t stream) {
+  const size_t smem = ptmg_smem_bytes(d.n_subjects);
+  cudaError_t e = cudaFuncSetAttribute(ptmg_queue_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  ptmg_queue_kernel<NB><<<grid, kThreads, smem, stream>>>(d, qu, scratch);
+  return cudaGetLastError();
+}
+
 }  // namespace
+
+int launch_ptmg_queue(const GeneData& d, const PtmgQueue& queue, double* scratch, int grid, void* stream) {
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  switch (d.n_coef) {
+    case 1: return launch_queue_nb<1>(d, queue, scratch, grid, s);
+    case 2: return launch_queue_nb<2>(d, queue, scratch, grid, s);
+    case 3: return launch_queue_nb<3>(d, queue, scratch, grid, s);
+    case 4: return launch_queue_nb<4>(d, queue, scratch, grid, s);
+    case 5: return launch_queue_nb<5>(d, queue, scratch, grid, s);
+    case 6: return launch_queue_nb<6>(d, queue, scratch, grid, s);
+    case 7: return launch_queue_nb<7>(d, queue, scratch, grid, s);
+    case 8: return launch_queue_nb<8>(d, queue, scratch, grid, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
 
 size_t ptmg_smem_bytes(int n_subjects) {
   return static_cast<size_t>(3 * n_subjects) * 8 + (n_subjects + 1 + kWarps + 1) * 4 + 16;

@@ -210,21 +210,62 @@ double DeviceFitter::end_step() {
   return ms;
 }
 
+void DeviceFitter::ensure_ptmg_scratch() {
+  if (d_scratch_) return;
+  const int K = data_.n_subjects;
+  int sms = 0, dev = 0;
+  cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+  cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute");
+  pgrid_ = sms;  // one CTA per SM (the kernel is bound to one resident block)
+  cuda_check(cudaMalloc(reinterpret_cast<void**>(&d_scratch_),
+                        static_cast<size_t>(pgrid_) * device::ptmg_scratch_doubles(K, data_.n_coef) * sizeof(double)),
+             "cudaMalloc");
+  owned_.push_back(d_scratch_);
+}
+
+size_t DeviceFitter::ptmg_stride() const {
+  return static_cast<size_t>(2 + device::ptmg_width_of(data_.n_coef)) * static_cast<size_t>(data_.n_subjects);
+}
+
+void DeviceFitter::ptmg_queue_start(size_t capacity) {
+  ensure_ptmg_scratch();
+  if (!ptmgq_ || ptmgq_->capacity() != capacity)
+    ptmgq_ = std::make_unique<RequestQueue>(sizeof(device::PtmgRequest), ptmg_stride() * sizeof(double), capacity);
+  ptmgq_->start(stream_, [&](const RequestQueue::View& v) {
+    device::PtmgQueue pq{};
+    pq.ring = static_cast<const device::PtmgRequest*>(v.ring);
+    pq.seq = v.seq;
+    pq.stop = v.stop;
+    pq.taken = v.taken;
+    pq.results = static_cast<double*>(v.results);
+    pq.result_stride = static_cast<long long>(ptmg_stride());
+    pq.done = v.done;
+    pq.status = v.status;
+    pq.mask = v.mask;
+    pq.idle_ns = v.idle_ns;
+    return static_cast<cudaError_t>(device::launch_ptmg_queue(data_, pq, d_scratch_, pgrid_, stream_));
+  });
+  ++launches_;
+}
+
+long long DeviceFitter::ptmg_post(const device::PtmgRequest* reqs, size_t n) { return ptmgq_->post(reqs, n); }
+bool DeviceFitter::ptmg_done(long long ticket) const { return ptmgq_->done(ticket); }
+const double* DeviceFitter::ptmg_result(long long ticket) const {
+  return static_cast<const double*>(ptmgq_->result(ticket));
+}
+bool DeviceFitter::ptmg_running() { return ptmgq_->running(); }
+void DeviceFitter::ptmg_stop() { ptmgq_->stop(); }
+void DeviceFitter::ptmg_abort() noexcept {
+  if (ptmgq_) ptmgq_->abort();
+}
+void DeviceFitter::ptmg_failure(const char* what) { ptmgq_->failure(what); }
+
 const double* DeviceFitter::run_ptmg(const std::vector<device::PtmgRequest>& reqs) {
   const size_t n = reqs.size();
   if (n == 0) return nullptr;
   const int K = data_.n_subjects;
   const size_t stride = static_cast<size_t>(2 + device::ptmg_width_of(data_.n_coef)) * K;
-  if (!d_scratch_) {
-    int sms = 0, dev = 0;
-    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
-    cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute");
-    pgrid_ = sms;  // one CTA per SM (the kernel is bound to one resident block)
-    cuda_check(cudaMalloc(reinterpret_cast<void**>(&d_scratch_),
-                          static_cast<size_t>(pgrid_) * device::ptmg_scratch_doubles(K, data_.n_coef) * sizeof(double)),
-               "cudaMalloc");
-    owned_.push_back(d_scratch_);
-  }
+  ensure_ptmg_scratch();
   if (n > pcapacity_) {
     size_t cap = std::max<size_t>(n, pcapacity_ * 2);
     if (d_preq_) cudaFree(d_preq_);
@@ -261,19 +302,8 @@ const double* DeviceFitter::run_ptmg(const std::vector<device::PtmgRequest>& req
 }
 
 DeviceFitter::~DeviceFitter() {
-  queue_abort();
-  for (cudaStream_t st : q_.posters)
-    if (st) cudaStreamSynchronize(st);
-  if (q_.h_ring) cudaFreeHost(q_.h_ring);
-  if (q_.h_seq) cudaFreeHost(q_.h_seq);
-  if (q_.h_one) cudaFreeHost(q_.h_one);
-  if (q_.h_results) cudaFreeHost(q_.h_results);
-  if (q_.h_done) cudaFreeHost(q_.h_done);
-  if (q_.ev0) cudaEventDestroy(q_.ev0);
-  if (q_.ev1) cudaEventDestroy(q_.ev1);
-  if (q_.ready) cudaEventDestroy(q_.ready);
-  for (cudaStream_t st : q_.posters)
-    if (st) cudaStreamDestroy(st);
+  fitq_.abort();
+  ptmg_abort();
   if (d_preq_) cudaFree(d_preq_);
   if (d_pres_) cudaFree(d_pres_);
   if (h_preq_) cudaFreeHost(h_preq_);
@@ -374,11 +404,6 @@ const device::FitResult* DeviceFitter::collect(int lane_index) {
 // ---------------------------------------------------------------------------
 // Streaming mode.
 
-namespace {
-constexpr size_t kQueueCapacity = 16384;      // tickets in the ring (a power of two)
-constexpr long long kQueueIdleNs = 30000000000LL;  // longest wait of a cluster for work: 30 s
-}  // namespace
-
 int DeviceFitter::cluster_for(size_t requests) const {
   // Spread each fit over more CTAs while (a) the fits in flight times the
   // cluster stay within about four times the resident CTA slots, so the
@@ -394,122 +419,36 @@ int DeviceFitter::cluster_for(size_t requests) const {
 }
 
 void DeviceFitter::queue_start(int cluster) {
-  if (q_.running) fail(NB_ERR_GPU, "the work queue is already running");
-  if (!q_.d_ring) {
-    const size_t cap = kQueueCapacity;
-    q_.capacity = cap;
-    cuda_check(cudaEventCreate(&q_.ev0), "event");
-    cuda_check(cudaEventCreate(&q_.ev1), "event");
-    cuda_check(cudaEventCreateWithFlags(&q_.ready, cudaEventDisableTiming), "event");
-    for (cudaStream_t& st : q_.posters)
-      cuda_check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
-    cuda_check(cudaMalloc(reinterpret_cast<void**>(&q_.d_ring), cap * sizeof(device::FitRequest)), "cudaMalloc");
-    owned_.push_back(q_.d_ring);
-    cuda_check(cudaMalloc(reinterpret_cast<void**>(&q_.d_seq), cap * sizeof(long long)), "cudaMalloc");
-    owned_.push_back(q_.d_seq);
-    cuda_check(cudaMalloc(reinterpret_cast<void**>(&q_.d_stop), sizeof(int)), "cudaMalloc");
-    owned_.push_back(q_.d_stop);
-    cuda_check(cudaMalloc(reinterpret_cast<void**>(&q_.d_taken), sizeof(unsigned long long)), "cudaMalloc");
-    owned_.push_back(q_.d_taken);
-    cuda_check(cudaMalloc(reinterpret_cast<void**>(&q_.d_status), sizeof(int)), "cudaMalloc");
-    owned_.push_back(q_.d_status);
-    cuda_check(cudaMallocHost(reinterpret_cast<void**>(&q_.h_ring), cap * sizeof(device::FitRequest)),
-               "cudaMallocHost");
-    cuda_check(cudaMallocHost(reinterpret_cast<void**>(&q_.h_seq), cap * sizeof(long long)), "cudaMallocHost");
-    cuda_check(cudaMallocHost(reinterpret_cast<void**>(&q_.h_one), sizeof(int)), "cudaMallocHost");
-    *q_.h_one = 1;
-    cuda_check(cudaHostAlloc(reinterpret_cast<void**>(&q_.h_results), cap * sizeof(device::FitResult),
-                             cudaHostAllocMapped),
-               "cudaHostAlloc");
-    cuda_check(cudaHostAlloc(reinterpret_cast<void**>(&q_.h_done), cap * sizeof(long long), cudaHostAllocMapped),
-               "cudaHostAlloc");
-  }
   if (cluster < 1 || cluster > device::kMaxCluster || queue_clusters_[cluster] <= 0)
     fail(NB_ERR_GPU, "no resident cluster of " + std::to_string(cluster) + " fit CTAs");
-  // tickets restart at zero: no stale sequence number or done flag may match one
-  std::memset(q_.h_done, 0, q_.capacity * sizeof(long long));
-  q_.next.store(0);
-  cuda_check(cudaMemsetAsync(q_.d_seq, 0xff, q_.capacity * sizeof(long long), stream_), "memset");
-  cuda_check(cudaMemsetAsync(q_.d_stop, 0, sizeof(int), stream_), "memset");
-  cuda_check(cudaMemsetAsync(q_.d_taken, 0, sizeof(unsigned long long), stream_), "memset");
-  cuda_check(cudaMemsetAsync(q_.d_status, 0, sizeof(int), stream_), "memset");
-  // posts follow the resets
-  cuda_check(cudaEventRecord(q_.ready, stream_), "event");
-  for (cudaStream_t st : q_.posters) cuda_check(cudaStreamWaitEvent(st, q_.ready, 0), "stream wait");
-  device::FitQueue fq{};
-  fq.ring = q_.d_ring;
-  fq.seq = q_.d_seq;
-  fq.stop = q_.d_stop;
-  fq.taken = q_.d_taken;
-  void* dev_ptr = nullptr;
-  cuda_check(cudaHostGetDevicePointer(&dev_ptr, q_.h_results, 0), "mapped results");
-  fq.results = static_cast<device::FitResult*>(dev_ptr);
-  cuda_check(cudaHostGetDevicePointer(&dev_ptr, q_.h_done, 0), "mapped flags");
-  fq.done = static_cast<long long*>(dev_ptr);
-  fq.status = q_.d_status;
-  fq.mask = static_cast<long long>(q_.capacity - 1);
-  fq.idle_ns = kQueueIdleNs;
   const int grid = queue_clusters_[cluster] * cluster;
-  cuda_check(cudaEventRecord(q_.ev0, stream_), "event");
-  cuda_check(static_cast<cudaError_t>(device::launch_fit_queue(data_, ctl_, fq, grid, cluster, stream_)),
-             "fit queue kernel launch");
-  cuda_check(cudaEventRecord(q_.ev1, stream_), "event");
-  q_.running = true;
+  fitq_.start(stream_, [&](const RequestQueue::View& v) {
+    device::FitQueue fq{};
+    fq.ring = static_cast<const device::FitRequest*>(v.ring);
+    fq.seq = v.seq;
+    fq.stop = v.stop;
+    fq.taken = v.taken;
+    fq.results = static_cast<device::FitResult*>(v.results);
+    fq.done = v.done;
+    fq.status = v.status;
+    fq.mask = v.mask;
+    fq.idle_ns = v.idle_ns;
+    return static_cast<cudaError_t>(device::launch_fit_queue(data_, ctl_, fq, grid, cluster, stream_));
+  });
   ++launches_;
 }
 
-void DeviceFitter::copy_range(void* dst, const void* src, size_t elem, long long first, size_t n, cudaStream_t s) {
-  const long long mask = static_cast<long long>(q_.capacity - 1);
-  size_t copied = 0;
-  while (copied < n) {
-    const size_t slot = static_cast<size_t>((first + static_cast<long long>(copied)) & mask);
-    const size_t len = std::min(n - copied, q_.capacity - slot);
-    cuda_check(cudaMemcpyAsync(static_cast<char*>(dst) + slot * elem, static_cast<const char*>(src) + slot * elem,
-                               len * elem, cudaMemcpyHostToDevice, s),
-               "queue copy");
-    copied += len;
-  }
-}
-
 long long DeviceFitter::queue_post(const device::FitRequest* reqs, size_t n, int poster, Tally* tally) {
-  if (n == 0) return q_.next.load();
-  if (n > q_.capacity / 2) fail(NB_ERR_GPU, "too many requests in one post");
-  std::lock_guard<std::mutex> lock(q_.post_mu);
-  const long long first = q_.next.fetch_add(static_cast<long long>(n));
-  const long long cap = static_cast<long long>(q_.capacity);
-  const long long mask = cap - 1;
-  for (size_t i = 0; i < n; ++i) {
-    const long long t = first + static_cast<long long>(i);
-    if (t >= cap && !queue_done(t - cap)) {
-      // the slot still holds an unfinished request: wait for it (bounded)
-      auto t0 = Clock::now();
-      while (!queue_done(t - cap)) {
-        if (!queue_running()) queue_failure("ended with work pending");
-        if (ms_since(t0) > 60000.0) queue_failure("made no progress for 60 s");
-        std::this_thread::yield();
-      }
-    }
-    q_.h_ring[t & mask] = reqs[i];
-    q_.h_seq[t & mask] = t;
-  }
-  // the requests, then (later on the same stream) their sequence numbers.
-  // Every post goes through one stream, one at a time (the lock above):
-  // copies from several streams into neighbouring ring slots lost updates.
   (void)poster;
-  cudaStream_t st = q_.posters[0];
-  copy_range(q_.d_ring, q_.h_ring, sizeof(device::FitRequest), first, n, st);
-  copy_range(q_.d_seq, q_.h_seq, sizeof(long long), first, n, st);
+  const long long first = fitq_.post(reqs, n);
   tally->h2d += n * (sizeof(device::FitRequest) + sizeof(long long));
   return first;
 }
 
-bool DeviceFitter::queue_done(long long ticket) const {
-  long long& flag = q_.h_done[ticket & static_cast<long long>(q_.capacity - 1)];
-  return std::atomic_ref<long long>(flag).load(std::memory_order_acquire) == ticket + 1;
-}
+bool DeviceFitter::queue_done(long long ticket) const { return fitq_.done(ticket); }
 
 const device::FitResult& DeviceFitter::queue_result(long long ticket) const {
-  return q_.h_results[ticket & static_cast<long long>(q_.capacity - 1)];
+  return *static_cast<const device::FitResult*>(fitq_.result(ticket));
 }
 
 void DeviceFitter::queue_account(long long ticket, int gene, Tally* tally) const {
@@ -532,49 +471,17 @@ void DeviceFitter::add_tally(const Tally& t) {
   d2h_bytes_ += t.d2h;
 }
 
-bool DeviceFitter::queue_running() {
-  const cudaError_t e = cudaEventQuery(q_.ev1);
-  if (e == cudaErrorNotReady) return true;
-  cuda_check(e, "fit queue kernel");
-  return false;
+bool DeviceFitter::queue_running() { return fitq_.running(); }
+
+void DeviceFitter::queue_stop() {
+  const double before = fitq_.device_ms();
+  fitq_.stop();
+  device_ms_ += fitq_.device_ms() - before;
 }
 
-void DeviceFitter::queue_stop_impl(bool check) {
-  if (!q_.running) return;
-  q_.running = false;
-  const cudaError_t e1 = cudaMemcpyAsync(q_.d_stop, q_.h_one, sizeof(int), cudaMemcpyHostToDevice, q_.posters[0]);
-  const cudaError_t e2 = cudaEventSynchronize(q_.ev1);
-  int status = 0;
-  const cudaError_t e3 = cudaMemcpy(&status, q_.d_status, sizeof(int), cudaMemcpyDeviceToHost);
-  for (cudaStream_t st : q_.posters) cudaStreamSynchronize(st);
-  if (!check) return;
-  cuda_check(e1, "stop copy");
-  cuda_check(e2, "fit queue kernel");
-  cuda_check(e3, "queue status");
-  float ms = 0.0f;
-  cuda_check(cudaEventElapsedTime(&ms, q_.ev0, q_.ev1), "event time");
-  device_ms_ += ms;
-  if (status != 0) fail(NB_ERR_GPU, "a fit cluster waited more than 30 s for work");
-}
+void DeviceFitter::queue_abort() noexcept { fitq_.abort(); }
 
-void DeviceFitter::queue_stop() { queue_stop_impl(true); }
-
-void DeviceFitter::queue_failure(const char* what) {
-  int status = -1;
-  cudaMemcpy(&status, q_.d_status, sizeof(int), cudaMemcpyDeviceToHost);
-  unsigned long long taken = 0;
-  cudaMemcpy(&taken, q_.d_taken, sizeof(taken), cudaMemcpyDeviceToHost);
-  fail(NB_ERR_GPU, std::string("the fit queue kernel ") + what + " (tickets posted " +
-                       std::to_string(q_.next.load()) + ", taken " + std::to_string(taken) +
-                       (status == 1 ? ", a cluster waited more than 30 s for work)" : ")"));
-}
-
-void DeviceFitter::queue_abort() noexcept {
-  try {
-    queue_stop_impl(false);
-  } catch (...) {
-  }
-}
+void DeviceFitter::queue_failure(const char* what) { fitq_.failure(what); }
 
 bool DeviceFitter::ready(int lane_index) {
   const cudaError_t e = cudaStreamQuery(lanes_[lane_index].stream);
@@ -669,60 +576,119 @@ std::unique_ptr<Session> create_session(const nb_csr* counts, const uint64_t* su
   auto t2 = Clock::now();
   ss->fitter = std::make_unique<DeviceFitter>(ss->prep, ss->genes, ss->opt.device);
   ss->ms_upload = ms_since(t2);
-  // stage one (nebula.rs:812-901): every gene's projected Newton in lockstep,
-  // one batched launch of marginal-likelihood cell passes per round
+  // stage one (nebula.rs:812-901): every gene's projected Newton at its own
+  // pace through one persistent launch of marginal-likelihood cell passes;
+  // host worker threads own the genes, assemble value, gradient and Hessian
+  // from a finished pass and post the gene's next point
   auto t1 = Clock::now();
   const int nb = sh.n_coef, K = sh.n_subjects, np = nb + 2;
-  const int W = ptmg_width(nb);
+  const size_t stride = ss->fitter->ptmg_stride();
   std::vector<std::unique_ptr<MarginalSearch>> search(G);
   std::vector<std::vector<double>> xy(G);
-  std::vector<size_t> active;
-  for (size_t g = 0; g < G; ++g) {
-    std::vector<double> start, lower, upper;
-    marginal_box(sh, ss->genes[g], &start, &lower, &upper);
-    search[g] = std::make_unique<MarginalSearch>(start, lower, upper, nb);
-    xy[g] = positive_xy(sh, ss->genes[g]);
-    active.push_back(g);
-  }
+  std::vector<long long> ticket(G, -1);
   ss->plans.resize(G);
-  std::vector<device::PtmgRequest> batch;
-  while (!active.empty()) {
-    batch.clear();
-    for (size_t g : active) {
-      const double* x = search[g]->ask();
-      Terms t(x[nb], x[nb + 1]);
-      device::PtmgRequest r{};
-      r.gene = static_cast<int32_t>(g);
-      r.alpha = t.alpha;
-      r.lambda = t.lambda;
-      r.gamma = t.gamma;
-      for (int j = 0; j < nb; ++j) r.beta[j] = x[j];
-      batch.push_back(r);
-    }
-    const double* res = ss->fitter->run_ptmg(batch);
-    const size_t stride = static_cast<size_t>(2 + W) * K;
-    std::vector<char> finished(active.size(), 0);
-    parallel_for(active.size(), ss->opt.host_threads, [&](size_t i) {
-      const size_t g = active[i];
-      const double* r = res + i * stride;
-      PtmgSums sums;
-      sums.cumsumxtb.assign(r, r + K);
-      sums.ylin.assign(r + K, r + 2 * K);
-      sums.sums.assign(r + 2 * K, r + stride);
-      MarginalGene mg{&sh, &ss->genes[g], &ss->prep.totals[ss->prep.kept[g] * K], xy[g].data()};
-      std::vector<double> grad(np), hess(static_cast<size_t>(np) * np);
-      std::vector<double> x(search[g]->ask(), search[g]->ask() + np);
-      double f = ptmg_assemble(mg, x.data(), sums, grad.data(), hess.data());
-      search[g]->tell(f, grad.data(), hess.data());
-      if (search[g]->done()) {
-        ss->plans[g] = plan_from(sh, ss->genes[g], search[g]->best(), search[g]->failed());
-        finished[i] = 1;
+  size_t capacity = 256;
+  while (capacity < 2 * G && capacity < 4096) capacity *= 2;
+  const int hw = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
+  const int workers = std::max(1, std::min<int>({ss->opt.host_threads > 0 ? ss->opt.host_threads : hw, 8,
+                                                 static_cast<int>(std::max<size_t>(G, 1))}));
+  std::atomic<bool> abort{false};
+  std::mutex err_mu;
+  std::optional<NbError> first_err;
+  auto request_of = [&](size_t g) {
+    const double* x = search[g]->ask();
+    Terms t(x[nb], x[nb + 1]);
+    device::PtmgRequest r{};
+    r.gene = static_cast<int32_t>(g);
+    r.alpha = t.alpha;
+    r.lambda = t.lambda;
+    r.gamma = t.gamma;
+    for (int j = 0; j < nb; ++j) r.beta[j] = x[j];
+    return r;
+  };
+  auto worker = [&](int w) {
+    try {
+      std::vector<size_t> waiting, owners;
+      std::vector<device::PtmgRequest> box;
+      auto post = [&]() {
+        if (box.empty()) return;
+        const long long first = ss->fitter->ptmg_post(box.data(), box.size());
+        for (size_t k = 0; k < owners.size(); ++k) ticket[owners[k]] = first + static_cast<long long>(k);
+        box.clear();
+        owners.clear();
+      };
+      for (size_t g = static_cast<size_t>(w); g < G; g += static_cast<size_t>(workers)) {
+        std::vector<double> start, lower, upper;
+        marginal_box(sh, ss->genes[g], &start, &lower, &upper);
+        search[g] = std::make_unique<MarginalSearch>(start, lower, upper, nb);
+        xy[g] = positive_xy(sh, ss->genes[g]);
+        box.push_back(request_of(g));
+        owners.push_back(g);
+        waiting.push_back(g);
+        if (box.size() >= 64) post();
       }
-    });
-    std::vector<size_t> still;
-    for (size_t i = 0; i < active.size(); ++i)
-      if (!finished[i]) still.push_back(active[i]);
-    active.swap(still);
+      post();
+      std::vector<double> grad(np), hess(static_cast<size_t>(np) * np), x(np);
+      auto last_progress = Clock::now();
+      while (!waiting.empty() && !abort.load(std::memory_order_relaxed)) {
+        bool progressed = false;
+        for (size_t i = 0; i < waiting.size();) {
+          const size_t g = waiting[i];
+          if (!ss->fitter->ptmg_done(ticket[g])) {
+            ++i;
+            continue;
+          }
+          progressed = true;
+          const double* r = ss->fitter->ptmg_result(ticket[g]);
+          PtmgSums sums;
+          sums.cumsumxtb.assign(r, r + K);
+          sums.ylin.assign(r + K, r + 2 * K);
+          sums.sums.assign(r + 2 * K, r + stride);
+          MarginalGene mg{&sh, &ss->genes[g], &ss->prep.totals[ss->prep.kept[g] * K], xy[g].data()};
+          x.assign(search[g]->ask(), search[g]->ask() + np);
+          const double f = ptmg_assemble(mg, x.data(), sums, grad.data(), hess.data());
+          search[g]->tell(f, grad.data(), hess.data());
+          if (search[g]->done()) {
+            ss->plans[g] = plan_from(sh, ss->genes[g], search[g]->best(), search[g]->failed());
+            waiting[i] = waiting.back();
+            waiting.pop_back();
+            continue;
+          }
+          box.push_back(request_of(g));
+          owners.push_back(g);
+          ++i;
+        }
+        post();
+        if (progressed) {
+          last_progress = Clock::now();
+        } else {
+          if (!ss->fitter->ptmg_running()) ss->fitter->ptmg_failure("ended with work pending");
+          if (ms_since(last_progress) > 60000.0) ss->fitter->ptmg_failure("made no progress for 60 s");
+          std::this_thread::yield();
+        }
+      }
+    } catch (const NbError& e) {
+      std::lock_guard<std::mutex> lock(err_mu);
+      if (!first_err) first_err = e;
+      abort.store(true);
+    } catch (const std::exception& e) {
+      std::lock_guard<std::mutex> lock(err_mu);
+      if (!first_err) first_err = NbError{NB_ERR_GPU, e.what()};
+      abort.store(true);
+    }
+  };
+  {
+    struct QueueGuard {
+      DeviceFitter& f;
+      ~QueueGuard() { f.ptmg_abort(); }
+    } guard{*ss->fitter};
+    ss->fitter->ptmg_queue_start(capacity);
+    std::vector<std::thread> pool;
+    for (int w = 1; w < workers; ++w) pool.emplace_back(worker, w);
+    worker(0);
+    for (auto& th : pool) th.join();
+    if (first_err) throw *first_err;
+    ss->fitter->ptmg_stop();
   }
   ss->ms_stage_one = ms_since(t1);
   return ss;

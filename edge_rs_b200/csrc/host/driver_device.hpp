@@ -4,12 +4,14 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <memory>
 #include <mutex>
 #include <vector>
 
 #include "../cuda/pml_device.cuh"
 #include "../cuda/ptmg_device.cuh"
 #include "common.hpp"
+#include "driver_queue.hpp"
 
 namespace nebula {
 
@@ -69,6 +71,17 @@ class DeviceFitter {
   // One batch of stage-one evaluations: per request (2 + W) * K doubles,
   // valid until the next call.
   const double* run_ptmg(const std::vector<device::PtmgRequest>& reqs);
+  // Stage one in streaming mode (device::PtmgQueue), the same protocol as
+  // the fit queue below; a result is ptmg_stride() doubles.
+  void ptmg_queue_start(size_t capacity);
+  long long ptmg_post(const device::PtmgRequest* reqs, size_t n);
+  bool ptmg_done(long long ticket) const;
+  const double* ptmg_result(long long ticket) const;
+  bool ptmg_running();
+  void ptmg_stop();
+  void ptmg_abort() noexcept;
+  [[noreturn]] void ptmg_failure(const char* what);
+  size_t ptmg_stride() const;
 
   double device_ms() const { return device_ms_; }
   uint64_t launches() const { return launches_; }
@@ -101,27 +114,9 @@ class DeviceFitter {
     size_t pending = 0;  // requests of the batch in flight
   };
   void reserve(Lane& lane, size_t n);
-  struct Queue {
-    size_t capacity = 0;  // a power of two
-    device::FitRequest* d_ring = nullptr;
-    long long* d_seq = nullptr;
-    int* d_stop = nullptr;
-    unsigned long long* d_taken = nullptr;
-    int* d_status = nullptr;
-    device::FitRequest* h_ring = nullptr;    // pinned staging, slot for slot
-    long long* h_seq = nullptr;              // pinned staging, slot for slot
-    int* h_one = nullptr;                    // pinned: 1
-    device::FitResult* h_results = nullptr;  // mapped
-    long long* h_done = nullptr;             // mapped
-    cudaStream_t posters[kMaxPosters] = {};
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ready = nullptr;
-    std::atomic<long long> next{0};
-    std::mutex post_mu;
-    bool running = false;
-  };
-  void copy_range(void* dst, const void* src, size_t elem, long long first, size_t n, cudaStream_t s);
-  void queue_stop_impl(bool check);
-  Queue q_;
+  RequestQueue fitq_{sizeof(device::FitRequest), sizeof(device::FitResult), 16384};
+  std::unique_ptr<RequestQueue> ptmgq_;
+  void ensure_ptmg_scratch();
   int queue_clusters_[device::kMaxCluster + 1] = {};
   cudaStream_t stream_ = nullptr;
   cudaEvent_t step0_ = nullptr, step1_ = nullptr;

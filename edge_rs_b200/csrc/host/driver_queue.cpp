@@ -1,0 +1,195 @@
+// Host side of the persistent kernels' request rings (driver_queue.hpp).
+#include "driver_queue.hpp"
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <thread>
+
+#include "common.hpp"
+
+namespace nebula {
+namespace {
+
+constexpr long long kIdleNs = 30000000000LL;  // longest wait of a cluster for work: 30 s
+
+void check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) fail(NB_ERR_GPU, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+double ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+}  // namespace
+
+RequestQueue::RequestQueue(size_t request_bytes, size_t result_bytes, size_t capacity)
+    : request_bytes_(request_bytes), result_bytes_(result_bytes), capacity_(capacity) {}
+
+RequestQueue::~RequestQueue() {
+  abort();
+  if (post_stream_) cudaStreamSynchronize(post_stream_);
+  if (d_ring_) cudaFree(d_ring_);
+  if (d_seq_) cudaFree(d_seq_);
+  if (d_stop_) cudaFree(d_stop_);
+  if (d_taken_) cudaFree(d_taken_);
+  if (d_status_) cudaFree(d_status_);
+  if (h_ring_) cudaFreeHost(h_ring_);
+  if (h_seq_) cudaFreeHost(h_seq_);
+  if (h_one_) cudaFreeHost(h_one_);
+  if (h_results_) cudaFreeHost(h_results_);
+  if (h_done_) cudaFreeHost(h_done_);
+  if (ev0_) cudaEventDestroy(ev0_);
+  if (ev1_) cudaEventDestroy(ev1_);
+  if (ready_) cudaEventDestroy(ready_);
+  if (post_stream_) cudaStreamDestroy(post_stream_);
+}
+
+void RequestQueue::start(cudaStream_t stream, const std::function<cudaError_t(const View&)>& launch) {
+  if (running_) fail(NB_ERR_GPU, "the work queue is already running");
+  const size_t cap = capacity_;
+  if (!d_ring_) {
+    check(cudaEventCreate(&ev0_), "event");
+    check(cudaEventCreate(&ev1_), "event");
+    check(cudaEventCreateWithFlags(&ready_, cudaEventDisableTiming), "event");
+    check(cudaStreamCreateWithFlags(&post_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+    check(cudaMalloc(reinterpret_cast<void**>(&d_ring_), cap * request_bytes_), "cudaMalloc");
+    check(cudaMalloc(reinterpret_cast<void**>(&d_seq_), cap * sizeof(long long)), "cudaMalloc");
+    check(cudaMalloc(reinterpret_cast<void**>(&d_stop_), sizeof(int)), "cudaMalloc");
+    check(cudaMalloc(reinterpret_cast<void**>(&d_taken_), sizeof(unsigned long long)), "cudaMalloc");
+    check(cudaMalloc(reinterpret_cast<void**>(&d_status_), sizeof(int)), "cudaMalloc");
+    check(cudaMallocHost(reinterpret_cast<void**>(&h_ring_), cap * request_bytes_), "cudaMallocHost");
+    check(cudaMallocHost(reinterpret_cast<void**>(&h_seq_), cap * sizeof(long long)), "cudaMallocHost");
+    check(cudaMallocHost(reinterpret_cast<void**>(&h_one_), sizeof(int)), "cudaMallocHost");
+    *h_one_ = 1;
+    check(cudaHostAlloc(reinterpret_cast<void**>(&h_results_), cap * result_bytes_, cudaHostAllocMapped),
+          "cudaHostAlloc");
+    check(cudaHostAlloc(reinterpret_cast<void**>(&h_done_), cap * sizeof(long long), cudaHostAllocMapped),
+          "cudaHostAlloc");
+  }
+  // tickets restart at zero: no stale sequence number or done flag may match one
+  std::memset(h_done_, 0, cap * sizeof(long long));
+  next_.store(0);
+  check(cudaMemsetAsync(d_seq_, 0xff, cap * sizeof(long long), stream), "memset");
+  check(cudaMemsetAsync(d_stop_, 0, sizeof(int), stream), "memset");
+  check(cudaMemsetAsync(d_taken_, 0, sizeof(unsigned long long), stream), "memset");
+  check(cudaMemsetAsync(d_status_, 0, sizeof(int), stream), "memset");
+  check(cudaEventRecord(ready_, stream), "event");
+  check(cudaStreamWaitEvent(post_stream_, ready_, 0), "stream wait");  // posts follow the resets
+  View v{};
+  v.ring = d_ring_;
+  v.seq = d_seq_;
+  v.stop = d_stop_;
+  v.taken = d_taken_;
+  void* dev_ptr = nullptr;
+  check(cudaHostGetDevicePointer(&dev_ptr, h_results_, 0), "mapped results");
+  v.results = dev_ptr;
+  check(cudaHostGetDevicePointer(&dev_ptr, h_done_, 0), "mapped flags");
+  v.done = static_cast<long long*>(dev_ptr);
+  v.status = d_status_;
+  v.mask = static_cast<long long>(cap - 1);
+  v.idle_ns = kIdleNs;
+  check(cudaEventRecord(ev0_, stream), "event");
+  check(launch(v), "queue kernel launch");
+  check(cudaEventRecord(ev1_, stream), "event");
+  running_ = true;
+}
+
+void RequestQueue::copy_range(void* dst, const void* src, size_t elem, long long first, size_t n) {
+  const long long mask = static_cast<long long>(capacity_ - 1);
+  size_t copied = 0;
+  while (copied < n) {
+    const size_t slot = static_cast<size_t>((first + static_cast<long long>(copied)) & mask);
+    const size_t len = std::min(n - copied, capacity_ - slot);
+    check(cudaMemcpyAsync(static_cast<char*>(dst) + slot * elem, static_cast<const char*>(src) + slot * elem,
+                          len * elem, cudaMemcpyHostToDevice, post_stream_),
+          "queue copy");
+    copied += len;
+  }
+}
+
+long long RequestQueue::post(const void* requests, size_t n) {
+  if (n == 0) return next_.load();
+  if (n > capacity_ / 2) fail(NB_ERR_GPU, "too many requests in one post");
+  // One post at a time through one stream: copies from several streams into
+  // neighbouring ring slots lost updates.
+  std::lock_guard<std::mutex> lock(post_mu_);
+  const long long first = next_.fetch_add(static_cast<long long>(n));
+  const long long cap = static_cast<long long>(capacity_);
+  const long long mask = cap - 1;
+  const char* src = static_cast<const char*>(requests);
+  for (size_t i = 0; i < n; ++i) {
+    const long long t = first + static_cast<long long>(i);
+    if (t >= cap && !done(t - cap)) {
+      // the slot still holds an unfinished request: wait for it (bounded)
+      const auto t0 = std::chrono::steady_clock::now();
+      while (!done(t - cap)) {
+        if (!running()) failure("ended with work pending");
+        if (ms_since(t0) > 60000.0) failure("made no progress for 60 s");
+        std::this_thread::yield();
+      }
+    }
+    std::memcpy(h_ring_ + static_cast<size_t>(t & mask) * request_bytes_, src + i * request_bytes_,
+                request_bytes_);
+    h_seq_[t & mask] = t;
+  }
+  // the requests, then (later on the same stream) their sequence numbers
+  copy_range(d_ring_, h_ring_, request_bytes_, first, n);
+  copy_range(d_seq_, h_seq_, sizeof(long long), first, n);
+  return first;
+}
+
+bool RequestQueue::done(long long ticket) const {
+  long long& flag = h_done_[ticket & static_cast<long long>(capacity_ - 1)];
+  return std::atomic_ref<long long>(flag).load(std::memory_order_acquire) == ticket + 1;
+}
+
+const void* RequestQueue::result(long long ticket) const {
+  return h_results_ + static_cast<size_t>(ticket & static_cast<long long>(capacity_ - 1)) * result_bytes_;
+}
+
+bool RequestQueue::running() {
+  const cudaError_t e = cudaEventQuery(ev1_);
+  if (e == cudaErrorNotReady) return true;
+  check(e, "queue kernel");
+  return false;
+}
+
+void RequestQueue::stop_impl(bool check_status) {
+  if (!running_) return;
+  running_ = false;
+  const cudaError_t e1 = cudaMemcpyAsync(d_stop_, h_one_, sizeof(int), cudaMemcpyHostToDevice, post_stream_);
+  const cudaError_t e2 = cudaEventSynchronize(ev1_);
+  int status = 0;
+  const cudaError_t e3 = cudaMemcpy(&status, d_status_, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaStreamSynchronize(post_stream_);
+  if (!check_status) return;
+  check(e1, "stop copy");
+  check(e2, "queue kernel");
+  check(e3, "queue status");
+  float ms = 0.0f;
+  check(cudaEventElapsedTime(&ms, ev0_, ev1_), "event time");
+  device_ms_ += ms;
+  if (status != 0) fail(NB_ERR_GPU, "a queue cluster waited more than 30 s for work");
+}
+
+void RequestQueue::stop() { stop_impl(true); }
+
+void RequestQueue::abort() noexcept {
+  try {
+    stop_impl(false);
+  } catch (...) {
+  }
+}
+
+void RequestQueue::failure(const char* what) {
+  int status = -1;
+  cudaMemcpy(&status, d_status_, sizeof(int), cudaMemcpyDeviceToHost);
+  unsigned long long taken = 0;
+  cudaMemcpy(&taken, d_taken_, sizeof(taken), cudaMemcpyDeviceToHost);
+  fail(NB_ERR_GPU, std::string("the queue kernel ") + what + " (tickets posted " + std::to_string(next_.load()) +
+                       ", taken " + std::to_string(taken) +
+                       (status == 1 ? ", a cluster waited more than 30 s for work)" : ")"));
+}
+
+}  // namespace nebula
