@@ -24,9 +24,6 @@ size_t ptmg_smem_bytes(int n_subjects);
 int ptmg_width_of(int n_coef);
 size_t ptmg_scratch_doubles(int n_subjects, int n_coef);  // per CTA
 
-int launch_ptmg(const GeneData& d, const PtmgRequest* req, double* results, double* scratch,
-                const int32_t* n_requests, int32_t* counter, int grid, void* stream);
-
 // Streaming mode for stage one: the request-ring protocol of FitQueue
 // (pml_device.cuh) with PtmgRequests and results of result_stride doubles
 // each in host-mapped memory; one CTA per request, `grid` CTAs each owning

@@ -15,9 +15,10 @@
 // The summation tree, the exp/log (nbmath.hpp) and the fused multiply-adds
 // (written explicitly; the file is compiled with -fmad=false) are those of the
 // CPU oracle (oracle/ptmg_cpu.cpp), so the two agree bit for bit. One
-// persistent CTA per SM slot takes requests off an atomic queue; the warp
-// slots live in a per-CTA global scratch region (L2-resident). Nothing waits
-// on anything but the CTA's own barriers.
+// persistent launch serves the whole stage: each CTA claims the next ticket
+// of the device request ring, waits (bounded) for the host to post it, and
+// writes its result to host-mapped memory; the warp slots live in a per-CTA
+// global scratch region (L2-resident).
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -257,30 +258,6 @@ __device__ void ptmg_one(const GeneData& d, const PtmgCta& c, const PtmgRequest&
   tree_pass<NB, 2, D::W>(d, c.fid, c.wcells, req.gene, beta, c.ym, req.gamma, c.slots, D::W, out + 2 * K, D::W);
 }
 
-template <int NB>
-__global__ void __launch_bounds__(kThreads, 1) ptmg_kernel(GeneData d, const PtmgRequest* __restrict__ requests,
-                                                           double* __restrict__ results,
-                                                           double* __restrict__ scratch,
-                                                           const int32_t* __restrict__ n_requests,
-                                                           int32_t* __restrict__ counter) {
-  using D = PDims<NB>;
-  extern __shared__ __align__(16) double smem[];
-  const PtmgCta c = ptmg_setup<NB>(d, smem, scratch);
-  __shared__ int next_req;
-  __shared__ double beta_sm[kMaxCoef];
-  const int total = *n_requests;
-  const size_t out_stride = static_cast<size_t>(2 + D::W) * d.n_subjects;
-  for (;;) {
-    __syncthreads();
-    if (threadIdx.x == 0) next_req = atomicAdd(counter, 1);
-    __syncthreads();
-    const int q = next_req;
-    if (q >= total) break;
-    const PtmgRequest req = requests[q];
-    ptmg_one<NB>(d, c, req, beta_sm, results + static_cast<size_t>(q) * out_stride);
-  }
-}
-
 __device__ __forceinline__ long long global_ns() {
   long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -338,17 +315,6 @@ __global__ void __launch_bounds__(kThreads, 1) ptmg_queue_kernel(GeneData d, Ptm
 }
 
 template <int NB>
-int launch_nb(const GeneData& d, const PtmgRequest* req, double* res, double* scratch, const int32_t* n_req,
-              int32_t* counter, int grid, cudaStream_t stream) {
-  const size_t smem = ptmg_smem_bytes(d.n_subjects);
-  cudaError_t e = cudaFuncSetAttribute(ptmg_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(smem));
-  if (e != cudaSuccess) return e;
-  ptmg_kernel<NB><<<grid, kThreads, smem, stream>>>(d, req, res, scratch, n_req, counter);
-  return cudaGetLastError();
-}
-
-template <int NB>
 int launch_queue_nb(const GeneData& d, const PtmgQueue& qu, double* scratch, int grid, cudaStream_t stream) {
   const size_t smem = ptmg_smem_bytes(d.n_subjects);
   cudaError_t e = cudaFuncSetAttribute(ptmg_queue_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -383,22 +349,6 @@ int ptmg_width_of(int n_coef) { return 9 + 4 * n_coef + n_coef * (n_coef + 1); }
 
 size_t ptmg_scratch_doubles(int n_subjects, int n_coef) {
   return static_cast<size_t>(2 * n_subjects + kWarps) * ptmg_width_of(n_coef);
-}
-
-int launch_ptmg(const GeneData& d, const PtmgRequest* req, double* results, double* scratch,
-                const int32_t* n_requests, int32_t* counter, int grid, void* stream) {
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  switch (d.n_coef) {
-    case 1: return launch_nb<1>(d, req, results, scratch, n_requests, counter, grid, s);
-    case 2: return launch_nb<2>(d, req, results, scratch, n_requests, counter, grid, s);
-    case 3: return launch_nb<3>(d, req, results, scratch, n_requests, counter, grid, s);
-    case 4: return launch_nb<4>(d, req, results, scratch, n_requests, counter, grid, s);
-    case 5: return launch_nb<5>(d, req, results, scratch, n_requests, counter, grid, s);
-    case 6: return launch_nb<6>(d, req, results, scratch, n_requests, counter, grid, s);
-    case 7: return launch_nb<7>(d, req, results, scratch, n_requests, counter, grid, s);
-    case 8: return launch_nb<8>(d, req, results, scratch, n_requests, counter, grid, s);
-    default: return cudaErrorInvalidValue;
-  }
 }
 
 }  // namespace device

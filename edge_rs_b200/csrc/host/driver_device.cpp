@@ -181,9 +181,6 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
     owned_.push_back(lane.d_counter);
     cuda_check(cudaMallocHost(reinterpret_cast<void**>(&lane.h_header), 2 * sizeof(int32_t)), "cudaMallocHost");
   }
-  cuda_check(cudaMalloc(reinterpret_cast<void**>(&d_pcounter_), 2 * sizeof(int32_t)), "cudaMalloc");
-  owned_.push_back(d_pcounter_);
-  cuda_check(cudaMallocHost(reinterpret_cast<void**>(&h_pheader_), 2 * sizeof(int32_t)), "cudaMallocHost");
   cuda_check(cudaEventCreate(&step0_), "event");
   cuda_check(cudaEventCreate(&step1_), "event");
 }
@@ -260,54 +257,10 @@ void DeviceFitter::ptmg_abort() noexcept {
 }
 void DeviceFitter::ptmg_failure(const char* what) { ptmgq_->failure(what); }
 
-const double* DeviceFitter::run_ptmg(const std::vector<device::PtmgRequest>& reqs) {
-  const size_t n = reqs.size();
-  if (n == 0) return nullptr;
-  const int K = data_.n_subjects;
-  const size_t stride = static_cast<size_t>(2 + device::ptmg_width_of(data_.n_coef)) * K;
-  ensure_ptmg_scratch();
-  if (n > pcapacity_) {
-    size_t cap = std::max<size_t>(n, pcapacity_ * 2);
-    if (d_preq_) cudaFree(d_preq_);
-    if (d_pres_) cudaFree(d_pres_);
-    if (h_preq_) cudaFreeHost(h_preq_);
-    if (h_pres_) cudaFreeHost(h_pres_);
-    cuda_check(cudaMalloc(reinterpret_cast<void**>(&d_preq_), cap * sizeof(device::PtmgRequest)), "cudaMalloc");
-    cuda_check(cudaMalloc(reinterpret_cast<void**>(&d_pres_), cap * stride * sizeof(double)), "cudaMalloc");
-    cuda_check(cudaMallocHost(reinterpret_cast<void**>(&h_preq_), cap * sizeof(device::PtmgRequest)),
-               "cudaMallocHost");
-    cuda_check(cudaMallocHost(reinterpret_cast<void**>(&h_pres_), cap * stride * sizeof(double)),
-               "cudaMallocHost");
-    pcapacity_ = cap;
-  }
-  std::memcpy(h_preq_, reqs.data(), n * sizeof(device::PtmgRequest));
-  h_pheader_[0] = static_cast<int32_t>(n);
-  h_pheader_[1] = 0;
-  cuda_check(cudaMemcpyAsync(d_preq_, h_preq_, n * sizeof(device::PtmgRequest), cudaMemcpyHostToDevice, stream_),
-             "stage-one request copy");
-  cuda_check(cudaMemcpyAsync(d_pcounter_, h_pheader_, 2 * sizeof(int32_t), cudaMemcpyHostToDevice, stream_),
-             "count copy");
-  const int grid = static_cast<int>(std::min<size_t>(pgrid_, n));
-  cuda_check(static_cast<cudaError_t>(device::launch_ptmg(data_, d_preq_, d_pres_, d_scratch_, d_pcounter_,
-                                                          d_pcounter_ + 1, grid, stream_)),
-             "stage-one kernel launch");
-  cuda_check(cudaMemcpyAsync(h_pres_, d_pres_, n * stride * sizeof(double), cudaMemcpyDeviceToHost, stream_),
-             "stage-one result copy");
-  cuda_check(cudaStreamSynchronize(stream_), "stage-one kernel");
-  ++launches_;
-  h2d_bytes_ += n * sizeof(device::PtmgRequest) + 2 * sizeof(int32_t);
-  d2h_bytes_ += n * stride * sizeof(double);
-  for (size_t i = 0; i < n; ++i) cell_visits_ += 2 * (n_cells_ + gene_nnz_[reqs[i].gene]);
-  return h_pres_;
-}
 
 DeviceFitter::~DeviceFitter() {
   fitq_.abort();
   ptmg_abort();
-  if (d_preq_) cudaFree(d_preq_);
-  if (d_pres_) cudaFree(d_pres_);
-  if (h_preq_) cudaFreeHost(h_preq_);
-  if (h_pres_) cudaFreeHost(h_pres_);
   for (Lane& lane : lanes_) {
     if (lane.stream) cudaStreamSynchronize(lane.stream);
     if (lane.d_req) cudaFree(lane.d_req);
@@ -320,7 +273,6 @@ DeviceFitter::~DeviceFitter() {
     if (lane.stream) cudaStreamDestroy(lane.stream);
   }
   for (void* p : owned_) cudaFree(p);
-  if (h_pheader_) cudaFreeHost(h_pheader_);
   if (step0_) cudaEventDestroy(step0_);
   if (step1_) cudaEventDestroy(step1_);
   if (stream_) cudaStreamDestroy(stream_);

@@ -68,9 +68,6 @@ class DeviceFitter {
   [[noreturn]] void queue_failure(const char* what);
   // CTAs per request for a stage with `requests` requests in flight.
   int cluster_for(size_t requests) const;
-  // One batch of stage-one evaluations: per request (2 + W) * K doubles,
-  // valid until the next call.
-  const double* run_ptmg(const std::vector<device::PtmgRequest>& reqs);
   // Stage one in streaming mode (device::PtmgQueue), the same protocol as
   // the fit queue below; a result is ptmg_stride() doubles.
   void ptmg_queue_start(size_t capacity);
@@ -129,14 +126,7 @@ class DeviceFitter {
   int grid_ = 0;
   int max_clusters_[device::kMaxCluster + 1] = {};  // resident clusters per cluster size
   // stage-one buffers
-  int32_t* h_pheader_ = nullptr;
-  int32_t* d_pcounter_ = nullptr;
-  device::PtmgRequest* d_preq_ = nullptr;
-  device::PtmgRequest* h_preq_ = nullptr;
-  double* d_pres_ = nullptr;
-  double* h_pres_ = nullptr;
   double* d_scratch_ = nullptr;
-  size_t pcapacity_ = 0;
   int pgrid_ = 0;
   double device_ms_ = 0.0;
   uint64_t launches_ = 0, requests_ = 0, sweeps_ = 0, cell_visits_ = 0, slot_cycles_ = 0;
