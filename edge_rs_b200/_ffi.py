@@ -55,7 +55,8 @@ class NbOptions(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("warm_start", ctypes.c_int32),
                 ("host_threads", ctypes.c_int32), ("audit_percent", ctypes.c_int32),
                 ("mlp_weights", c_float_p), ("cluster", ctypes.c_int32),
-                ("warm_points", ctypes.POINTER(ctypes.c_double)), ("evaluations", ctypes.POINTER(ctypes.c_int32))]
+                ("warm_points", ctypes.POINTER(ctypes.c_double)), ("evaluations", ctypes.POINTER(ctypes.c_int32)),
+                ("warm_radius", ctypes.c_double)]
 
 
 class NbStats(ctypes.Structure):
@@ -97,6 +98,8 @@ PRODUCT_SIGNATURES = {
                                         c_double_p, c_double_p, ctypes.c_char_p, ctypes.c_size_t]),
     "nb_bobyqa_new": (ctypes.c_void_p, [c_double_p, c_double_p, c_double_p, ctypes.c_uint32,
                                         ctypes.c_double, ctypes.c_uint32]),
+    "nb_bobyqa_new_scaled": (ctypes.c_void_p, [c_double_p, c_double_p, c_double_p, ctypes.c_uint32,
+                                               ctypes.c_double, ctypes.c_uint32, ctypes.c_double]),
     "nb_bobyqa_ask": (ctypes.c_int32, [ctypes.c_void_p, c_double_p]),
     "nb_bobyqa_tell": (None, [ctypes.c_void_p, ctypes.c_double]),
     "nb_bobyqa_result": (ctypes.c_int32, [ctypes.c_void_p, c_double_p, c_double_p,

@@ -553,7 +553,7 @@ void update(int n, int npt, double* bmat, double* zmat, int ndim, double* vlag, 
 // nlopt_set_default_initial_step, nlopt_compute_rescaling and bobyqa()'s
 // adjustment of the start against the bounds (bobyqa.rs:318-511).
 Bobyqa::Bobyqa(const double* x0, const double* lower, const double* upper, int n,
-               double xtol_rel, int maxeval)
+               double xtol_rel, int maxeval, double radius_scale)
     : n_(n), maxeval_(maxeval) {
   if (n <= 0) {
     ok_ = false;
@@ -598,6 +598,7 @@ Bobyqa::Bobyqa(const double* x0, const double* lower, const double* upper, int n
   }
   rhobeg_ = std::fabs(dx[0] / s_[0]);
   rhoend_ = xtol_rel * rhobeg_;
+  if (radius_scale < 1.0) rhobeg_ = std::max(rhobeg_ * radius_scale, 16.0 * rhoend_);
   npt_ = 2 * n + 1;
   ndim_ = npt_ + n;
   sl0_.assign(n + 1, 0.0);

@@ -39,8 +39,13 @@ class Bobyqa {
  public:
   // Sets the search up as nlopt_optimize + bobyqa do. `ok()` is false when the
   // box is too narrow for the initial radius (NLopt refuses it).
+  //
+  // `radius_scale` < 1 starts the trust region at that fraction of NLopt's
+  // initial radius while rhoend stays xtol_rel times the unscaled radius: a
+  // search from a start already close to the optimum skips the coarse radii
+  // and ends at the same final resolution. 1 is NLopt's search exactly.
   Bobyqa(const double* x0, const double* lower, const double* upper, int n,
-         double xtol_rel = 1e-6, int maxeval = 1000);
+         double xtol_rel = 1e-6, int maxeval = 1000, double radius_scale = 1.0);
   ~Bobyqa();
   Bobyqa(const Bobyqa&) = delete;
   Bobyqa& operator=(const Bobyqa&) = delete;

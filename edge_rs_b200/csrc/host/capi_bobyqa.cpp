@@ -9,20 +9,26 @@
 
 struct nb_bobyqa {
   nebula::Bobyqa search;
-  nb_bobyqa(const double* x0, const double* lo, const double* hi, int n, double xtol, int maxeval)
-      : search(x0, lo, hi, n, xtol, maxeval) {}
+  nb_bobyqa(const double* x0, const double* lo, const double* hi, int n, double xtol, int maxeval,
+            double radius_scale)
+      : search(x0, lo, hi, n, xtol, maxeval, radius_scale) {}
 };
 
-NB_API nb_bobyqa* nb_bobyqa_new(const double* x0, const double* lower, const double* upper,
-                                uint32_t n, double xtol_rel, uint32_t maxeval) {
-  if (!x0 || !lower || !upper || n == 0) return nullptr;
+NB_API nb_bobyqa* nb_bobyqa_new_scaled(const double* x0, const double* lower, const double* upper,
+                                       uint32_t n, double xtol_rel, uint32_t maxeval, double radius_scale) {
+  if (!x0 || !lower || !upper || n == 0 || !(radius_scale > 0.0)) return nullptr;
   auto* h = new (std::nothrow) nb_bobyqa(x0, lower, upper, static_cast<int>(n), xtol_rel,
-                                         static_cast<int>(maxeval));
+                                         static_cast<int>(maxeval), radius_scale);
   if (h && !h->search.ok()) {
     delete h;
     return nullptr;
   }
   return h;
+}
+
+NB_API nb_bobyqa* nb_bobyqa_new(const double* x0, const double* lower, const double* upper,
+                                uint32_t n, double xtol_rel, uint32_t maxeval) {
+  return nb_bobyqa_new_scaled(x0, lower, upper, n, xtol_rel, maxeval, 1.0);
 }
 
 NB_API int32_t nb_bobyqa_ask(const nb_bobyqa* h, double* x) {

@@ -1,13 +1,14 @@
 // nebula_sparse_cuda: the drop-in for nebula_sparse (src/sc/nebula.rs:434-445)
 // with every penalised inner fit on the GPU.
 //
-// Mirrors the reference's device path (src/gpu/stage_two.rs:281-320 fit_all,
-// :362-544 search_all) but keeps the finish on the device: stage one runs on
-// host threads; stage two advances every gene's search in lockstep, one
-// batched launch per round holding each search's pending point(s); stage
-// three batches the final fit of every gene into one more launch. The host
-// only steps the searches and assembles the objective from the four scalars
-// each device fit returns.
+// Covers the reference's device path (src/gpu/stage_two.rs:281-320 fit_all,
+// :362-544 search_all) and the two stages around it. Stage one's cell passes
+// and every inner fit of stages two and three run in persistent launches fed
+// by device request rings (driver_queue.hpp); host worker threads own
+// disjoint sets of genes, step each gene's search (Newton for stage one,
+// BOBYQA for stage two) as soon as its points return, and post the gene's
+// next points. No gene waits for another. The host only steps the searches
+// and assembles the objective from the scalars each device fit returns.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -451,6 +452,14 @@ const device::FitResult* DeviceFitter::run(const std::vector<device::FitRequest>
 
 namespace {
 
+// Default initial trust radius of a warm search, as a fraction of NLopt's.
+// On 500 genes x 100,000 cells (stage one's start within about 1%) it cuts
+// the search's evaluations by 38% against the full radius; on genes drawn
+// with sigma^2 and phi LogNormal sd 1.0 (starts off by about 10%) by 32%,
+// with the warm search ending worse than the cold one on 1 of 200 genes
+// (2 of 200 at the full radius). Smaller radii gain nothing more there.
+constexpr double kWarmRadius = 0.03;
+
 struct GeneTask {
   std::unique_ptr<StageTwoSearch> search;
   VarianceObjective objective;
@@ -711,6 +720,8 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
   std::vector<std::array<double, 2>> warm_point(G);
   std::vector<double> budget(G, 0.0);
   if (warm) warm_starts(ss, &warm_point, &budget);
+  // The warm search's initial trust radius, a fraction of NLopt's.
+  const double radius = ss.opt.warm_radius > 0.0 ? std::min(ss.opt.warm_radius, 1.0) : kWarmRadius;
   std::vector<size_t> audit_of;
   std::vector<long long> twin(G, -1);
   if (warm) {
@@ -852,7 +863,7 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
         std::vector<double> lower, upper;
         variance_bounds(sh.params, fixed_cell.has_value(), &lower, &upper);
         for (size_t d = 0; d < start.size(); ++d) start[d] = std::clamp(start[d], lower[d], upper[d]);
-        tasks[v].search = std::make_unique<StageTwoSearch>(start, lower, upper, plan.ord);
+        tasks[v].search = std::make_unique<StageTwoSearch>(start, lower, upper, plan.ord, use_warm ? radius : 1.0);
         tasks[v].objective = VarianceObjective::make(sh, ss.genes[g], fixed_cell);
         plan_points(v, &box);
         waiting.push_back(v);
@@ -878,8 +889,11 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
             continue;
           }
           Flight& f = flight[g];
+          // a gene planned earlier in this pass (an audited gene whose cold
+          // twin just finished) holds tickets of -1 until the pass posts them
           bool ready = true;
-          for (size_t k = f.tickets.size(); k > 0 && ready; --k) ready = fitter.queue_done(f.tickets[k - 1]);
+          for (size_t k = f.tickets.size(); k > 0 && ready; --k)
+            ready = f.tickets[k - 1] >= 0 && fitter.queue_done(f.tickets[k - 1]);
           if (!ready) {
             ++i;
             continue;

@@ -140,6 +140,7 @@ long long RequestQueue::post(const void* requests, size_t n) {
 }
 
 bool RequestQueue::done(long long ticket) const {
+  if (ticket < 0) return false;  // not posted yet
   long long& flag = h_done_[ticket & static_cast<long long>(capacity_ - 1)];
   return std::atomic_ref<long long>(flag).load(std::memory_order_acquire) == ticket + 1;
 }

@@ -212,8 +212,8 @@ class NelderMead {
 // StageTwoSearch (nebula.rs:1607-1951)
 
 StageTwoSearch::StageTwoSearch(const std::vector<double>& start, const std::vector<double>& lower,
-                               const std::vector<double>& upper, int ord)
-    : lower_(lower), upper_(upper), start_(start), order_(ord) {
+                               const std::vector<double>& upper, int ord, double radius_scale)
+    : lower_(lower), upper_(upper), start_(start), order_(ord), radius_scale_(radius_scale) {
   begin_pass();
 }
 
@@ -233,7 +233,8 @@ void StageTwoSearch::begin_pass() {
   failed_ = false;
   if (start_.size() == 2) {
     std::vector<double> x0 = clamped(start_);
-    bobyqa_ = std::make_unique<Bobyqa>(x0.data(), lower_.data(), upper_.data(), 2);
+    bobyqa_ = std::make_unique<Bobyqa>(x0.data(), lower_.data(), upper_.data(), 2, 1e-6, 1000, radius_scale_);
+    radius_scale_ = 1.0;
     if (!bobyqa_->ok()) {
       bobyqa_.reset();
       end_pass(std::nullopt);

@@ -29,8 +29,11 @@ class NelderMead;  // the one-component simplex of NEBULA-LN's restricted refit
 // clamped minimiser once more, and three quadratic polish stencils.
 class StageTwoSearch {
  public:
+  // `radius_scale` < 1 narrows the first BOBYQA pass's initial trust region
+  // (Bobyqa's radius_scale) for a start believed close to the optimum; a
+  // restarted pass uses the full radius.
   StageTwoSearch(const std::vector<double>& start, const std::vector<double>& lower,
-                 const std::vector<double>& upper, int ord);
+                 const std::vector<double>& upper, int ord, double radius_scale = 1.0);
   ~StageTwoSearch();
   int order() const { return order_; }
   bool done() const { return stage_ == Stage::Done; }
@@ -56,6 +59,7 @@ class StageTwoSearch {
 
   std::vector<double> lower_, upper_, start_;
   int order_;
+  double radius_scale_ = 1.0;
   bool invalid_ = false;
   Stage stage_ = Stage::Start;
   std::vector<std::vector<double>> asked_;

@@ -127,6 +127,9 @@ typedef struct nb_options {
   const double* warm_points; /* warm_start 2: n_genes x 2 starts (sigma, gamma) */
   int32_t* evaluations;  /* optional out: stage-two objective evaluations per
                             kept gene (the kept genes' order of nb_fit) */
+  double warm_radius;    /* warm start only: the search's initial BOBYQA trust
+                            radius as a fraction of NLopt's (the final radius
+                            stays NLopt's); 0 = the library default, 1 = NLopt's */
 } nb_options;
 
 /* Counters of one call (timings in milliseconds of host wall clock, device
@@ -284,6 +287,14 @@ typedef struct nb_bobyqa nb_bobyqa;
 nb_bobyqa* nb_bobyqa_new(const double* x0, const double* lower,
                          const double* upper, uint32_t n, double xtol_rel,
                          uint32_t maxeval);
+/* As nb_bobyqa_new with the initial trust radius at radius_scale (0, 1] of
+ * NLopt's and the final radius NLopt's (xtol_rel times the unscaled initial
+ * radius): the warm search of nb_options.warm_radius. No counterpart in the
+ * reference; radius_scale 1 is nb_bobyqa_new. */
+nb_bobyqa* nb_bobyqa_new_scaled(const double* x0, const double* lower,
+                                const double* upper, uint32_t n,
+                                double xtol_rel, uint32_t maxeval,
+                                double radius_scale);
 int32_t nb_bobyqa_ask(const nb_bobyqa* h, double* x); /* 1: x pending */
 void nb_bobyqa_tell(nb_bobyqa* h, double value);
 /* returns the NLopt status: 4 xtol, 5 maxeval, 1 success, -4 roundoff */

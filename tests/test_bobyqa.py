@@ -47,11 +47,14 @@ CASES = [
 ]
 
 
-def run(f, x0, lo, hi):
+def run(f, x0, lo, hi, radius_scale=None):
     lib = _ffi.product_library()
     n = len(x0)
     arr = lambda v: (ctypes.c_double * n)(*v)
-    h = lib.nb_bobyqa_new(arr(x0), arr(lo), arr(hi), n, 1e-6, 1000)
+    if radius_scale is None:
+        h = lib.nb_bobyqa_new(arr(x0), arr(lo), arr(hi), n, 1e-6, 1000)
+    else:
+        h = lib.nb_bobyqa_new_scaled(arr(x0), arr(lo), arr(hi), n, 1e-6, 1000, radius_scale)
     assert h
     trace = []
     x = (ctypes.c_double * n)()
@@ -88,3 +91,36 @@ def test_bobyqa_refuses_a_box_narrower_than_two_radii():
     arr = lambda v: (ctypes.c_double * 2)(*v)
     # the initial radius is a quarter of the narrowest side; a degenerate side refuses
     assert not lib.nb_bobyqa_new(arr([0.0, 0.0]), arr([0.0, 0.0]), arr([0.0, 1.0]), 2, 1e-6, 1000)
+
+
+def test_scaled_radius_one_is_nlopts_search():
+    for tag, f, x0, lo, hi, _ in CASES:
+        a, *_ = run(f, x0, lo, hi)
+        b, *_ = run(f, x0, lo, hi, radius_scale=1.0)
+        assert np.array_equal(a, b), tag
+
+
+def bowl(x):
+    """A smooth objective shaped like the variance search's near its optimum."""
+    a, b = np.log(x[0] / 0.45), np.log(x[1] / 2.0)
+    return 3.0 * a * a + 0.8 * a * b + 0.5 * b * b + 0.2 * a * a * a
+
+
+def test_scaled_radius_from_a_close_start_saves_evaluations():
+    """From a start within 1% of the minimum, in the variance search's box,
+    a search whose trust region starts at 3% of NLopt's radius ends at the
+    same minimum (the final radius is NLopt's) in fewer evaluations."""
+    x0, lo, hi = [0.454, 1.98], [1e-4, 1e-4], [10.0, 1000.0]
+    _, x_full, f_full, n_full, _ = run(bowl, x0, lo, hi)
+    _, x_warm, f_warm, n_warm, st = run(bowl, x0, lo, hi, radius_scale=0.03)
+    assert st == 4  # xtol reached
+    assert n_warm < 0.8 * n_full, (n_warm, n_full)
+    assert np.allclose(x_warm, [0.45, 2.0], rtol=1e-5) and np.allclose(x_full, [0.45, 2.0], rtol=1e-5)
+    assert f_warm < 1e-10 and f_full < 1e-10
+
+
+def test_scaled_radius_still_travels_from_a_far_start():
+    """A start far from the minimum with a narrow initial region: the region
+    grows with successful steps and the search still reaches the minimum."""
+    _, x, f, _, _ = run(rosen, [-1.2, 1.0], [-2.0, -1.0], [2.0, 3.0], radius_scale=0.03)
+    assert np.allclose(x, [1.0, 1.0], atol=1e-4) and f < 1e-8
