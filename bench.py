@@ -44,14 +44,28 @@ METRIC = "NEBULA-HL genes/s @100k cells, 1 B200: warm-start+batched vs plain; ro
 PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "fit_kernel_traffic.json")
 
 
-def flops_per_visit(nb):
-    """FP64 operations of one cell visit of the fit kernel's sweep.
+def flops_per_visit(nv):
+    """FP64 operations of one cell visit of the fit kernel's sweep, whose
+    per-cell work covers only the nv design columns that vary within
+    subjects (the subject-constant columns' shares are applied per subject).
 
-    eta (nb FMAs), exp (34), t, log (35), 1/t and the fold scalars (5), the
-    fold: resid and weight (2), per column X'd FMA, p x and its sum (4 nb),
-    the p x x' triangle (nb(nb+1) as FMAs); an FMA counts two, a division one.
+    eta (the offset plus the subject's constant share, then nv FMAs), exp
+    (34), t, log (35), 1/t and the fold scalars (5), the fold: resid and
+    weight (2), per varying column X'd FMA, p x and its sum (4 nv), the p x x'
+    triangle (nv(nv+1) as FMAs); an FMA counts two, a division one.
     """
-    return 2 * nb + 1 + 34 + 1 + 35 + 5 + 1 + 2 + 4 * nb + nb * (nb + 1)
+    return 2 * nv + 1 + 34 + 1 + 35 + 5 + 1 + 2 + 4 * nv + nv * (nv + 1)
+
+
+def varying_columns(design, subject):
+    """How many design columns take more than one value within some subject
+    (the reference's cell_level_columns, ptmg.rs:1962-2005)."""
+    order = np.argsort(subject, kind="stable")
+    x, sid = design[order], subject[order]
+    starts = np.flatnonzero(np.r_[True, sid[1:] != sid[:-1]])
+    lo = np.minimum.reduceat(x, starts, axis=0)
+    hi = np.maximum.reduceat(x, starts, axis=0)
+    return int(np.sum(np.any(lo != hi, axis=0)))
 
 
 def parse():
@@ -241,7 +255,8 @@ def ours_arm(args, world, rank, local, dist):
     fp64_peak = measure_fp64_tflops(5)
     # the fit kernel is the whole step (one persistent launch serves stages
     # two and three), so its FLOP are divided by the step's device time
-    achieved = visits * flops_per_visit(work.n_coef) / (float(np.sum(step_ms)) / 1000.0) / 1e12
+    n_varying = varying_columns(work.design, work.subject)
+    achieved = visits * flops_per_visit(n_varying) / (float(np.sum(step_ms)) / 1000.0) / 1e12
     traffic = None
     if os.path.exists(PROFILE_SUMMARY):
         try:
@@ -302,7 +317,8 @@ def ours_arm(args, world, rank, local, dist):
                                                 "warm": float(fit.evaluations.mean())}},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                      "frac": achieved / fp64_peak if fp64_peak > 0 else None, "traffic": traffic,
-                     "kernel": "fit_kernel", "flops_per_visit": flops_per_visit(work.n_coef),
+                     "kernel": "fit_kernel", "flops_per_visit": flops_per_visit(n_varying),
+                     "varying_columns": n_varying,
                      "time": "device time of the step (CUDA events around the persistent launch)",
                      "peak_source": "measured on this GPU: FP64 FMA chains (nb_measure_fp64_tflops)"},
         "e2e": {"value": float(np.mean(e2e_vals)) if e2e_vals else None, "unit": "genes/s",

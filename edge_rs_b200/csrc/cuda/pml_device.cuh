@@ -7,6 +7,7 @@
 // resolution is ~1e-6, retraces the same points.
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
 
 namespace nebula {
@@ -63,7 +64,36 @@ struct GeneData {
   int32_t n_cells;
   int32_t n_subjects;
   int32_t n_coef;
+  // The columns that vary within some subject, increasing (the reference's
+  // cell_level_columns, ptmg.rs:1962-2005); every other column is constant
+  // within each subject, and a sweep applies its share per subject instead
+  // of per cell.
+  int32_t n_varying;
+  int32_t varying[kMaxCoef];
 };
+
+// The columns of a row-major n_cells x n_coef design that take more than one
+// value within some subject (subjects are the contiguous blocks between
+// fid[s] and fid[s + 1]); writes them increasing into `out` and returns how
+// many there are.
+template <typename Boundary>
+inline int varying_columns(const double* design, int n_coef, const Boundary* fid, int n_subjects, int32_t* out) {
+  int n = 0;
+  for (int j = 0; j < n_coef; ++j) {
+    bool varies = false;
+    for (int s = 0; s < n_subjects && !varies; ++s) {
+      if (fid[s] >= fid[s + 1]) continue;
+      const double first = design[static_cast<size_t>(fid[s]) * n_coef + j];
+      for (size_t i = static_cast<size_t>(fid[s]) + 1; i < static_cast<size_t>(fid[s + 1]); ++i)
+        if (design[i * n_coef + j] != first) {
+          varies = true;
+          break;
+        }
+    }
+    if (varies) out[n++] = j;
+  }
+  return n;
+}
 
 struct FitControl {
   double eps;
@@ -71,8 +101,9 @@ struct FitControl {
   int32_t max_backtrack;
 };
 
-// Shared-memory bytes one fit CTA needs for n_subjects and n_coef.
-size_t fit_smem_bytes(int n_subjects, int n_coef);
+// Shared-memory bytes one fit CTA needs for n_subjects, n_coef columns and
+// n_varying of them varying within subjects.
+size_t fit_smem_bytes(int n_subjects, int n_coef, int n_varying);
 
 // Launches the persistent fit kernel over *n_requests (read on the device)
 // requests; `counter` must be zeroed before each launch (work queue).
@@ -108,14 +139,14 @@ int launch_fit_queue(const GeneData& data, const FitControl& ctl, const FitQueue
                      void* stream);
 
 // Clusters of `cluster` CTAs the streaming kernel can keep resident at once.
-int fit_queue_max_clusters(int n_subjects, int n_coef, int cluster);
+int fit_queue_max_clusters(int n_subjects, int n_coef, int n_varying, int cluster);
 
 // CTAs per SM the fit kernel can keep resident for this shape.
-int fit_blocks_per_sm(int n_subjects, int n_coef);
+int fit_blocks_per_sm(int n_subjects, int n_coef, int n_varying);
 
 // Clusters of `cluster` CTAs the fit kernel can keep resident at once (0 if
 // none fits).
-int fit_max_clusters(int n_subjects, int n_coef, int cluster);
+int fit_max_clusters(int n_subjects, int n_coef, int n_varying, int cluster);
 
 }  // namespace device
 }  // namespace nebula

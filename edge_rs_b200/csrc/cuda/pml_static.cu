@@ -103,9 +103,11 @@ namespace nebula {
 namespace device {
 namespace {
 
-// Checks the subject blocks and positive cells, and writes the derived
-// per-subject layout and the request records into the scratch array.
-__global__ void stage_noalloc(unsigned char* scratch, Layout L, const uint64_t* subject_start, uint32_t k,
+// Checks the subject blocks and positive cells, marks the design columns
+// that vary within a subject (header[3], one bit per column), and writes the
+// derived per-subject layout and the request records into the scratch array.
+__global__ void stage_noalloc(unsigned char* scratch, Layout L, const double* design,
+                              const uint64_t* subject_start, uint32_t k,
                               uint64_t n_cells, const uint32_t* cells, uint64_t n_pos, uint32_t n_req,
                               uint32_t n_beta, const double* beta_init, const double* subject, const double* cell,
                               const int32_t* ord, int32_t reml) {
@@ -123,6 +125,18 @@ __global__ void stage_noalloc(unsigned char* scratch, Layout L, const uint64_t* 
   for (uint64_t i = tid; i < n_pos; i += stride) {
     const uint32_t c = cells[i];
     if (c >= n_cells || (i > 0 && c <= cells[i - 1])) atomicOr(&header[2], kBadCells);
+  }
+  for (uint64_t r = tid; r < n_cells; r += stride) {
+    // the subject block holding cell r: the last s with subject_start[s] <= r
+    uint64_t lo = 0, hi = k;
+    while (lo < hi) {
+      const uint64_t mid = lo + (hi - lo + 1) / 2;
+      if (subject_start[mid] <= r) lo = mid; else hi = mid - 1;
+    }
+    const uint64_t first = subject_start[lo];
+    if (first >= r) continue;  // r starts its block (or the blocks are malformed)
+    for (uint32_t j = 0; j < n_beta; ++j)
+      if (design[r * n_beta + j] != design[first * n_beta + j]) atomicOr(&header[3], 1 << j);
   }
   for (uint64_t s = tid; s <= k; s += stride) {
     const uint64_t b = subject_start[s];
@@ -256,10 +270,6 @@ NB_API int32_t nb_opt_pml_cuda_noalloc(const double* design, const double* offse
       fail(NB_ERR_INVALID_ARGUMENT, "null request or output array");
 
     const DeviceSlot slot = slot_for_current_device();
-    const int per_sm = fit_blocks_per_sm(static_cast<int>(k), static_cast<int>(n_beta));
-    if (per_sm <= 0)
-      fail(NB_ERR_UNSUPPORTED, "the fit kernel cannot be resident with " + std::to_string(k) + " subjects and " +
-                                   std::to_string(n_beta) + " columns");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const Layout L = layout_for(k, n_requests);
     unsigned char* base = slot.scratch;
@@ -270,15 +280,19 @@ NB_API int32_t nb_opt_pml_cuda_noalloc(const double* design, const double* offse
     if (k + uint64_t{1} > items) items = k + uint64_t{1};
     if (n_requests > items) items = n_requests;
     if (static_cast<uint64_t>(kRanges) + 1 > items) items = kRanges + 1;
+    if (n_cells > items) items = n_cells;
     uint64_t blocks = (items + kStageThreads - 1) / kStageThreads;
     const uint64_t max_blocks = static_cast<uint64_t>(slot.sms) * 8;
     if (blocks > max_blocks) blocks = max_blocks;
     stage_noalloc<<<static_cast<unsigned>(blocks), kStageThreads, 0, st>>>(
-        base, L, subject_start, k, n_cells, cells, n_pos, n_requests, n_beta, beta_init, subject, cell, ord, reml);
+        base, L, design, subject_start, k, n_cells, cells, n_pos, n_requests, n_beta, beta_init, subject, cell, ord,
+        reml);
     check(cudaGetLastError(), "staging launch");
-    int32_t flags = 0;
-    check(cudaMemcpyAsync(&flags, header + 2, sizeof(int32_t), cudaMemcpyDeviceToHost, st), "validation flags");
+    int32_t flags_mask[2] = {0, 0};  // validation flags, varying columns
+    check(cudaMemcpyAsync(flags_mask, header + 2, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, st),
+          "validation flags");
     check(cudaStreamSynchronize(st), "staging");
+    const int32_t flags = flags_mask[0];
     if (flags & kBadSubjectRange) fail(NB_ERR_INVALID_ARGUMENT, "subject_start must run from 0 to n_cells");
     if (flags & kBadSubjectBlock) fail(NB_ERR_SUBJECTS_NOT_CONTIGUOUS, "empty or unordered subject block");
     if (flags & kBadCells)
@@ -299,6 +313,13 @@ NB_API int32_t nb_opt_pml_cuda_noalloc(const double* design, const double* offse
     data.n_cells = static_cast<int32_t>(n_cells);
     data.n_subjects = static_cast<int32_t>(k);
     data.n_coef = static_cast<int32_t>(n_beta);
+    data.n_varying = 0;
+    for (uint32_t j = 0; j < n_beta; ++j)
+      if (flags_mask[1] & (1 << j)) data.varying[data.n_varying++] = static_cast<int32_t>(j);
+    const int per_sm = fit_blocks_per_sm(static_cast<int>(k), static_cast<int>(n_beta), data.n_varying);
+    if (per_sm <= 0)
+      fail(NB_ERR_UNSUPPORTED, "the fit kernel cannot be resident with " + std::to_string(k) + " subjects and " +
+                                   std::to_string(n_beta) + " columns");
     FitControl ctl{};
     ctl.eps = eps;
     ctl.max_iter = kPmlMaxIter;

@@ -150,6 +150,7 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
   data_.n_cells = static_cast<int32_t>(sh.n_cells);
   data_.n_subjects = K;
   data_.n_coef = sh.n_coef;
+  data_.n_varying = device::varying_columns(sh.design.data(), sh.n_coef, sh.fid.data(), K, data_.varying);
   {
     // per gene two (beta, log_w) slots for warm inner starts
     double* warm = nullptr;
@@ -165,15 +166,15 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
   int sms = 0, dev = 0;
   cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
   cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute");
-  int per_sm = device::fit_blocks_per_sm(K, sh.n_coef);
+  int per_sm = device::fit_blocks_per_sm(K, sh.n_coef, data_.n_varying);
   if (per_sm <= 0)
     fail(NB_ERR_UNSUPPORTED, "the fit kernel cannot be resident with " + std::to_string(K) +
                                  " subjects and " + std::to_string(sh.n_coef) + " columns");
   grid_ = per_sm * sms;
   for (int c = 2; c <= device::kMaxCluster; c *= 2)
-    max_clusters_[c] = device::fit_max_clusters(K, sh.n_coef, c);
+    max_clusters_[c] = device::fit_max_clusters(K, sh.n_coef, data_.n_varying, c);
   for (int c = 1; c <= device::kMaxCluster; c *= 2)
-    queue_clusters_[c] = device::fit_queue_max_clusters(K, sh.n_coef, c);
+    queue_clusters_[c] = device::fit_queue_max_clusters(K, sh.n_coef, data_.n_varying, c);
   for (Lane& lane : lanes_) {
     cuda_check(cudaStreamCreateWithFlags(&lane.stream, cudaStreamNonBlocking), "cudaStreamCreate");
     cuda_check(cudaEventCreate(&lane.ev0), "event");
@@ -452,6 +453,12 @@ const device::FitResult* DeviceFitter::run(const std::vector<device::FitRequest>
 
 namespace {
 
+// Admission order of stage two's requests: a warm search takes about this
+// share of the plain search's evaluations (c1, initial radius 0.03), and a
+// cold fit about this many warm fits' sweeps.
+constexpr double kWarmEvaluationShare = 0.62;
+constexpr double kColdFitCost = 1.5;
+
 // Default initial trust radius of a warm search, as a fraction of NLopt's.
 // On 500 genes x 100,000 cells (stage one's start within about 1%) it cuts
 // the search's evaluations by 38% against the full radius; on genes drawn
@@ -489,6 +496,9 @@ struct Session {
   std::vector<int> tune_candidates;
   std::vector<double> tune_ms;
   int tuned = 0;
+  // the warm-start network's outputs per kept gene (mlp::kOut each), computed
+  // on the session's first fit; empty until then
+  std::vector<float> net_y;
 };
 
 int choose_cluster(Session& ss, size_t G) {
@@ -656,13 +666,32 @@ std::unique_ptr<Session> create_session(const nb_csr* counts, const uint64_t* su
 }
 
 // Starts of the warm-started searches: the caller's points (warm_start 2) or
-// the network's prediction from the genes' features (warm_start 1), with the
-// network's log evaluation budget; a non-finite or non-positive start falls
-// back to stage one's.
-void warm_starts(Session& ss, std::vector<std::array<double, 2>>* point, std::vector<double>* budget) {
+// the network's prediction from the genes' features (warm_start 1); a
+// non-finite or non-positive start falls back to stage one's.
+// The warm-start network's outputs for every kept gene (cached in the
+// session): log-corrections of stage one's (sigma, gamma) and the log of the
+// plain search's evaluation count.
+const std::vector<float>& network_outputs(Session& ss) {
   const Shared& sh = ss.prep.shared;
   const size_t G = ss.genes.size();
   const int K = sh.n_subjects;
+  if (ss.net_y.size() == G * mlp::kOut) return ss.net_y;
+  std::vector<float> features(G * mlp::kIn), y(G * mlp::kOut);
+  parallel_for(G, ss.opt.host_threads, [&](size_t g) {
+    warm_features(sh, ss.genes[g], &ss.prep.totals[ss.prep.kept[g] * K], ss.plans[g], &features[g * mlp::kIn]);
+  });
+  const float* params = ss.opt.mlp_weights ? ss.opt.mlp_weights : builtin_mlp_params();
+  char err[256] = {};
+  if (G > 0) {
+    const int32_t rc = nb_mlp_predict_cuda(params, features.data(), G, y.data(), err, sizeof(err));
+    if (rc != NB_OK) fail(rc, std::string("warm-start network: ") + err);
+  }
+  ss.net_y = std::move(y);
+  return ss.net_y;
+}
+
+void warm_starts(Session& ss, std::vector<std::array<double, 2>>* point) {
+  const size_t G = ss.genes.size();
   for (size_t g = 0; g < G; ++g) (*point)[g] = {ss.plans[g].sigma, ss.plans[g].gamma};
   auto accept = [&](size_t g, double sigma, double gamma) {
     if (std::isfinite(sigma) && sigma > 0.0) (*point)[g][0] = sigma;
@@ -677,14 +706,7 @@ void warm_starts(Session& ss, std::vector<std::array<double, 2>>* point, std::ve
     }
     return;
   }
-  std::vector<float> features(G * mlp::kIn), y(G * mlp::kOut);
-  parallel_for(G, ss.opt.host_threads, [&](size_t g) {
-    warm_features(sh, ss.genes[g], &ss.prep.totals[ss.prep.kept[g] * K], ss.plans[g], &features[g * mlp::kIn]);
-  });
-  const float* params = ss.opt.mlp_weights ? ss.opt.mlp_weights : builtin_mlp_params();
-  char err[256] = {};
-  const int32_t rc = nb_mlp_predict_cuda(params, features.data(), G, y.data(), err, sizeof(err));
-  if (rc != NB_OK) fail(rc, std::string("warm-start network: ") + err);
+  const std::vector<float>& y = network_outputs(ss);
   // Corrections smaller than about twice the network's held-out error
   // (log-ratio 0.07) are dropped: stage one's start is then as good.
   constexpr double kGate = 0.07;
@@ -693,7 +715,6 @@ void warm_starts(Session& ss, std::vector<std::array<double, 2>>* point, std::ve
     const double d0 = gate(static_cast<double>(y[g * mlp::kOut + 0]));
     const double d1 = gate(static_cast<double>(y[g * mlp::kOut + 1]));
     accept(g, ss.plans[g].sigma * std::exp(d0), ss.plans[g].gamma * std::exp(d1));
-    (*budget)[g] = y[g * mlp::kOut + 2];
   }
 }
 
@@ -718,8 +739,14 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
   // search's best objective is worse.
   const int warm = (ss.opt.warm_start >= 1 && ss.opt.warm_start <= 3) ? ss.opt.warm_start : 0;
   std::vector<std::array<double, 2>> warm_point(G);
-  std::vector<double> budget(G, 0.0);
-  if (warm) warm_starts(ss, &warm_point, &budget);
+  if (warm) warm_starts(ss, &warm_point);
+  // the plain search's predicted evaluation count per gene (the network's
+  // third output), for the order in which requests are admitted
+  std::vector<double> budget(G);
+  {
+    const std::vector<float>& y = network_outputs(ss);
+    for (size_t g = 0; g < G; ++g) budget[g] = std::exp(std::clamp(static_cast<double>(y[g * mlp::kOut + 2]), 0.0, 8.0));
+  }
   // The warm search's initial trust radius, a fraction of NLopt's.
   const double radius = ss.opt.warm_radius > 0.0 ? std::min(ss.opt.warm_radius, 1.0) : kWarmRadius;
   std::vector<size_t> audit_of;
@@ -822,18 +849,77 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
     box->owners.emplace_back(g, 0);
     box->reqs.push_back(r);
   };
-  auto post = [&](Outbox* box, int poster, DeviceFitter::Tally* tally) {
-    if (box->reqs.empty()) return;
-    const long long first = fitter.queue_post(box->reqs.data(), box->reqs.size(), poster, tally);
-    for (size_t k = 0; k < box->owners.size(); ++k)
-      flight[box->owners[k].first].tickets[box->owners[k].second] = first + static_cast<long long>(k);
-    box->reqs.clear();
-    box->owners.clear();
-  };
   const int hw = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
   const int workers = std::max(1, std::min<int>({ss.opt.host_threads > 0 ? ss.opt.host_threads : hw, 8,
                                                  static_cast<int>(std::max<size_t>(G, 1))}));
   const int cluster = choose_cluster(ss, G);
+  // Admission. A gene's search is a chain of dependent evaluations, so the
+  // step ends when the longest chains do. Requests in the ring are served
+  // in ticket order, so posting every ready request at once would advance
+  // all genes at the same slow pace and leave the long chains for last with
+  // the SMs idle. Instead at most `cap` requests are in flight (twice the
+  // fits the kernel runs at once); the others wait in a heap keyed by their
+  // task's predicted remaining work (longest first: the cold audit searches,
+  // then the genes the network predicts to need the most evaluations, the
+  // final fits last). The results do not depend on the order.
+  struct Entry {
+    double priority;
+    uint64_t order;
+    size_t v;
+    std::vector<device::FitRequest> reqs;
+  };
+  auto entry_less = [](const Entry& a, const Entry& b) {
+    return a.priority < b.priority || (a.priority == b.priority && a.order > b.order);
+  };
+  std::mutex gate_mu;
+  std::vector<Entry> heap;
+  uint64_t gate_order = 0;
+  long long in_flight = 0;
+  const long long cap = 2 * static_cast<long long>(std::max(1, fitter.resident_fits(cluster)));
+  // predicted remaining evaluations of task v, in units of a warm fit
+  auto remaining = [&](size_t v) {
+    const bool cold = !(warm && v < G);
+    const double predicted = budget[gene_of(v)] * (cold ? 1.0 : kWarmEvaluationShare);
+    const double done = static_cast<double>(tasks[v].search->evaluations());
+    return std::max(predicted - done, 1.0) * (cold ? kColdFitCost : 1.0) + 1.0;
+  };
+  // Queues the box's requests and posts from the heap while room remains;
+  // `released` requests of the caller's have been consumed since its last call.
+  auto post = [&](Outbox* box, long long released, int poster, DeviceFitter::Tally* tally) {
+    std::lock_guard<std::mutex> lock(gate_mu);
+    in_flight -= released;
+    for (size_t k = 0; k < box->reqs.size();) {
+      Entry e;
+      e.v = box->owners[k].first;
+      e.order = gate_order++;
+      e.priority = flight[e.v].final_fit ? 1.0 : remaining(e.v);
+      for (; k < box->reqs.size() && box->owners[k].first == e.v; ++k) e.reqs.push_back(box->reqs[k]);
+      heap.push_back(std::move(e));
+      std::push_heap(heap.begin(), heap.end(), entry_less);
+    }
+    box->reqs.clear();
+    box->owners.clear();
+    std::vector<device::FitRequest> batch;
+    std::vector<std::pair<size_t, size_t>> owners;
+    while (!heap.empty()) {
+      const long long n = static_cast<long long>(heap.front().reqs.size());
+      if (in_flight > 0 && in_flight + n > cap) break;
+      std::pop_heap(heap.begin(), heap.end(), entry_less);
+      Entry e = std::move(heap.back());
+      heap.pop_back();
+      for (size_t k = 0; k < e.reqs.size(); ++k) {
+        batch.push_back(e.reqs[k]);
+        owners.emplace_back(e.v, k);
+      }
+      in_flight += n;
+    }
+    if (batch.empty()) return;
+    const long long first = fitter.queue_post(batch.data(), batch.size(), poster, tally);
+    // another worker may own these tasks: it reads the tickets with acquire loads
+    for (size_t k = 0; k < owners.size(); ++k)
+      std::atomic_ref<long long>(flight[owners[k].first].tickets[owners[k].second])
+          .store(first + static_cast<long long>(k), std::memory_order_release);
+  };
   std::vector<DeviceFitter::Tally> tallies(workers);
   std::vector<uint64_t> steps(workers, 0);
   std::atomic<bool> abort{false};
@@ -876,12 +962,13 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
           plan_final(g, &box);
           waiting.push_back(g);
         }
-        if (box.reqs.size() >= 64) post(&box, w, tally);
+        if (box.reqs.size() >= 64) post(&box, 0, w, tally);
       }
-      post(&box, w, tally);
+      post(&box, 0, w, tally);
       auto last_progress = Clock::now();
       while (!waiting.empty() && !abort.load(std::memory_order_relaxed)) {
         bool progressed = false;
+        long long released = 0;  // this pass's consumed requests
         for (size_t i = 0; i < waiting.size();) {
           const size_t g = waiting[i];
           if (parked[g]) {
@@ -892,14 +979,17 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
           // a gene planned earlier in this pass (an audited gene whose cold
           // twin just finished) holds tickets of -1 until the pass posts them
           bool ready = true;
-          for (size_t k = f.tickets.size(); k > 0 && ready; --k)
-            ready = f.tickets[k - 1] >= 0 && fitter.queue_done(f.tickets[k - 1]);
+          for (size_t k = f.tickets.size(); k > 0 && ready; --k) {
+            const long long t = std::atomic_ref<long long>(f.tickets[k - 1]).load(std::memory_order_acquire);
+            ready = t >= 0 && fitter.queue_done(t);
+          }
           if (!ready) {
             ++i;
             continue;
           }
           progressed = true;
           ++steps[w];
+          released += static_cast<long long>(f.tickets.size());
           if (f.final_fit) {
             fitter.queue_account(f.tickets[0], static_cast<int>(g), tally);
             const device::FitResult& r = fitter.queue_result(f.tickets[0]);
@@ -974,7 +1064,7 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
           }
           ++i;
         }
-        post(&box, w, tally);
+        if (released > 0 || !box.reqs.empty()) post(&box, released, w, tally);
         if (progressed) {
           last_progress = Clock::now();
         } else {

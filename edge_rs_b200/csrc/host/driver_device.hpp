@@ -68,6 +68,8 @@ class DeviceFitter {
   [[noreturn]] void queue_failure(const char* what);
   // CTAs per request for a stage with `requests` requests in flight.
   int cluster_for(size_t requests) const;
+  // Fits the streaming kernel runs at once with `cluster` CTAs per fit.
+  int resident_fits(int cluster) const { return queue_clusters_[cluster]; }
   // Stage one in streaming mode (device::PtmgQueue), the same protocol as
   // the fit queue below; a result is ptmg_stride() doubles.
   void ptmg_queue_start(size_t capacity);

@@ -75,14 +75,73 @@ namespace {
 // sum y ln t, X'd (nb), sum p x (nb), sum p x x' (upper triangle).
 enum { kResid = 0, kWeight = 1, kSumLog = 2, kLinear = 3, kWlog = 4, kScore = 5 };
 
-double eta_of(const PmlData& d, const std::vector<double>& beta, size_t r) {
-  const double* row = d.design + r * d.n_beta;
-  double eta = d.offset[r];
-  for (int j = 0; j < d.n_beta; ++j) eta = nebula::nb_fma(row[j], beta[j], eta);
+// The design columns that take more than one value within some subject (the
+// reference's cell_level_columns, ptmg.rs:1962-2005), increasing; vpos[a] is
+// column a's index among them, or -1 for a column constant within every
+// subject. A sweep sums only the varying columns per cell and applies each
+// constant column's share per subject.
+struct Split {
+  std::vector<int> varying, vpos;
+};
+
+Split split_columns(const PmlData& d) {
+  Split sp;
+  sp.vpos.assign(d.n_beta, -1);
+  for (int j = 0; j < d.n_beta; ++j) {
+    bool varies = false;
+    for (int s = 0; s < d.k && !varies; ++s) {
+      if (d.subject_start[s] >= d.subject_start[s + 1]) continue;
+      const double first = d.design[d.subject_start[s] * d.n_beta + j];
+      for (size_t r = d.subject_start[s] + 1; r < d.subject_start[s + 1] && !varies; ++r)
+        varies = d.design[r * d.n_beta + j] != first;
+    }
+    if (varies) {
+      sp.vpos[j] = static_cast<int>(sp.varying.size());
+      sp.varying.push_back(j);
+    }
+  }
+  return sp;
+}
+
+// Subject s's design row (its constant columns' values); zeros for a subject
+// without cells.
+std::vector<double> subject_row(const PmlData& d, int s) {
+  std::vector<double> x(d.n_beta, 0.0);
+  if (d.subject_start[s] < d.subject_start[s + 1])
+    for (int a = 0; a < d.n_beta; ++a) x[a] = d.design[d.subject_start[s] * d.n_beta + a];
+  return x;
+}
+
+// Per subject, the constant columns' share of eta (cs, in column order) and
+// cs + log_w.
+void constant_shares(const PmlData& d, const Split& sp, const std::vector<double>& beta,
+                     const std::vector<double>& log_w, std::vector<double>* cs, std::vector<double>* csl) {
+  cs->assign(d.k, 0.0);
+  csl->assign(d.k, 0.0);
+  for (int s = 0; s < d.k; ++s) {
+    const std::vector<double> x = subject_row(d, s);
+    double c = 0.0;
+    for (int a = 0; a < d.n_beta; ++a)
+      if (sp.vpos[a] < 0) c = nebula::nb_fma(x[a], beta[a], c);
+    (*cs)[s] = c;
+    (*csl)[s] = c + log_w[s];
+  }
+}
+
+// Cell r's varying design values, and eta over them continuing from `start`.
+int varying_row(const PmlData& d, const Split& sp, size_t r, double* x) {
+  const int nv = static_cast<int>(sp.varying.size());
+  for (int j = 0; j < nv; ++j) x[j] = d.design[r * d.n_beta + sp.varying[j]];
+  return nv;
+}
+double varying_eta(const Split& sp, const double* x, const std::vector<double>& beta, double start) {
+  double eta = start;
+  for (size_t j = 0; j < sp.varying.size(); ++j) eta = nebula::nb_fma(x[j], beta[sp.varying[j]], eta);
   return eta;
 }
 
-// The fold of pml.rs:1469-1489: d into the gradient, p into the curvature.
+// The fold of pml.rs:1469-1489 over the varying columns (nb of them): d
+// into the gradient, p into the curvature.
 void fold(double* acc, const double* x, int nb, double dd, double p) {
   acc[kResid] += dd;
   acc[kWeight] += p;
@@ -107,28 +166,61 @@ void fold(double* acc, const double* x, int nb, double dd, double p) {
 void sweep(const PmlData& d, const std::vector<double>& beta, const std::vector<double>& log_w,
            double gamma, const Penalty& pen, Sweep& out) {
   const int nb = d.n_beta, k = d.k, T = nb * (nb + 1) / 2, nv = 5 + 2 * nb + T;
+  const Split sp = split_columns(d);
+  const int nr = static_cast<int>(sp.varying.size());
+  const int nsr = 5 + 2 * nr + nr * (nr + 1) / 2;  // reduced slot: the varying columns only
+  std::vector<double> cs, csl;
+  constant_shares(d, sp, beta, log_w, &cs, &csl);
   auto dense = [&](double* acc, size_t r, int s) {
-    double eta = eta_of(d, beta, r);
-    double e = nebula::nb_exp_tab(eta + log_w[s], &nebula::kNbTables);
+    double x[8];
+    varying_row(d, sp, r, x);
+    double e = nebula::nb_exp_tab(varying_eta(sp, x, beta, d.offset[r] + csl[s]), &nebula::kNbTables);
     double t = e + gamma;
     acc[kSumLog] += nebula::nb_log_tab(t, &nebula::kNbTables);
     double inv = 1.0 / t;
     double u = e * inv;
-    fold(acc, d.design + r * nb, nb, -gamma * u, (gamma * u) * inv);
+    fold(acc, x, nr, -gamma * u, (gamma * u) * inv);
   };
   auto sparse = [&](double* acc, size_t i, int s) {
     size_t c = d.cells[i];
     double y = d.counts[i];
-    double eta = eta_of(d, beta, c);
+    double x[8];
+    varying_row(d, sp, c, x);
+    double eta = varying_eta(sp, x, beta, d.offset[c] + cs[s]);
     double e = nebula::nb_exp_tab(eta + log_w[s], &nebula::kNbTables);
     double t = e + gamma;
     acc[kLinear] = nebula::nb_fma(eta, y, acc[kLinear]);
     acc[kWlog] = nebula::nb_fma(y, nebula::nb_log_tab(t, &nebula::kNbTables), acc[kWlog]);
     double inv = 1.0 / t;
     double u = e * inv;
-    fold(acc, d.design + c * nb, nb, y * (1.0 - u), (y * u) * inv);
+    fold(acc, x, nr, y * (1.0 - u), (y * u) * inv);
   };
-  std::vector<double> tot = range_sums(d, nv, dense, sparse);
+  const std::vector<double> red = range_sums(d, nsr, dense, sparse);
+  // every column's sums per subject: a constant column a's are its value
+  // times the matching sums without it
+  std::vector<double> tot(static_cast<size_t>(k) * nv);
+  for (int s = 0; s < k; ++s) {
+    const double* R = &red[static_cast<size_t>(s) * nsr];
+    const std::vector<double> X = subject_row(d, s);
+    double* F = &tot[static_cast<size_t>(s) * nv];
+    for (int x = 0; x < kScore; ++x) F[x] = R[x];
+    for (int a = 0; a < nb; ++a) {
+      const int va = sp.vpos[a];
+      F[kScore + a] = va >= 0 ? R[kScore + va] : X[a] * R[kResid];
+      F[kScore + nb + a] = va >= 0 ? R[kScore + nr + va] : X[a] * R[kWeight];
+    }
+    int t = 0;
+    for (int a = 0; a < nb; ++a)
+      for (int b = a; b < nb; ++b, ++t) {
+        const int va = sp.vpos[a], vb = sp.vpos[b];
+        double v;
+        if (va >= 0 && vb >= 0) v = R[kScore + 2 * nr + va * nr - va * (va - 1) / 2 + (vb - va)];
+        else if (vb >= 0) v = X[a] * R[kScore + nr + vb];
+        else if (va >= 0) v = X[b] * R[kScore + nr + va];
+        else v = X[a] * (X[b] * R[kWeight]);
+        F[kScore + 2 * nb + t] = v;
+      }
+  }
   std::vector<double> llv(k);
   for (int s = 0; s < k; ++s) {
     const double* S = &tot[static_cast<size_t>(s) * nv];
@@ -256,11 +348,19 @@ double laplace_correction(const PmlData& d, const std::vector<double>& beta, con
     acc[2] += scale * (p4 * (gamma * gamma + e2 - (4.0 * gamma) * e));
     acc[3] += scale * (p5 * (gamma * gamma * gamma - (11.0 * gamma * gamma) * e + (11.0 * gamma) * e2 - e2 * e));
   };
+  const Split sp = split_columns(d);
+  std::vector<double> cs, csl;
+  constant_shares(d, sp, beta, log_w, &cs, &csl);
   auto dense = [&](double* acc, size_t r, int s) {
-    terms(nebula::nb_exp_tab(eta_of(d, beta, r) + log_w[s], &nebula::kNbTables), gamma, acc);
+    double x[8];
+    varying_row(d, sp, r, x);
+    terms(nebula::nb_exp_tab(varying_eta(sp, x, beta, d.offset[r] + csl[s]), &nebula::kNbTables), gamma, acc);
   };
   auto sparse = [&](double* acc, size_t i, int s) {
-    terms(nebula::nb_exp_tab(eta_of(d, beta, d.cells[i]) + log_w[s], &nebula::kNbTables), d.counts[i], acc);
+    double x[8];
+    varying_row(d, sp, d.cells[i], x);
+    const double eta = varying_eta(sp, x, beta, d.offset[d.cells[i]] + cs[s]);
+    terms(nebula::nb_exp_tab(eta + log_w[s], &nebula::kNbTables), d.counts[i], acc);
   };
   std::vector<double> tot = range_sums(d, 4, dense, sparse);
   double third_acc = 0, fourth_acc = 0, fifth_acc = 0;
