@@ -338,7 +338,11 @@ def ours_arm(args, world, rank, local, dist):
                                                                    * 1e-3 * clocks["sm_mhz"] * 1e6)
                    if clocks.get("sm_mhz") else None,
                    "cycles_per_visit_per_cta": stats[-1]["slot_cycles"] / stats[-1]["cell_visits"],
-                   "ctas_per_fit": stats[-1]["cluster"]},
+                   "ctas_per_fit": stats[-1]["cluster"], "fit_slots": stats[-1]["fit_slots"],
+                   # device time from the first fit's start to the last fit's end, and
+                   # the step's device time outside it (start-up and the drain)
+                   "busy_span_ms": stats[-1]["ms_busy_span"],
+                   "outside_span_ms": stats[-1]["ms_step_device"] - stats[-1]["ms_busy_span"]},
     }
     print(json.dumps(line), flush=True)
 

@@ -37,6 +37,7 @@ struct alignas(16) FitResult {
   double information[kMaxCoef * kMaxCoef];
   int32_t iterations, backtracks, sweeps, status;  // status 0 ok, 1 rejected arguments
   int64_t cycles;  // SM clock cycles the request held its CTAs (summed over the cluster)
+  int64_t start_ns, end_ns;  // global timer when the fit began and ended
   int64_t pad;
 };
 

@@ -651,6 +651,12 @@ __device__ double determinant(double* a) {
   return det;
 }
 
+__device__ __forceinline__ long long global_ns() {
+  long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 // One inner fit (optimise, pml.rs:1614-1800) by the calling cluster: every
 // CTA of the cluster runs it in step (each sweep shared over the cluster's
 // CTAs) and rank 0 writes the result to `out`.
@@ -660,6 +666,7 @@ __device__ void fit_one(const GeneData& d, const FitControl& ctl, Smem<NB, NV>& 
   const int K = sm.K;
   const int tid = threadIdx.x;
   const int gene = req.gene;
+  const long long ns_start = global_ns();
 
   // gamma_penalty (pml.rs:432-441) and the argument checks of optimise
   const double exps = nb_exp(req.subject);
@@ -670,6 +677,8 @@ __device__ void fit_one(const GeneData& d, const FitControl& ctl, Smem<NB, NV>& 
       out->iterations = 0;
       out->sweeps = 0;
       out->cycles = 0;
+      out->start_ns = ns_start;
+      out->end_ns = global_ns();
     }
     return;
   }
@@ -889,6 +898,8 @@ __device__ void fit_one(const GeneData& d, const FitControl& ctl, Smem<NB, NV>& 
     out->sweeps = static_cast<int32_t>(sm.sc[kSweeps]);
     out->status = 0;
     out->cycles = (clock64() - t_start) * cl.size;  // every CTA of the cluster was busy
+    out->start_ns = ns_start;
+    out->end_ns = global_ns();
   }
 }
 
@@ -975,12 +986,6 @@ __global__ void __launch_bounds__(kThreads, min_blocks(NB, NV)) fit_kernel(GeneD
     const FitRequest req = requests[q];
     fit_one<NB, NV>(d, ctl, sm, req, results + q, cl, parity, clock64());
   }
-}
-
-__device__ __forceinline__ long long global_ns() {
-  long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
 }
 
 // Streaming mode (FitQueue): one persistent launch for a whole stage.

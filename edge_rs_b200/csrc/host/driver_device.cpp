@@ -190,6 +190,8 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
 void DeviceFitter::reset_counters() {
   device_ms_ = 0.0;
   launches_ = requests_ = sweeps_ = cell_visits_ = slot_cycles_ = h2d_bytes_ = d2h_bytes_ = 0;
+  first_ns_ = INT64_MAX;
+  last_ns_ = INT64_MIN;
 }
 
 void DeviceFitter::begin_step() {
@@ -414,6 +416,8 @@ void DeviceFitter::queue_account(long long ticket, int gene, Tally* tally) const
   tally->sweeps += sw;
   tally->cell_visits += sw * (n_cells_ + gene_nnz_[static_cast<size_t>(gene)]);
   tally->slot_cycles += static_cast<uint64_t>(r.cycles);
+  tally->first_ns = std::min<int64_t>(tally->first_ns, r.start_ns);
+  tally->last_ns = std::max<int64_t>(tally->last_ns, r.end_ns);
 }
 
 void DeviceFitter::add_tally(const Tally& t) {
@@ -423,6 +427,8 @@ void DeviceFitter::add_tally(const Tally& t) {
   slot_cycles_ += t.slot_cycles;
   h2d_bytes_ += t.h2d;
   d2h_bytes_ += t.d2h;
+  first_ns_ = std::min(first_ns_, t.first_ns);
+  last_ns_ = std::max(last_ns_, t.last_ns);
 }
 
 bool DeviceFitter::queue_running() { return fitq_.running(); }
@@ -850,7 +856,7 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
     box->reqs.push_back(r);
   };
   const int hw = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
-  const int workers = std::max(1, std::min<int>({ss.opt.host_threads > 0 ? ss.opt.host_threads : hw, 8,
+  const int workers = std::max(1, std::min<int>({ss.opt.host_threads > 0 ? ss.opt.host_threads : std::min(hw, 8), 32,
                                                  static_cast<int>(std::max<size_t>(G, 1))}));
   const int cluster = choose_cluster(ss, G);
   // Admission. A gene's search is a chain of dependent evaluations, so the
@@ -962,7 +968,7 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
           plan_final(g, &box);
           waiting.push_back(g);
         }
-        if (box.reqs.size() >= 64) post(&box, 0, w, tally);
+        post(&box, 0, w, tally);  // every gene's first request as soon as it is planned
       }
       post(&box, 0, w, tally);
       auto last_progress = Clock::now();
@@ -1114,7 +1120,7 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
     stats->requests = fitter.requests();
     stats->sweeps = fitter.sweeps();
     stats->cell_visits = fitter.cell_visits();
-    stats->fit_slots = static_cast<uint64_t>(fitter.grid());
+    stats->fit_slots = static_cast<uint64_t>(fitter.queue_grid(cluster));
     stats->slot_cycles = fitter.slot_cycles();
     stats->cluster = static_cast<uint64_t>(cluster);
     stats->audited = audit_of.size();
@@ -1122,6 +1128,7 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
     stats->gpu_launches = fitter.launches();
     stats->ms_prepare = ss.ms_prepare;
     stats->ms_upload = ss.ms_upload;
+    stats->ms_busy_span = fitter.busy_span_ms();
     stats->ms_stage_one = ss.ms_stage_one;
     stats->ms_stage_two = ms_stage_two;
     stats->ms_stage_three = ms_stage_three;

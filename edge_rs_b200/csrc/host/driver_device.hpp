@@ -53,6 +53,7 @@ class DeviceFitter {
   static constexpr int kMaxPosters = 8;
   struct Tally {
     uint64_t requests = 0, sweeps = 0, cell_visits = 0, slot_cycles = 0, h2d = 0, d2h = 0;
+    int64_t first_ns = INT64_MAX, last_ns = INT64_MIN;  // earliest fit start, latest fit end
   };
   void queue_start(int cluster);
   long long queue_post(const device::FitRequest* reqs, size_t n, int poster, Tally* tally);
@@ -88,6 +89,11 @@ class DeviceFitter {
   uint64_t sweeps() const { return sweeps_; }
   uint64_t cell_visits() const { return cell_visits_; }
   uint64_t slot_cycles() const { return slot_cycles_; }
+  // Device time from the first fit's start to the last fit's end since the
+  // last reset_counters, in ms (0 before any fit).
+  double busy_span_ms() const { return last_ns_ > first_ns_ ? (last_ns_ - first_ns_) / 1e6 : 0.0; }
+  // CTAs the streaming kernel launches with `cluster` CTAs per fit.
+  int queue_grid(int cluster) const { return queue_clusters_[cluster] * cluster; }
   int grid() const { return grid_; }
   int lanes() const { return static_cast<int>(lanes_.size()); }
   uint64_t h2d_bytes() const { return h2d_bytes_; }
@@ -132,6 +138,7 @@ class DeviceFitter {
   int pgrid_ = 0;
   double device_ms_ = 0.0;
   uint64_t launches_ = 0, requests_ = 0, sweeps_ = 0, cell_visits_ = 0, slot_cycles_ = 0;
+  int64_t first_ns_ = INT64_MAX, last_ns_ = INT64_MIN;
   uint64_t h2d_bytes_ = 0, d2h_bytes_ = 0;
 };
 

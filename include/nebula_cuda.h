@@ -151,6 +151,8 @@ typedef struct nb_stats {
   uint64_t slot_cycles;     /* SM clock cycles the fit CTAs spent on requests */
   uint64_t cluster;         /* CTAs that shared each fit in stages two and three */
   double ms_upload;         /* host wall time of the device upload */
+  double ms_busy_span;      /* device time from the first fit's start to the
+                               last fit's end in stages two and three */
 } nb_stats;
 
 void nb_params_default(nb_params* params);
