@@ -249,7 +249,8 @@ void DeviceFitter::ptmg_queue_start(size_t capacity) {
   ++launches_;
 }
 
-long long DeviceFitter::ptmg_post(const device::PtmgRequest* reqs, size_t n) { return ptmgq_->post(reqs, n); }
+long long DeviceFitter::ptmg_post(const device::PtmgRequest* reqs, size_t n) { return ptmgq_->try_post(reqs, n); }
+void DeviceFitter::ptmg_consumed(long long ticket) { ptmgq_->consumed(ticket); }
 bool DeviceFitter::ptmg_done(long long ticket) const { return ptmgq_->done(ticket); }
 const double* DeviceFitter::ptmg_result(long long ticket) const {
   return static_cast<const double*>(ptmgq_->result(ticket));
@@ -567,7 +568,7 @@ std::unique_ptr<Session> create_session(const nb_csr* counts, const uint64_t* su
   size_t capacity = 256;
   while (capacity < 2 * G && capacity < 4096) capacity *= 2;
   const int hw = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
-  const int workers = std::max(1, std::min<int>({ss->opt.host_threads > 0 ? ss->opt.host_threads : hw, 8,
+  const int workers = std::max(1, std::min<int>({ss->opt.host_threads > 0 ? ss->opt.host_threads : 2 * hw, 32,
                                                  static_cast<int>(std::max<size_t>(G, 1))}));
   std::atomic<bool> abort{false};
   std::mutex err_mu;
@@ -590,6 +591,7 @@ std::unique_ptr<Session> create_session(const nb_csr* counts, const uint64_t* su
       auto post = [&]() {
         if (box.empty()) return;
         const long long first = ss->fitter->ptmg_post(box.data(), box.size());
+        if (first < 0) return;  // a slot's previous result is unread: retry after this worker's next pass
         for (size_t k = 0; k < owners.size(); ++k) ticket[owners[k]] = first + static_cast<long long>(k);
         box.clear();
         owners.clear();
@@ -621,6 +623,8 @@ std::unique_ptr<Session> create_session(const nb_csr* counts, const uint64_t* su
           sums.cumsumxtb.assign(r, r + K);
           sums.ylin.assign(r + K, r + 2 * K);
           sums.sums.assign(r + 2 * K, r + stride);
+          ss->fitter->ptmg_consumed(ticket[g]);
+          ticket[g] = -1;
           MarginalGene mg{&sh, &ss->genes[g], &ss->prep.totals[ss->prep.kept[g] * K], xy[g].data()};
           x.assign(search[g]->ask(), search[g]->ask() + np);
           const double f = ptmg_assemble(mg, x.data(), sums, grad.data(), hess.data());
@@ -856,9 +860,17 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
     box->reqs.push_back(r);
   };
   const int hw = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
-  const int workers = std::max(1, std::min<int>({ss.opt.host_threads > 0 ? ss.opt.host_threads : std::min(hw, 8), 32,
+  // Twice as many workers as hardware threads: a worker mostly polls for
+  // results and yields, and more of them turn results around sooner (on 16
+  // threads, warm c1: 6267 genes/s with 16 workers, 7061 with 32).
+  const int workers = std::max(1, std::min<int>({ss.opt.host_threads > 0 ? ss.opt.host_threads : 2 * hw, 32,
                                                  static_cast<int>(std::max<size_t>(G, 1))}));
   const int cluster = choose_cluster(ss, G);
+  std::vector<DeviceFitter::Tally> tallies(workers + 1);  // the workers', then the poster's
+  std::vector<uint64_t> steps(workers, 0);
+  std::atomic<bool> abort{false};
+  std::mutex err_mu;
+  std::optional<NbError> first_err;
   // Admission. A gene's search is a chain of dependent evaluations, so the
   // step ends when the longest chains do. Requests in the ring are served
   // in ticket order, so posting every ready request at once would advance
@@ -889,9 +901,9 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
     const double done = static_cast<double>(tasks[v].search->evaluations());
     return std::max(predicted - done, 1.0) * (cold ? kColdFitCost : 1.0) + 1.0;
   };
-  // Queues the box's requests and posts from the heap while room remains;
-  // `released` requests of the caller's have been consumed since its last call.
-  auto post = [&](Outbox* box, long long released, int poster, DeviceFitter::Tally* tally) {
+  // Workers queue their ready requests here (`released` of theirs have been
+  // consumed since their last call); the poster thread below posts them.
+  auto post = [&](Outbox* box, long long released, int, DeviceFitter::Tally*) {
     std::lock_guard<std::mutex> lock(gate_mu);
     in_flight -= released;
     for (size_t k = 0; k < box->reqs.size();) {
@@ -905,33 +917,63 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
     }
     box->reqs.clear();
     box->owners.clear();
+  };
+  // One poster thread drains the heap while room remains and posts each
+  // drain as one batch outside the lock, so workers never wait on the copies
+  // and the batches grow while a post is under way (posting from every
+  // worker held the lock for half of the step, one or two requests a post).
+  std::atomic<int> workers_left{0};
+  auto poster = [&](DeviceFitter::Tally* tally) {
     std::vector<device::FitRequest> batch;
     std::vector<std::pair<size_t, size_t>> owners;
-    while (!heap.empty()) {
-      const long long n = static_cast<long long>(heap.front().reqs.size());
-      if (in_flight > 0 && in_flight + n > cap) break;
-      std::pop_heap(heap.begin(), heap.end(), entry_less);
-      Entry e = std::move(heap.back());
-      heap.pop_back();
-      for (size_t k = 0; k < e.reqs.size(); ++k) {
-        batch.push_back(e.reqs[k]);
-        owners.emplace_back(e.v, k);
+    try {
+      while (!abort.load(std::memory_order_relaxed)) {
+        batch.clear();
+        owners.clear();
+        bool idle = false;
+        {
+          std::lock_guard<std::mutex> lock(gate_mu);
+          while (!heap.empty()) {
+            const long long n = static_cast<long long>(heap.front().reqs.size());
+            if (in_flight > 0 && in_flight + n > cap) break;
+            std::pop_heap(heap.begin(), heap.end(), entry_less);
+            Entry e = std::move(heap.back());
+            heap.pop_back();
+            for (size_t k = 0; k < e.reqs.size(); ++k) {
+              batch.push_back(e.reqs[k]);
+              owners.emplace_back(e.v, k);
+            }
+            in_flight += n;
+            if (batch.size() >= 4096) break;
+          }
+          idle = batch.empty() && heap.empty() && workers_left.load() == 0;
+        }
+        if (idle) return;
+        if (batch.empty()) {
+          std::this_thread::yield();
+          continue;
+        }
+        const long long first = fitter.queue_post(batch.data(), batch.size(), 0, tally);
+        // the owning workers read the tickets with acquire loads
+        for (size_t k = 0; k < owners.size(); ++k)
+          std::atomic_ref<long long>(flight[owners[k].first].tickets[owners[k].second])
+              .store(first + static_cast<long long>(k), std::memory_order_release);
       }
-      in_flight += n;
+    } catch (const NbError& e) {
+      std::lock_guard<std::mutex> lock(err_mu);
+      if (!first_err) first_err = e;
+      abort.store(true);
+    } catch (const std::exception& e) {
+      std::lock_guard<std::mutex> lock(err_mu);
+      if (!first_err) first_err = NbError{NB_ERR_GPU, e.what()};
+      abort.store(true);
     }
-    if (batch.empty()) return;
-    const long long first = fitter.queue_post(batch.data(), batch.size(), poster, tally);
-    // another worker may own these tasks: it reads the tickets with acquire loads
-    for (size_t k = 0; k < owners.size(); ++k)
-      std::atomic_ref<long long>(flight[owners[k].first].tickets[owners[k].second])
-          .store(first + static_cast<long long>(k), std::memory_order_release);
   };
-  std::vector<DeviceFitter::Tally> tallies(workers);
-  std::vector<uint64_t> steps(workers, 0);
-  std::atomic<bool> abort{false};
-  std::mutex err_mu;
-  std::optional<NbError> first_err;
   auto worker = [&](int w) {
+    struct Leave {
+      std::atomic<int>& left;
+      ~Leave() { left.fetch_sub(1); }
+    } leave{workers_left};
     try {
       DeviceFitter::Tally* tally = &tallies[w];
       Outbox box;
@@ -1009,6 +1051,7 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
             ff.log_likelihood = r.log_likelihood;
             ff.iterations = r.iterations;
             ff.backtracks = r.backtracks;
+            fitter.queue_consumed(f.tickets[0]);
             waiting[i] = waiting.back();
             waiting.pop_back();
             continue;
@@ -1031,6 +1074,7 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
             wvalid[g][wb] = f.anchor >= 0 && fitter.queue_result(f.tickets[static_cast<size_t>(f.anchor)]).status == 0;
             ++wstep[g];
           }
+          for (long long t : f.tickets) fitter.queue_consumed(t);
           t.search->tell(values);
           if (t.search->done()) {
             t.refit = t.search->result();
@@ -1095,10 +1139,13 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
       ~QueueGuard() { f.queue_abort(); }
     } guard{fitter};
     fitter.queue_start(cluster);
+    workers_left.store(workers);
+    std::thread post_thread(poster, &tallies[workers]);
     std::vector<std::thread> pool;
     for (int w = 1; w < workers; ++w) pool.emplace_back(worker, w);
     worker(0);
     for (auto& th : pool) th.join();
+    post_thread.join();
     if (first_err) throw *first_err;
     fitter.queue_stop();
   }

@@ -59,6 +59,8 @@ class DeviceFitter {
   long long queue_post(const device::FitRequest* reqs, size_t n, int poster, Tally* tally);
   bool queue_done(long long ticket) const;
   const device::FitResult& queue_result(long long ticket) const;
+  // The caller has read ticket's result (RequestQueue::consumed).
+  void queue_consumed(long long ticket) { fitq_.consumed(ticket); }
   void queue_account(long long ticket, int gene, Tally* tally) const;
   void add_tally(const Tally& t);
   bool queue_running();
@@ -74,7 +76,9 @@ class DeviceFitter {
   // Stage one in streaming mode (device::PtmgQueue), the same protocol as
   // the fit queue below; a result is ptmg_stride() doubles.
   void ptmg_queue_start(size_t capacity);
+  // -1 (nothing posted) while a slot's previous result is unread (try_post)
   long long ptmg_post(const device::PtmgRequest* reqs, size_t n);
+  void ptmg_consumed(long long ticket);
   bool ptmg_done(long long ticket) const;
   const double* ptmg_result(long long ticket) const;
   bool ptmg_running();

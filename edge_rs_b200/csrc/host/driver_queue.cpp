@@ -69,6 +69,8 @@ void RequestQueue::start(cudaStream_t stream, const std::function<cudaError_t(co
   }
   // tickets restart at zero: no stale sequence number or done flag may match one
   std::memset(h_done_, 0, cap * sizeof(long long));
+  if (!consumed_) consumed_.reset(new std::atomic<long long>[cap]);
+  for (size_t i = 0; i < cap; ++i) consumed_[i].store(0);
   next_.store(0);
   check(cudaMemsetAsync(d_seq_, 0xff, cap * sizeof(long long), stream), "memset");
   check(cudaMemsetAsync(d_stop_, 0, sizeof(int), stream), "memset");
@@ -108,27 +110,46 @@ void RequestQueue::copy_range(void* dst, const void* src, size_t elem, long long
   }
 }
 
-long long RequestQueue::post(const void* requests, size_t n) {
+long long RequestQueue::post(const void* requests, size_t n) { return post_impl(requests, n, true); }
+
+long long RequestQueue::try_post(const void* requests, size_t n) { return post_impl(requests, n, false); }
+
+void RequestQueue::consumed(long long ticket) {
+  if (ticket >= 0) consumed_[ticket & static_cast<long long>(capacity_ - 1)].store(ticket + 1, std::memory_order_release);
+}
+
+// Ticket t may take its slot once the slot's previous ticket, t - capacity,
+// has been read.
+bool RequestQueue::slot_free(long long t) const {
+  const long long cap = static_cast<long long>(capacity_);
+  return t < cap || consumed_[t & (cap - 1)].load(std::memory_order_acquire) == t - cap + 1;
+}
+
+long long RequestQueue::post_impl(const void* requests, size_t n, bool wait) {
   if (n == 0) return next_.load();
   if (n > capacity_ / 2) fail(NB_ERR_GPU, "too many requests in one post");
   // One post at a time through one stream: copies from several streams into
   // neighbouring ring slots lost updates.
   std::lock_guard<std::mutex> lock(post_mu_);
-  const long long first = next_.fetch_add(static_cast<long long>(n));
+  const long long first = next_.load();
   const long long cap = static_cast<long long>(capacity_);
   const long long mask = cap - 1;
+  for (size_t i = 0; i < n; ++i) {
+    const long long t = first + static_cast<long long>(i);
+    if (slot_free(t)) continue;
+    if (!wait) return -1;
+    // the slot's previous result has not been read yet: wait for it (bounded)
+    const auto t0 = std::chrono::steady_clock::now();
+    while (!slot_free(t)) {
+      if (!running()) failure("ended with work pending");
+      if (ms_since(t0) > 60000.0) failure("made no progress for 60 s");
+      std::this_thread::yield();
+    }
+  }
+  next_.store(first + static_cast<long long>(n));
   const char* src = static_cast<const char*>(requests);
   for (size_t i = 0; i < n; ++i) {
     const long long t = first + static_cast<long long>(i);
-    if (t >= cap && !done(t - cap)) {
-      // the slot still holds an unfinished request: wait for it (bounded)
-      const auto t0 = std::chrono::steady_clock::now();
-      while (!done(t - cap)) {
-        if (!running()) failure("ended with work pending");
-        if (ms_since(t0) > 60000.0) failure("made no progress for 60 s");
-        std::this_thread::yield();
-      }
-    }
     std::memcpy(h_ring_ + static_cast<size_t>(t & mask) * request_bytes_, src + i * request_bytes_,
                 request_bytes_);
     h_seq_[t & mask] = t;

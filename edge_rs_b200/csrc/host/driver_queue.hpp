@@ -9,6 +9,7 @@
 #include <atomic>
 #include <cstddef>
 #include <functional>
+#include <memory>
 #include <mutex>
 #include <string>
 
@@ -40,8 +41,15 @@ class RequestQueue {
   // persistent kernel on `stream` (after the resets, which run on it).
   void start(cudaStream_t stream, const std::function<cudaError_t(const View&)>& launch);
   // Copies n requests into the ring (safe from several host threads; one at
-  // a time) and returns the first one's ticket.
+  // a time) and returns the first one's ticket. A slot is reused only once
+  // the result of the ticket it last held has been read (consumed()); post
+  // waits for that (bounded), try_post returns -1 instead and posts nothing.
+  // A thread that reads results itself must use try_post: it could otherwise
+  // wait on a result only it would read.
   long long post(const void* requests, size_t n);
+  long long try_post(const void* requests, size_t n);
+  // The caller has read ticket's result: its slot may take a new ticket.
+  void consumed(long long ticket);
   bool done(long long ticket) const;
   const void* result(long long ticket) const;
   bool running();
@@ -57,6 +65,8 @@ class RequestQueue {
  private:
   void stop_impl(bool check);
   void copy_range(void* dst, const void* src, size_t elem, long long first, size_t n);
+  long long post_impl(const void* requests, size_t n, bool wait);
+  bool slot_free(long long ticket) const;
   size_t request_bytes_, result_bytes_, capacity_;
   char* d_ring_ = nullptr;
   long long* d_seq_ = nullptr;
@@ -71,6 +81,7 @@ class RequestQueue {
   cudaStream_t post_stream_ = nullptr;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr, ready_ = nullptr;
   std::atomic<long long> next_{0};
+  std::unique_ptr<std::atomic<long long>[]> consumed_;  // per slot: last ticket read + 1
   std::mutex post_mu_;
   bool running_ = false;
   double device_ms_ = 0.0;

@@ -119,7 +119,8 @@ typedef struct nb_fit {
 typedef struct nb_options {
   int32_t device;        /* CUDA ordinal; -1 = current device */
   int32_t warm_start;    /* 0 plain, 1 learned, 2 caller's starts, 3 stage one's */
-  int32_t host_threads;  /* host threads; 0 = all cores */
+  int32_t host_threads;  /* worker threads stepping the genes' searches; 0 =
+                            twice the hardware threads, at most 32 */
   int32_t audit_percent; /* warm start only: share of genes also run cold */
   const float* mlp_weights; /* warm_start 1: NB_MLP_PARAMS floats; NULL = built-in */
   int32_t cluster;       /* CTAs sharing each inner fit in stages two and three
