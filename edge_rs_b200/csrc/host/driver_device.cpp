@@ -68,12 +68,35 @@ void parallel_for(size_t n, int threads, F&& f) {
   if (first_err) throw first_err->second;
 }
 
+// The per-call arrays come from the device's default memory pool in stream
+// order and go back to it in stream order when the call ends. The pool keeps
+// what is freed (release threshold raised once per device), so a later call
+// takes its arrays from it instead of allocating, and no call waits for a
+// synchronous free at its end.
+void keep_pool_memory() {
+  static std::atomic<bool> done[64];
+  int dev = 0;
+  cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+  if (dev < 0 || dev >= 64 || done[dev].exchange(true)) return;
+  cudaMemPool_t pool = nullptr;
+  cuda_check(cudaDeviceGetDefaultMemPool(&pool, dev), "default memory pool");
+  uint64_t keep = UINT64_MAX;
+  cuda_check(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "memory pool threshold");
+}
+
 template <typename T>
-T* device_copy(const T* host, size_t n, std::vector<void*>* owned) {
+T* pool_alloc(size_t n, cudaStream_t stream, std::vector<void*>* pooled) {
   T* d = nullptr;
-  cuda_check(cudaMalloc(reinterpret_cast<void**>(&d), std::max<size_t>(n, 1) * sizeof(T)), "cudaMalloc");
-  owned->push_back(d);
-  if (n) cuda_check(cudaMemcpy(d, host, n * sizeof(T), cudaMemcpyHostToDevice), "cudaMemcpy H2D");
+  cuda_check(cudaMallocAsync(reinterpret_cast<void**>(&d), std::max<size_t>(n, 1) * sizeof(T), stream),
+             "cudaMallocAsync");
+  pooled->push_back(d);
+  return d;
+}
+
+template <typename T>
+T* device_copy(const T* host, size_t n, cudaStream_t stream, std::vector<void*>* pooled) {
+  T* d = pool_alloc<T>(n, stream, pooled);
+  if (n) cuda_check(cudaMemcpyAsync(d, host, n * sizeof(T), cudaMemcpyHostToDevice, stream), "H2D copy");
   return d;
 }
 
@@ -87,6 +110,7 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
   const Shared& sh = prep.shared;
   if (device >= 0) cuda_check(cudaSetDevice(device), "cudaSetDevice");
   cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  keep_pool_memory();
   const int K = sh.n_subjects;
   const size_t G = genes.size();
   std::vector<uint64_t> gene_ptr(G + 1, 0);
@@ -133,17 +157,17 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
     }
   }
 
-  data_.design = device_copy(sh.design.data(), sh.design.size(), &owned_);
-  data_.log_offset = device_copy(sh.log_offset.data(), sh.log_offset.size(), &owned_);
-  data_.fid = device_copy(fid.data(), fid.size(), &owned_);
-  data_.gene_ptr = device_copy(gene_ptr.data(), gene_ptr.size(), &owned_);
-  data_.cells = device_copy(cells.get(), nnz, &owned_);
-  data_.counts = device_copy(counts.get(), nnz, &owned_);
-  data_.runs = device_copy(runs.data(), runs.size(), &owned_);
-  data_.totals = device_copy(totals.data(), totals.size(), &owned_);
-  data_.warp_cells = device_copy(wcells.data(), wcells.size(), &owned_);
-  data_.range_cells = device_copy(rcells.data(), rcells.size(), &owned_);
-  data_.range_pos = device_copy(rpos.data(), rpos.size(), &owned_);
+  data_.design = device_copy(sh.design.data(), sh.design.size(), stream_, &pooled_);
+  data_.log_offset = device_copy(sh.log_offset.data(), sh.log_offset.size(), stream_, &pooled_);
+  data_.fid = device_copy(fid.data(), fid.size(), stream_, &pooled_);
+  data_.gene_ptr = device_copy(gene_ptr.data(), gene_ptr.size(), stream_, &pooled_);
+  data_.cells = device_copy(cells.get(), nnz, stream_, &pooled_);
+  data_.counts = device_copy(counts.get(), nnz, stream_, &pooled_);
+  data_.runs = device_copy(runs.data(), runs.size(), stream_, &pooled_);
+  data_.totals = device_copy(totals.data(), totals.size(), stream_, &pooled_);
+  data_.warp_cells = device_copy(wcells.data(), wcells.size(), stream_, &pooled_);
+  data_.range_cells = device_copy(rcells.data(), rcells.size(), stream_, &pooled_);
+  data_.range_pos = device_copy(rpos.data(), rpos.size(), stream_, &pooled_);
   h2d_bytes_ = (sh.design.size() + sh.log_offset.size() + nnz + totals.size()) * sizeof(double) +
                (fid.size() + nnz + wcells.size() + rcells.size()) * sizeof(uint32_t) +
                (gene_ptr.size() + runs.size() + rpos.size()) * sizeof(uint64_t);
@@ -153,11 +177,8 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
   data_.n_varying = device::varying_columns(sh.design.data(), sh.n_coef, sh.fid.data(), K, data_.varying);
   {
     // per gene two (beta, log_w) slots for warm inner starts
-    double* warm = nullptr;
     const size_t doubles = std::max<size_t>(G, 1) * 2 * static_cast<size_t>(sh.n_coef + K);
-    cuda_check(cudaMalloc(reinterpret_cast<void**>(&warm), doubles * sizeof(double)), "cudaMalloc");
-    owned_.push_back(warm);
-    data_.warm_state = warm;
+    data_.warm_state = pool_alloc<double>(doubles, stream_, &pooled_);
   }
   ctl_.eps = sh.params.eps;
   ctl_.max_iter = kPmlMaxIter;
@@ -175,14 +196,6 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
     max_clusters_[c] = device::fit_max_clusters(K, sh.n_coef, data_.n_varying, c);
   for (int c = 1; c <= device::kMaxCluster; c *= 2)
     queue_clusters_[c] = device::fit_queue_max_clusters(K, sh.n_coef, data_.n_varying, c);
-  for (Lane& lane : lanes_) {
-    cuda_check(cudaStreamCreateWithFlags(&lane.stream, cudaStreamNonBlocking), "cudaStreamCreate");
-    cuda_check(cudaEventCreate(&lane.ev0), "event");
-    cuda_check(cudaEventCreate(&lane.ev1), "event");
-    cuda_check(cudaMalloc(reinterpret_cast<void**>(&lane.d_counter), 2 * sizeof(int32_t)), "cudaMalloc");
-    owned_.push_back(lane.d_counter);
-    cuda_check(cudaMallocHost(reinterpret_cast<void**>(&lane.h_header), 2 * sizeof(int32_t)), "cudaMallocHost");
-  }
   cuda_check(cudaEventCreate(&step0_), "event");
   cuda_check(cudaEventCreate(&step1_), "event");
 }
@@ -196,11 +209,26 @@ void DeviceFitter::reset_counters() {
 
 void DeviceFitter::begin_step() {
   cuda_check(cudaEventRecord(step0_, stream_), "event");
-  for (Lane& lane : lanes_) cuda_check(cudaStreamWaitEvent(lane.stream, step0_, 0), "stream wait");
+  for (Lane& lane : lanes_)
+    if (lane.stream) cuda_check(cudaStreamWaitEvent(lane.stream, step0_, 0), "stream wait");
+}
+
+// A batch lane's stream, events and counters, made on its first use (only
+// the kernel-level entry runs batches); the lane's work follows stream_'s.
+void DeviceFitter::ensure_lane(Lane& lane) {
+  if (lane.stream) return;
+  cuda_check(cudaStreamCreateWithFlags(&lane.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  cuda_check(cudaEventCreate(&lane.ev0), "event");
+  cuda_check(cudaEventCreate(&lane.ev1), "event");
+  lane.d_counter = pool_alloc<int32_t>(2, stream_, &pooled_);
+  cuda_check(cudaMallocHost(reinterpret_cast<void**>(&lane.h_header), 2 * sizeof(int32_t)), "cudaMallocHost");
+  cuda_check(cudaEventRecord(lane.ev0, stream_), "event");
+  cuda_check(cudaStreamWaitEvent(lane.stream, lane.ev0, 0), "stream wait");
 }
 
 double DeviceFitter::end_step() {
   for (Lane& lane : lanes_) {
+    if (!lane.stream) continue;
     cuda_check(cudaEventRecord(lane.ev1, lane.stream), "event");
     cuda_check(cudaStreamWaitEvent(stream_, lane.ev1, 0), "stream wait");
   }
@@ -218,10 +246,8 @@ void DeviceFitter::ensure_ptmg_scratch() {
   cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
   cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute");
   pgrid_ = sms;  // one CTA per SM (the kernel is bound to one resident block)
-  cuda_check(cudaMalloc(reinterpret_cast<void**>(&d_scratch_),
-                        static_cast<size_t>(pgrid_) * device::ptmg_scratch_doubles(K, data_.n_coef) * sizeof(double)),
-             "cudaMalloc");
-  owned_.push_back(d_scratch_);
+  d_scratch_ = pool_alloc<double>(static_cast<size_t>(pgrid_) * device::ptmg_scratch_doubles(K, data_.n_coef),
+                                   stream_, &pooled_);
 }
 
 size_t DeviceFitter::ptmg_stride() const {
@@ -277,7 +303,7 @@ DeviceFitter::~DeviceFitter() {
     if (lane.ev1) cudaEventDestroy(lane.ev1);
     if (lane.stream) cudaStreamDestroy(lane.stream);
   }
-  for (void* p : owned_) cudaFree(p);
+  for (void* p : pooled_) cudaFreeAsync(p, stream_);  // back to the device's pool
   if (step0_) cudaEventDestroy(step0_);
   if (step1_) cudaEventDestroy(step1_);
   if (stream_) cudaStreamDestroy(stream_);
@@ -301,6 +327,7 @@ void DeviceFitter::reserve(Lane& lane, size_t n) {
 
 void DeviceFitter::submit(int lane_index, const std::vector<device::FitRequest>& reqs) {
   Lane& lane = lanes_[lane_index];
+  ensure_lane(lane);
   const size_t n = reqs.size();
   lane.pending = n;
   if (n == 0) return;

@@ -123,6 +123,7 @@ class DeviceFitter {
     size_t pending = 0;  // requests of the batch in flight
   };
   void reserve(Lane& lane, size_t n);
+  void ensure_lane(Lane& lane);
   RequestQueue fitq_{sizeof(device::FitRequest), sizeof(device::FitResult), 16384};
   std::unique_ptr<RequestQueue> ptmgq_;
   void ensure_ptmg_scratch();
@@ -134,7 +135,7 @@ class DeviceFitter {
   size_t n_cells_ = 0;
   device::GeneData data_{};
   device::FitControl ctl_{};
-  std::vector<void*> owned_;
+  std::vector<void*> pooled_;  // stream-ordered allocations from the device's memory pool
   int grid_ = 0;
   int max_clusters_[device::kMaxCluster + 1] = {};  // resident clusters per cluster size
   // stage-one buffers

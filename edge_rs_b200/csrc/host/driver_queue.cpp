@@ -5,6 +5,7 @@
 #include <chrono>
 #include <cstring>
 #include <thread>
+#include <vector>
 
 #include "common.hpp"
 
@@ -21,6 +22,36 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
+// A ring's buffers, stream and events. Pinned and mapped host memory is slow
+// to allocate and to free, so a ring's set goes back to a process-wide pool
+// when the ring is destroyed and the next ring of the same shape on the same
+// device takes it (the memory is held until the process exits).
+struct RingSet {
+  int device;
+  size_t request_bytes, result_bytes, capacity;
+  char* d_ring;
+  long long* d_seq;
+  int* d_stop;
+  unsigned long long* d_taken;
+  int* d_status;
+  char* h_ring;
+  long long* h_seq;
+  int* h_one;
+  char* h_results;
+  long long* h_done;
+  cudaStream_t post_stream;
+  cudaEvent_t ev0, ev1, ready;
+};
+
+std::mutex& pool_mutex() {
+  static std::mutex mu;
+  return mu;
+}
+std::vector<RingSet>& ring_pool() {
+  static std::vector<RingSet>* pool = new std::vector<RingSet>();  // kept until exit
+  return *pool;
+}
+
 }  // namespace
 
 RequestQueue::RequestQueue(size_t request_bytes, size_t result_bytes, size_t capacity)
@@ -28,26 +59,44 @@ RequestQueue::RequestQueue(size_t request_bytes, size_t result_bytes, size_t cap
 
 RequestQueue::~RequestQueue() {
   abort();
-  if (post_stream_) cudaStreamSynchronize(post_stream_);
-  if (d_ring_) cudaFree(d_ring_);
-  if (d_seq_) cudaFree(d_seq_);
-  if (d_stop_) cudaFree(d_stop_);
-  if (d_taken_) cudaFree(d_taken_);
-  if (d_status_) cudaFree(d_status_);
-  if (h_ring_) cudaFreeHost(h_ring_);
-  if (h_seq_) cudaFreeHost(h_seq_);
-  if (h_one_) cudaFreeHost(h_one_);
-  if (h_results_) cudaFreeHost(h_results_);
-  if (h_done_) cudaFreeHost(h_done_);
-  if (ev0_) cudaEventDestroy(ev0_);
-  if (ev1_) cudaEventDestroy(ev1_);
-  if (ready_) cudaEventDestroy(ready_);
-  if (post_stream_) cudaStreamDestroy(post_stream_);
+  if (!d_ring_) return;
+  cudaStreamSynchronize(post_stream_);
+  std::lock_guard<std::mutex> lock(pool_mutex());
+  ring_pool().push_back(RingSet{device_, request_bytes_, result_bytes_, capacity_, d_ring_, d_seq_, d_stop_,
+                                d_taken_, d_status_, h_ring_, h_seq_, h_one_, h_results_, h_done_, post_stream_,
+                                ev0_, ev1_, ready_});
 }
 
 void RequestQueue::start(cudaStream_t stream, const std::function<cudaError_t(const View&)>& launch) {
   if (running_) fail(NB_ERR_GPU, "the work queue is already running");
   const size_t cap = capacity_;
+  if (!d_ring_) {
+    check(cudaGetDevice(&device_), "cudaGetDevice");
+    std::lock_guard<std::mutex> lock(pool_mutex());
+    std::vector<RingSet>& pool = ring_pool();
+    for (size_t i = 0; i < pool.size(); ++i) {
+      const RingSet& r = pool[i];
+      if (r.device != device_ || r.request_bytes != request_bytes_ || r.result_bytes != result_bytes_ ||
+          r.capacity != cap)
+        continue;
+      d_ring_ = r.d_ring;
+      d_seq_ = r.d_seq;
+      d_stop_ = r.d_stop;
+      d_taken_ = r.d_taken;
+      d_status_ = r.d_status;
+      h_ring_ = r.h_ring;
+      h_seq_ = r.h_seq;
+      h_one_ = r.h_one;
+      h_results_ = r.h_results;
+      h_done_ = r.h_done;
+      post_stream_ = r.post_stream;
+      ev0_ = r.ev0;
+      ev1_ = r.ev1;
+      ready_ = r.ready;
+      pool.erase(pool.begin() + static_cast<long>(i));
+      break;
+    }
+  }
   if (!d_ring_) {
     check(cudaEventCreate(&ev0_), "event");
     check(cudaEventCreate(&ev1_), "event");

@@ -84,6 +84,7 @@ class RequestQueue {
   std::unique_ptr<std::atomic<long long>[]> consumed_;  // per slot: last ticket read + 1
   std::mutex post_mu_;
   bool running_ = false;
+  int device_ = -1;
   double device_ms_ = 0.0;
 };
 
