@@ -26,10 +26,11 @@ namespace {
 
 using namespace nebula;
 
-oracle::PmlData pml_view(const Shared& sh, const GeneCounts& gc, const double* totals) {
+oracle::PmlData pml_view(const Shared& sh, const GeneCounts& gc, const double* totals,
+                         const zero::Tables* zeros) {
   return oracle::PmlData{sh.design.data(), sh.log_offset.data(), sh.n_cells, sh.n_coef,
                          gc.counts.data(), gc.cells.data(), gc.counts.size(), sh.fid.data(),
-                         sh.n_subjects, totals};
+                         sh.n_subjects, totals, zeros};
 }
 
 struct GeneStats {
@@ -37,13 +38,13 @@ struct GeneStats {
 };
 
 GeneOutcome fit_gene_cpu(const Shared& sh, const CsrView& csr, const std::vector<double>& totals,
-                         size_t g, GeneStats* stats) {
+                         size_t g, const zero::Tables* zeros, GeneStats* stats) {
   const int k = sh.n_subjects;
   const double* tot = &totals[g * k];
   GeneCounts gc = positive_indices(csr, g);
   int marginal_evaluations = 0;
   GenePlan plan = oracle::plan_gene(sh, gc, tot, &marginal_evaluations);
-  oracle::PmlData data = pml_view(sh, gc, tot);
+  oracle::PmlData data = pml_view(sh, gc, tot, zeros);
   std::optional<std::optional<std::pair<std::vector<double>, bool>>> refit;
   if (plan.refit != Refit::None) {
     std::optional<double> fixed_cell;
@@ -124,6 +125,11 @@ ORACLE_API int32_t oracle_nebula_sparse(const nb_csr* counts, const uint64_t* su
   try {
     Prepared prep = prepare(counts, subject_id, design, n_coef, offset, params);
     const size_t n = prep.kept.size();
+    // the run's zero-count tables, built once (nebula.rs:641, zeros.rs:219)
+    const Shared& sh = prep.shared;
+    zero::Tables tables;
+    const bool tabled = zero::build_tables(sh.design.data(), sh.log_offset.data(), sh.fid.data(), sh.n_subjects,
+                                           sh.n_coef, &tables, threads);
     std::vector<GeneOutcome> outcomes(n);
     std::vector<GeneStats> stats(n);
     std::vector<int> failed(n, 0);
@@ -136,7 +142,8 @@ ORACLE_API int32_t oracle_nebula_sparse(const nb_csr* counts, const uint64_t* su
         size_t i = next.fetch_add(1);
         if (i >= n) return;
         try {
-          outcomes[i] = fit_gene_cpu(prep.shared, prep.counts, prep.totals, prep.kept[i], &stats[i]);
+          outcomes[i] = fit_gene_cpu(prep.shared, prep.counts, prep.totals, prep.kept[i],
+                                     tabled ? &tables : nullptr, &stats[i]);
         } catch (const NbError& e) {
           failed[i] = 1;
           errors[i] = e;

@@ -15,11 +15,16 @@ ORACLE_API int32_t oracle_opt_pml(const double* design, const double* offset, ui
                                   const double* subject_total, const double* beta_init,
                                   const double* log_w_init, double subject, double cell,
                                   int32_t reml, double eps, int32_t ord, int32_t max_iter,
-                                  int32_t prior_lognormal, double* beta_out, double* log_w_out,
+                                  int32_t prior_lognormal, int32_t tabled, double* beta_out, double* log_w_out,
                                   double* information_out, double* scalars_out,
                                   int32_t* ints_out) {
   oracle::PmlData d{design, offset, n_cells, static_cast<int>(n_beta), counts, cells, n_pos,
                     subject_start, static_cast<int>(k), subject_total};
+  // the zero-count tables of this design and these offsets, when they apply
+  nebula::zero::Tables tables;
+  if (tabled && nebula::zero::build_tables(design, offset, subject_start, static_cast<int>(k), static_cast<int>(n_beta),
+                                           &tables))
+    d.zeros = &tables;
   oracle::PmlParams p;
   p.reml = reml != 0;
   p.eps = eps;
@@ -70,4 +75,37 @@ ORACLE_API void oracle_nbmath(int32_t which, const double* x, double* out, uint6
       default: out[i] = nebula::nb_log_tab(x[i], &nebula::kNbTables); break;
     }
   }
+}
+
+// The zero-count tables (zero_tables.hpp) of one group holding every cell of
+// log offsets log_o (n >= 32), evaluated at s[0..m): out[i * count + j] is sum
+// `from + j` (0 = L ... 5 = E) at s[i]; range_out = {s_lo, s_hi}. Returns 0,
+// or 1 when no tables were built.
+ORACLE_API int32_t oracle_zero_eval(const double* log_o, uint64_t n, const double* s, uint64_t m, int32_t from,
+                                    int32_t count, double* out, double* range_out) {
+  std::vector<double> design(n, 1.0);
+  const uint64_t fid[2] = {0, n};
+  nebula::zero::Tables t;
+  if (!nebula::zero::build_tables(design.data(), log_o, fid, 1, 1, &t) || t.groups.size() != 1) return 1;
+  for (uint64_t i = 0; i < m; ++i)
+    nebula::zero::eval(t.groups[0], t.index.data(), t.panels.data(), s[i], from, count, out + i * count);
+  range_out[0] = t.groups[0].s_lo;
+  range_out[1] = t.groups[0].s_hi;
+  return 0;
+}
+
+// How build_tables groups a design: returns the number of tabled groups (-1
+// when no tables are built); rows_out (n_cells) gets each group's design row
+// cell, loose_out (n_cells) the loose cells, *n_loose their number.
+ORACLE_API int32_t oracle_zero_groups(const double* design, const double* log_offset, const uint64_t* subject_start,
+                                      uint32_t k, uint32_t n_coef, int64_t* rows_out, uint32_t* loose_out,
+                                      uint64_t* n_loose) {
+  nebula::zero::Tables t;
+  if (!nebula::zero::build_tables(design, log_offset, subject_start, static_cast<int>(k), static_cast<int>(n_coef),
+                                  &t))
+    return -1;
+  for (size_t g = 0; g < t.groups.size(); ++g) rows_out[g] = t.groups[g].row;
+  for (size_t i = 0; i < t.loose.size(); ++i) loose_out[i] = t.loose[i];
+  *n_loose = t.loose.size();
+  return static_cast<int32_t>(t.groups.size());
 }

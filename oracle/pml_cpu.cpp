@@ -195,7 +195,25 @@ void sweep(const PmlData& d, const std::vector<double>& beta, const std::vector<
     double u = e * inv;
     fold(acc, x, nr, y * (1.0 - u), (y * u) * inv);
   };
-  const std::vector<double> red = range_sums(d, nsr, dense, sparse);
+  std::vector<double> red = range_sums(d, nsr, dense, sparse);
+  // each tabled group's cells at a count of zero (pml.rs:1515-1526): with
+  // s = ln tau, sum ln t = n ln gamma + L, sum d = -gamma A, sum p = B
+  if (d.zeros) {
+    const double ln_gamma = nebula::nb_log(gamma);
+    for (int s = 0; s < k; ++s) {
+      double* R = &red[static_cast<size_t>(s) * nsr];
+      for (uint32_t g = d.zeros->subject_groups[s]; g < d.zeros->subject_groups[s + 1]; ++g) {
+        const nebula::zero::Group& G = d.zeros->groups[g];
+        double x[8];
+        varying_row(d, sp, static_cast<size_t>(G.row), x);
+        const double log_tau = varying_eta(sp, x, beta, csl[s] - ln_gamma);
+        double f[3];
+        nebula::zero::eval(G, d.zeros->index.data(), d.zeros->panels.data(), log_tau, 0, 3, f);
+        R[kSumLog] += G.n * ln_gamma + f[0];
+        fold(R, x, nr, -gamma * f[1], f[2]);
+      }
+    }
+  }
   // every column's sums per subject: a constant column a's are its value
   // times the matching sums without it
   std::vector<double> tot(static_cast<size_t>(k) * nv);
@@ -363,6 +381,21 @@ double laplace_correction(const PmlData& d, const std::vector<double>& beta, con
     terms(nebula::nb_exp_tab(eta + log_w[s], &nebula::kNbTables), d.counts[i], acc);
   };
   std::vector<double> tot = range_sums(d, 4, dense, sparse);
+  // each tabled group's B, C, D and E (pml.rs:1875-1885)
+  if (d.zeros) {
+    const double ln_gamma = nebula::nb_log(gamma);
+    for (int s = 0; s < d.k; ++s) {
+      for (uint32_t g = d.zeros->subject_groups[s]; g < d.zeros->subject_groups[s + 1]; ++g) {
+        const nebula::zero::Group& G = d.zeros->groups[g];
+        double x[8];
+        varying_row(d, sp, static_cast<size_t>(G.row), x);
+        const double log_tau = varying_eta(sp, x, beta, csl[s] - ln_gamma);
+        double f[4];
+        nebula::zero::eval(G, d.zeros->index.data(), d.zeros->panels.data(), log_tau, 2, 4, f);
+        for (int j = 0; j < 4; ++j) tot[static_cast<size_t>(s) * 4 + j] += f[j];
+      }
+    }
+  }
   double third_acc = 0, fourth_acc = 0, fifth_acc = 0;
   for (int s = 0; s < d.k; ++s) {
     const double* S = &tot[static_cast<size_t>(s) * 4];

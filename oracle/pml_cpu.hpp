@@ -13,6 +13,8 @@
 #include <cstdint>
 #include <vector>
 
+#include "zero_tables.hpp"
+
 namespace oracle {
 
 // One gene in the layout of PmlData (pml.rs:122-136).
@@ -27,6 +29,8 @@ struct PmlData {
   const uint64_t* subject_start;  // k + 1 boundaries
   int k;
   const double* subject_total;    // k
+  // the run's zero-count tables (zeros.rs), or null to sweep every cell
+  const nebula::zero::Tables* zeros = nullptr;
 };
 
 struct PmlParams {

@@ -101,7 +101,10 @@ std::vector<double> tree_sums(const PmlData& d, const std::vector<size_t>& run, 
 // p0 + l + kLanes, ...); the partials are butterflied as above into the
 // segment's piece. A subject's total is 0 + the pieces of the non-empty
 // ranges that meet it, in range order. The tree does not depend on how many
-// warps or CTAs share the ranges.
+// warps or CTAs share the ranges. With zero-count tables (d.zeros) the dense
+// part visits only the segment's loose cells, lane l taking loose entries
+// q0 + l, q0 + l + kLanes, ... (the tabled groups are added per subject by
+// the caller).
 constexpr int kRanges = 64;
 
 inline size_t range_start(const PmlData& d, int v) { return d.n_cells * static_cast<size_t>(v) / kRanges; }
@@ -125,8 +128,16 @@ std::vector<double> range_sums(const PmlData& d, int nv, Dense cell, Sparse pos)
       const size_t s_end = std::min<size_t>(b, d.subject_start[s + 1]);
       const size_t p_end = first_entry(s_end);
       tree.clear();
-      for (int l = 0; l < kLanes; ++l)
-        for (size_t r = c0 + l; r < s_end; r += kLanes) cell(tree.lane(l), r, s);
+      if (d.zeros) {
+        const std::vector<uint32_t>& loose = d.zeros->loose;
+        const size_t q0 = static_cast<size_t>(std::lower_bound(loose.begin(), loose.end(), c0) - loose.begin());
+        const size_t q1 = static_cast<size_t>(std::lower_bound(loose.begin(), loose.end(), s_end) - loose.begin());
+        for (int l = 0; l < kLanes; ++l)
+          for (size_t q = q0 + l; q < q1; q += kLanes) cell(tree.lane(l), loose[q], s);
+      } else {
+        for (int l = 0; l < kLanes; ++l)
+          for (size_t r = c0 + l; r < s_end; r += kLanes) cell(tree.lane(l), r, s);
+      }
       for (int l = 0; l < kLanes; ++l)
         for (size_t i = pa + l; i < p_end; i += kLanes) pos(tree.lane(l), i, s);
       tree.reduce(&pieces[static_cast<size_t>(s + v) * nv]);

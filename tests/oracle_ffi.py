@@ -31,7 +31,10 @@ def _p(a):
 
 
 def opt_pml(design, offset, n_beta, counts, cells, subject_start, subject_total, beta_init, subject, cell,
-            reml=False, eps=1e-6, ord=1, max_iter=50, lognormal=False, log_w_init=None):
+            reml=False, eps=1e-6, ord=1, max_iter=50, lognormal=False, log_w_init=None, tabled=True):
+    """The oracle's opt_pml; with `tabled` the zero-count tables of the design
+    and offsets are used where they apply (as the device path does), without
+    it every cell is swept."""
     design = np.ascontiguousarray(design, np.float64)
     offset = np.ascontiguousarray(offset, np.float64)
     counts = np.ascontiguousarray(counts, np.float64)
@@ -50,7 +53,8 @@ def opt_pml(design, offset, n_beta, counts, cells, subject_start, subject_total,
                               _p(counts), _p(cells), ctypes.c_uint64(counts.size), _p(ss), ctypes.c_uint32(k),
                               _p(tot), _p(b0), _p(lw0), ctypes.c_double(subject), ctypes.c_double(cell),
                               ctypes.c_int32(int(reml)), ctypes.c_double(eps), ctypes.c_int32(ord),
-                              ctypes.c_int32(max_iter), ctypes.c_int32(int(lognormal)), _p(beta), _p(log_w),
+                              ctypes.c_int32(max_iter), ctypes.c_int32(int(lognormal)), ctypes.c_int32(int(tabled)),
+                              _p(beta), _p(log_w),
                               _p(info), _p(sc), _p(ints))
     if rc != 0:
         raise NebulaError(rc, "opt_pml rejected its arguments")
