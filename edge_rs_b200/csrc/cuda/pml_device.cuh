@@ -10,6 +10,8 @@
 #include <cstddef>
 #include <cstdint>
 
+#include "../host/zero_group.hpp"
+
 namespace nebula {
 namespace device {
 
@@ -71,6 +73,17 @@ struct GeneData {
   // of per cell.
   int32_t n_varying;
   int32_t varying[kMaxCoef];
+  // Zero-count tables (zero_group.hpp) when the design is categorical enough
+  // (zero_tables.hpp): a sweep's dense part then visits only the loose cells,
+  // and each subject's tabled groups add their looked-up sums.
+  int32_t tabled;
+  const zero::Group* zgroups;     // subject by subject
+  const uint32_t* zsubject;       // n_subjects + 1 into zgroups
+  const uint32_t* zindex;         // per base panel: first panel, depth
+  const double* zpanels;          // zero::kPanelDoubles per panel
+  const uint32_t* loose;          // cells in no tabled group, ascending
+  const uint32_t* subject_loose;  // n_subjects + 1 into loose
+  const uint64_t* loose_pos;      // kRanges + 1: first loose entry at or after each range boundary
 };
 
 // The columns of a row-major n_cells x n_coef design that take more than one

@@ -347,61 +347,95 @@ __device__ void sweep_sums(const GeneData& d, Smem<NB, NV>& sm, const double* be
       // its next iteration's two cells' varying design values and offsets
       // into shared memory (cp.async, double-buffered) while it computes the
       // current ones, and reads only what it copied itself.
-      double* stg = sm.stage + warp * Smem<NB, NV>::kStageDoubles;
-      auto prefetch = [&](int r, int buf) {
-        double* dst = stg + buf * 2 * (NV + 1) * 32 + lane;
+      if (d.tabled) {
+        // zero-count tables: the dense part visits the segment's loose cells
+        // only, two per iteration like the positive entries below
+        const uint64_t q_begin = max(static_cast<uint64_t>(__ldg(d.subject_loose + s)), __ldg(d.loose_pos + v));
+        const uint64_t q_end = min(static_cast<uint64_t>(__ldg(d.subject_loose + s + 1)), __ldg(d.loose_pos + v + 1));
+        for (uint64_t q = q_begin + lane; q < q_end; q += 64) {
+          const bool has_b = q + 32 < q_end;
+          const int ca = static_cast<int>(__ldg(d.loose + q)), cb = static_cast<int>(__ldg(d.loose + (has_b ? q + 32 : q)));
+          double xa[NX], xb[NX];
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
-          const int c = r + 32 * k;
-          if (c < s_end) {
-            const double* row = d.design + static_cast<size_t>(c) * NB;
-#pragma unroll
-            for (int j = 0; j < NV; ++j) cp_async8(dst + (k * (NV + 1) + j) * 32, row + vc[j]);
-            cp_async8(dst + (k * (NV + 1) + NV) * 32, d.log_offset + c);
+          for (int j = 0; j < NV; ++j) {
+            xa[j] = __ldg(d.design + static_cast<size_t>(ca) * NB + vc[j]);
+            xb[j] = __ldg(d.design + static_cast<size_t>(cb) * NB + vc[j]);
+          }
+          const double ea = nb_exp_tab(linear_eta<NV>(xa, beta, __ldg(d.log_offset + ca) + csl), tab);
+          const double eb = nb_exp_tab(linear_eta<NV>(xb, beta, __ldg(d.log_offset + cb) + csl), tab);
+          const double ta = ea + gamma, tb = eb + gamma;
+          if (MODE == 0) {
+            const double la = nb_log_tab(ta, tab), lb = nb_log_tab(tb, tab);
+            const double inva = 1.0 / ta, invb = 1.0 / tb;
+            const double ua = ea * inva, ub = eb * invb;
+            acc[kSumLog] += la;
+            fold<NV>(acc, xa, -gamma * ua, (gamma * ua) * inva);
+            if (has_b) {
+              acc[kSumLog] += lb;
+              fold<NV>(acc, xb, -gamma * ub, (gamma * ub) * invb);
+            }
+          } else {
+            laplace_terms(acc, ea, ta, gamma, gamma);
+            if (has_b) laplace_terms(acc, eb, tb, gamma, gamma);
           }
         }
-        cp_async_commit();
-      };
-      int buf = 0;
-      prefetch(c0 + lane, 0);
-      for (int r = c0 + lane; r < s_end; r += 64) {
-        prefetch(r + 64, buf ^ 1);
-        cp_async_wait<1>();
-        const bool has_b = r + 32 < s_end;
-        const double* src = stg + buf * 2 * (NV + 1) * 32 + lane;
-        double xa[NX], xb[NX];
+      } else {
+        double* stg = sm.stage + warp * Smem<NB, NV>::kStageDoubles;
+        auto prefetch = [&](int r, int buf) {
+          double* dst = stg + buf * 2 * (NV + 1) * 32 + lane;
 #pragma unroll
-        for (int j = 0; j < NV; ++j) xa[j] = src[j * 32];
-        const double offa = src[NV * 32];
-        double offb = offa;
-        if (has_b) {
+          for (int k = 0; k < 2; ++k) {
+            const int c = r + 32 * k;
+            if (c < s_end) {
+              const double* row = d.design + static_cast<size_t>(c) * NB;
 #pragma unroll
-          for (int j = 0; j < NV; ++j) xb[j] = src[((NV + 1) + j) * 32];
-          offb = src[(2 * NV + 1) * 32];
-        } else {
+              for (int j = 0; j < NV; ++j) cp_async8(dst + (k * (NV + 1) + j) * 32, row + vc[j]);
+              cp_async8(dst + (k * (NV + 1) + NV) * 32, d.log_offset + c);
+            }
+          }
+          cp_async_commit();
+        };
+        int buf = 0;
+        prefetch(c0 + lane, 0);
+        for (int r = c0 + lane; r < s_end; r += 64) {
+          prefetch(r + 64, buf ^ 1);
+          cp_async_wait<1>();
+          const bool has_b = r + 32 < s_end;
+          const double* src = stg + buf * 2 * (NV + 1) * 32 + lane;
+          double xa[NX], xb[NX];
 #pragma unroll
-          for (int j = 0; j < NV; ++j) xb[j] = xa[j];
-        }
-        buf ^= 1;
-        const double ea = nb_exp_tab(linear_eta<NV>(xa, beta, offa + csl), tab);
-        const double eb = nb_exp_tab(linear_eta<NV>(xb, beta, offb + csl), tab);
-        const double ta = ea + gamma, tb = eb + gamma;
-        if (MODE == 0) {
-          const double la = nb_log_tab(ta, tab), lb = nb_log_tab(tb, tab);
-          const double inva = 1.0 / ta, invb = 1.0 / tb;
-          const double ua = ea * inva, ub = eb * invb;
-          acc[kSumLog] += la;
-          fold<NV>(acc, xa, -gamma * ua, (gamma * ua) * inva);
+          for (int j = 0; j < NV; ++j) xa[j] = src[j * 32];
+          const double offa = src[NV * 32];
+          double offb = offa;
           if (has_b) {
-            acc[kSumLog] += lb;
-            fold<NV>(acc, xb, -gamma * ub, (gamma * ub) * invb);
+#pragma unroll
+            for (int j = 0; j < NV; ++j) xb[j] = src[((NV + 1) + j) * 32];
+            offb = src[(2 * NV + 1) * 32];
+          } else {
+#pragma unroll
+            for (int j = 0; j < NV; ++j) xb[j] = xa[j];
           }
-        } else {
-          laplace_terms(acc, ea, ta, gamma, gamma);
-          if (has_b) laplace_terms(acc, eb, tb, gamma, gamma);
+          buf ^= 1;
+          const double ea = nb_exp_tab(linear_eta<NV>(xa, beta, offa + csl), tab);
+          const double eb = nb_exp_tab(linear_eta<NV>(xb, beta, offb + csl), tab);
+          const double ta = ea + gamma, tb = eb + gamma;
+          if (MODE == 0) {
+            const double la = nb_log_tab(ta, tab), lb = nb_log_tab(tb, tab);
+            const double inva = 1.0 / ta, invb = 1.0 / tb;
+            const double ua = ea * inva, ub = eb * invb;
+            acc[kSumLog] += la;
+            fold<NV>(acc, xa, -gamma * ua, (gamma * ua) * inva);
+            if (has_b) {
+              acc[kSumLog] += lb;
+              fold<NV>(acc, xb, -gamma * ub, (gamma * ub) * invb);
+            }
+          } else {
+            laplace_terms(acc, ea, ta, gamma, gamma);
+            if (has_b) laplace_terms(acc, eb, tb, gamma, gamma);
+          }
         }
+        cp_async_wait<0>();
       }
-      cp_async_wait<0>();
       // sparse: the segment's positive entries, into the same partials
       for (uint64_t p = pa + lane; p < p_end; p += 64) {
         const bool has_b = p + 32 < p_end;
@@ -455,6 +489,35 @@ __device__ void sweep_sums(const GeneData& d, Smem<NB, NV>& sm, const double* be
     sm.rtot[s * NP + x] = total;
   }
   __syncthreads();
+  if (d.tabled) {
+    // each tabled group's cells at a count of zero, per subject in group
+    // order (pml.rs:1515-1526, 1875-1885): with s = ln tau, sum ln t =
+    // n ln gamma + L, sum d = -gamma A, sum p = B; the Laplace pass adds B..E
+    const double ln_gamma = nb_log(gamma);
+    for (int s = threadIdx.x; s < K; s += blockDim.x) {
+      double* R = sm.rtot + s * NP;
+      const uint32_t g_end = __ldg(d.zsubject + s + 1);
+      for (uint32_t g = __ldg(d.zsubject + s); g < g_end; ++g) {
+        const zero::Group G = d.zgroups[g];
+        double xg[NX];
+#pragma unroll
+        for (int j = 0; j < NV; ++j) xg[j] = __ldg(d.design + static_cast<size_t>(G.row) * NB + vc[j]);
+        const double log_tau = linear_eta<NV>(xg, beta, sm.csl[s] - ln_gamma);
+        if (MODE == 0) {
+          double f[3];
+          zero::eval(G, d.zindex, d.zpanels, log_tau, 0, 3, f);
+          R[kSumLog] += G.n * ln_gamma + f[0];
+          fold<NV>(R, xg, -gamma * f[1], f[2]);
+        } else {
+          double f[4];
+          zero::eval(G, d.zindex, d.zpanels, log_tau, 2, 4, f);
+#pragma unroll
+          for (int j = 0; j < 4; ++j) R[j] += f[j];
+        }
+      }
+    }
+    __syncthreads();
+  }
 }
 
 // Slot x of subject s over every column (Dims<NB> layout) from its reduced

@@ -29,6 +29,7 @@
 #include "search.hpp"
 #include "stage_one.hpp"
 #include "warm_start.hpp"
+#include "zero_tables.hpp"
 
 namespace nebula {
 namespace {
@@ -171,6 +172,30 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
   h2d_bytes_ = (sh.design.size() + sh.log_offset.size() + nnz + totals.size()) * sizeof(double) +
                (fid.size() + nnz + wcells.size() + rcells.size()) * sizeof(uint32_t) +
                (gene_ptr.size() + runs.size() + rpos.size()) * sizeof(uint64_t);
+  // zero-count tables (the reference's ZeroCells, nebula.rs:641): built once
+  // for the call when enough cells share their subject's design rows
+  {
+    zero::Tables zt;
+    if (zero::build_tables(sh.design.data(), sh.log_offset.data(), sh.fid.data(), K, sh.n_coef, &zt)) {
+      std::vector<uint64_t> lpos(R + 1);
+      for (int v = 0; v <= R; ++v)
+        lpos[v] = static_cast<uint64_t>(std::lower_bound(zt.loose.begin(), zt.loose.end(), rcells[v]) -
+                                        zt.loose.begin());
+      data_.tabled = 1;
+      data_.zgroups = device_copy(zt.groups.data(), zt.groups.size(), stream_, &pooled_);
+      data_.zsubject = device_copy(zt.subject_groups.data(), zt.subject_groups.size(), stream_, &pooled_);
+      data_.zindex = device_copy(zt.index.data(), zt.index.size(), stream_, &pooled_);
+      data_.zpanels = device_copy(zt.panels.data(), zt.panels.size(), stream_, &pooled_);
+      data_.loose = device_copy(zt.loose.data(), zt.loose.size(), stream_, &pooled_);
+      data_.subject_loose = device_copy(zt.subject_loose.data(), zt.subject_loose.size(), stream_, &pooled_);
+      data_.loose_pos = device_copy(lpos.data(), lpos.size(), stream_, &pooled_);
+      tabled_groups_ = zt.groups.size();
+      h2d_bytes_ += zt.groups.size() * sizeof(zero::Group) + zt.panels.size() * sizeof(double) +
+                    (zt.subject_groups.size() + zt.index.size() + zt.loose.size() + zt.subject_loose.size()) *
+                        sizeof(uint32_t) +
+                    lpos.size() * sizeof(uint64_t);
+    }
+  }
   data_.n_cells = static_cast<int32_t>(sh.n_cells);
   data_.n_subjects = K;
   data_.n_coef = sh.n_coef;

@@ -93,6 +93,8 @@ class DeviceFitter {
   uint64_t sweeps() const { return sweeps_; }
   uint64_t cell_visits() const { return cell_visits_; }
   uint64_t slot_cycles() const { return slot_cycles_; }
+  // Zero-count groups the sweeps look up (0: every cell is swept).
+  size_t tabled_groups() const { return tabled_groups_; }
   // Device time from the first fit's start to the last fit's end since the
   // last reset_counters, in ms (0 before any fit).
   double busy_span_ms() const { return last_ns_ > first_ns_ ? (last_ns_ - first_ns_) / 1e6 : 0.0; }
@@ -135,7 +137,8 @@ class DeviceFitter {
   size_t n_cells_ = 0;
   device::GeneData data_{};
   device::FitControl ctl_{};
-  std::vector<void*> pooled_;  // stream-ordered allocations from the device's memory pool
+  std::vector<void*> pooled_;
+  size_t tabled_groups_ = 0;  // stream-ordered allocations from the device's memory pool
   int grid_ = 0;
   int max_clusters_[device::kMaxCluster + 1] = {};  // resident clusters per cluster size
   // stage-one buffers

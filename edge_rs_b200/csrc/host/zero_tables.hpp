@@ -178,6 +178,23 @@ inline Built build_group(int64_t row, std::vector<double> log_o) {
 inline bool build_tables(const double* design, const double* log_offset, const uint64_t* fid, int n_subjects,
                          int n_coef, Tables* out, int threads = 0) {
   const size_t n_cells = static_cast<size_t>(fid[n_subjects]);
+  // A cell can sit in a tabled group only if its value in every column occurs
+  // at least kMinGroupCells times; counting the values of each column bounds
+  // the tabled cells from above, and a continuous column ends the build here
+  // without grouping the rows.
+  {
+    std::vector<uint64_t> bits(n_cells);
+    for (int j = 0; j < n_coef; ++j) {
+      for (size_t r = 0; r < n_cells; ++r) std::memcpy(&bits[r], &design[r * n_coef + j], sizeof(double));
+      std::sort(bits.begin(), bits.end());
+      size_t coverable = 0;
+      for (size_t a = 0, b; a < n_cells; a = b) {
+        for (b = a + 1; b < n_cells && bits[b] == bits[a];) ++b;
+        if (b - a >= kMinGroupCells) coverable += b - a;
+      }
+      if (static_cast<double>(coverable) < kMinTabledShare * static_cast<double>(n_cells)) return false;
+    }
+  }
   std::vector<std::vector<uint32_t>> members;  // tabled groups, subject by subject
   Tables t;
   t.subject_groups.assign(static_cast<size_t>(n_subjects) + 1, 0);
