@@ -85,6 +85,10 @@ def parse():
     ap.add_argument("--fit-batch", type=int, default=0,
                     help="instead of the bench: time launches of the fit kernel in batch mode, this many inner fits "
                          "of the workload's first gene per launch (the profiling workload)")
+    ap.add_argument("--zero-tables", action="store_true",
+                    help="instead of the bench: the plain method on a categorical design (intercept and a "
+                         "subject-level binary) of the default size, with the zero-count tables and with every "
+                         "cell swept")
     return ap.parse_args()
 
 
@@ -353,6 +357,48 @@ def ours_arm(args, world, rank, local, dist):
     print(json.dumps(line), flush=True)
 
 
+def zero_tables(args):
+    """The plain method (stages two and three on resident inputs, L2 flushed
+    before each step) on a categorical design at the default workload's size,
+    once with the zero-count tables and once with every cell swept. Prints one
+    JSON line."""
+    import torch
+    from edge_rs_b200.api import Session
+    base = workloads.CONFIGS[args.config]
+    work = workloads.make("c0", seed=1000, n_genes=args.genes or base["n_genes"], n_cells=base["n_cells"],
+                          n_subjects=base["n_subjects"])
+    params = NebulaParams(method="HL")
+    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    out, fits = {}, {}
+    for name, dense in (("tables", False), ("dense", True)):
+        s = Session(work.csr, work.subject, work.design, work.n_coef, work.offset, params, dense_sweep=dense)
+        for _ in range(args.warmup):
+            s.fit()
+        ms = []
+        for _ in range(args.steps):
+            l2_flush(flush)
+            torch.cuda.synchronize()
+            f = s.fit()
+            ms.append(f.stats["ms_step_device"])
+        s.close()
+        fits[name] = f
+        out[name] = {"genes_per_s": len(f.gene_index) * args.steps / (float(np.sum(ms)) / 1000.0),
+                     "ms_per_step": float(np.mean(ms)), "zero_groups": f.stats["zero_groups"],
+                     "cell_visits_per_step": f.stats["cell_visits"], "sweeps_per_step": f.stats["sweeps"]}
+    a, b = fits["tables"], fits["dense"]
+    print(json.dumps({"mode": "zero-tables", "config": {"workload": f"c0 design: {work.n_genes} genes x "
+                                                        f"{work.n_cells} cells, {len(work.truth['sizes'])} subjects, "
+                                                        f"{work.n_coef} columns, forced HL, plain method"},
+                      **out, "speedup": out["tables"]["genes_per_s"] / out["dense"]["genes_per_s"],
+                      "max_rel_diff": {"subject_overdispersion": max_rel(a.subject_overdispersion,
+                                                                         b.subject_overdispersion),
+                                       "cell_overdispersion": max_rel(a.cell_overdispersion, b.cell_overdispersion),
+                                       "coefficients": max_rel(a.coefficients, b.coefficients)},
+                      "median_rel_diff": {"subject_overdispersion": med_rel(a.subject_overdispersion,
+                                                                            b.subject_overdispersion),
+                                          "coefficients": med_rel(a.coefficients, b.coefficients)}}), flush=True)
+
+
 def fit_batch(args):
     """R inner fits of one c1-shaped gene per launch through nb_opt_pml_cuda:
     the per-fit code of the persistent launch (fit_one) in the batch kernel,
@@ -389,6 +435,9 @@ def main():
     args = parse()
     if args.fit_batch > 0:
         fit_batch(args)
+        return
+    if args.zero_tables:
+        zero_tables(args)
         return
     if args.impl == "reference":  # rank 0 alone times the CPU path; other ranks exit
         reference_arm(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), None)

@@ -122,7 +122,7 @@ def call_nebula(fn, counts, subject_id, design, n_coef, offset, params, extra_ar
 
 
 def _options(device, warm_start, host_threads, audit_percent, cluster, n_genes, warm_points=None,
-             mlp_weights=None, warm_radius=0.0):
+             mlp_weights=None, warm_radius=0.0, dense_sweep=False):
     """An NbOptions plus the arrays it points into (kept alive by the caller)."""
     evaluations = np.zeros(max(int(n_genes), 1), np.int32)
     wp = None if warm_points is None else np.ascontiguousarray(warm_points, np.float64).reshape(-1, 2)
@@ -134,13 +134,13 @@ def _options(device, warm_start, host_threads, audit_percent, cluster, n_genes, 
     mode = int(warm_start)
     opts = _ffi.NbOptions(int(device), mode, int(host_threads), int(audit_percent),
                           _ffi.ptr(mw, ctypes.c_float), int(cluster), _ffi.ptr(wp, ctypes.c_double),
-                          _ffi.ptr(evaluations, ctypes.c_int32), float(warm_radius))
+                          _ffi.ptr(evaluations, ctypes.c_int32), float(warm_radius), int(bool(dense_sweep)))
     return opts, [evaluations, wp, mw]
 
 
 def nebula_sparse_cuda(counts, subject_id, design, n_coef, offset=None, params: Optional[NebulaParams] = None,
                        warm_start=False, device=-1, host_threads=0, audit_percent=5, cluster=0, warm_points=None,
-                       mlp_weights=None, warm_radius=0.0):
+                       mlp_weights=None, warm_radius=0.0, dense_sweep=False):
     """Fits NEBULA per gene with every inner penalised fit on the GPU.
 
     warm_start: False/0 plain (the reference's method). Otherwise every
@@ -152,11 +152,14 @@ def nebula_sparse_cuda(counts, subject_id, design, n_coef, offset=None, params: 
     result when its objective is better. warm_radius: the warm search's
     initial BOBYQA trust radius as a fraction of NLopt's (0: the library's
     default; 1: NLopt's); the final radius is NLopt's either way.
+    dense_sweep: visit every cell in every sweep even where the zero-count
+    tables of a categorical design apply (by default they are used, as the
+    reference's CPU path uses them).
     """
     lib = _ffi.product_library()
     n_genes = int(_as_csr(counts).struct.n_genes)
     opts, keep = _options(device, warm_start, host_threads, audit_percent, cluster, n_genes, warm_points,
-                          mlp_weights, warm_radius)
+                          mlp_weights, warm_radius, dense_sweep)
     fit = call_nebula(lib.nebula_sparse_cuda_ex, counts, subject_id, design, n_coef, offset, params,
                       options=opts, want_stats=True)
     fit.evaluations = keep[0][: len(fit.gene_index)].copy()
@@ -203,7 +206,7 @@ class Session:
 
     def __init__(self, counts, subject_id, design, n_coef, offset=None, params: Optional[NebulaParams] = None,
                  warm_start=False, device=-1, host_threads=0, audit_percent=5, cluster=0, warm_points=None,
-                 mlp_weights=None, warm_radius=0.0):
+                 mlp_weights=None, warm_radius=0.0, dense_sweep=False):
         self._lib = _ffi.product_library()
         self._keep = []
         csr = _as_csr(counts)
@@ -214,7 +217,7 @@ class Session:
         self.n_coef = int(n_coef)
         p = (params or NebulaParams()).to_c()
         opts, arrays = _options(device, warm_start, host_threads, audit_percent, cluster, self.n_genes,
-                                warm_points, mlp_weights, warm_radius)
+                                warm_points, mlp_weights, warm_radius, dense_sweep)
         self._evaluations = arrays[0]
         self._keep = [csr, subject, design, off, p, opts, arrays]
         handle = ctypes.c_void_p()

@@ -106,7 +106,8 @@ T* device_copy(const T* host, size_t n, cudaStream_t stream, std::vector<void*>*
 // ---------------------------------------------------------------------------
 // Resident device copy of one call's inputs, and the per-round launch.
 
-DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& genes, int device, int lanes)
+DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& genes, int device, int lanes,
+                           bool tables)
     : lanes_(static_cast<size_t>(std::max(1, std::min(lanes, kMaxLanes)))) {
   const Shared& sh = prep.shared;
   if (device >= 0) cuda_check(cudaSetDevice(device), "cudaSetDevice");
@@ -140,6 +141,7 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
   gene_nnz_.resize(G);
   for (size_t g = 0; g < G; ++g) gene_nnz_[g] = genes[g].cells.size();
   n_cells_ = sh.n_cells;
+  dense_cells_ = sh.n_cells;
   std::vector<uint32_t> fid(sh.fid.begin(), sh.fid.end());
   std::vector<uint32_t> wcells(device::kWarps + 1);
   for (int w = 0; w <= device::kWarps; ++w)
@@ -176,7 +178,7 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
   // for the call when enough cells share their subject's design rows
   {
     zero::Tables zt;
-    if (zero::build_tables(sh.design.data(), sh.log_offset.data(), sh.fid.data(), K, sh.n_coef, &zt)) {
+    if (tables && zero::build_tables(sh.design.data(), sh.log_offset.data(), sh.fid.data(), K, sh.n_coef, &zt)) {
       std::vector<uint64_t> lpos(R + 1);
       for (int v = 0; v <= R; ++v)
         lpos[v] = static_cast<uint64_t>(std::lower_bound(zt.loose.begin(), zt.loose.end(), rcells[v]) -
@@ -190,12 +192,16 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
       data_.subject_loose = device_copy(zt.subject_loose.data(), zt.subject_loose.size(), stream_, &pooled_);
       data_.loose_pos = device_copy(lpos.data(), lpos.size(), stream_, &pooled_);
       tabled_groups_ = zt.groups.size();
+      dense_cells_ = zt.loose.size();
       h2d_bytes_ += zt.groups.size() * sizeof(zero::Group) + zt.panels.size() * sizeof(double) +
                     (zt.subject_groups.size() + zt.index.size() + zt.loose.size() + zt.subject_loose.size()) *
                         sizeof(uint32_t) +
                     lpos.size() * sizeof(uint64_t);
     }
   }
+  // cells a sweep of an average gene visits: the dense part (every cell, or
+  // the loose ones under zero-count tables) and the positive entries
+  sweep_cells_ = dense_cells_ + (G ? nnz / G : 0);
   data_.n_cells = static_cast<int32_t>(sh.n_cells);
   data_.n_subjects = K;
   data_.n_coef = sh.n_coef;
@@ -403,7 +409,7 @@ const device::FitResult* DeviceFitter::collect(int lane_index) {
   for (size_t i = 0; i < n; ++i) {
     const uint64_t sw = static_cast<uint64_t>(lane.h_res[i].sweeps);
     sweeps_ += sw;
-    cell_visits_ += sw * (n_cells_ + gene_nnz_[lane.h_req[i].gene]);
+    cell_visits_ += sw * (dense_cells_ + gene_nnz_[lane.h_req[i].gene]);
     slot_cycles_ += static_cast<uint64_t>(lane.h_res[i].cycles);
   }
   lane.pending = 0;
@@ -417,12 +423,14 @@ int DeviceFitter::cluster_for(size_t requests) const {
   // Spread each fit over more CTAs while (a) the fits in flight times the
   // cluster stay within about four times the resident CTA slots, so the
   // searches that finish last still find the SMs busy, and (b) each CTA keeps
-  // at least ~40,000 cells per sweep, so a sweep's fixed costs (the cluster
-  // barrier, the combine, the Newton step every CTA repeats) stay small.
+  // at least ~40,000 cell visits per sweep (the dense cells, only the loose
+  // ones under zero-count tables, plus a gene's positive entries), so a
+  // sweep's fixed costs (the cluster barrier, the combine, the Newton step
+  // every CTA repeats) stay small.
   int cluster = 1;
   while (cluster < device::kMaxCluster && queue_clusters_[cluster * 2] > 0 &&
          requests * static_cast<size_t>(cluster) * 2 <= 4 * static_cast<size_t>(grid_) &&
-         n_cells_ >= static_cast<size_t>(cluster) * 2 * 40000)
+         sweep_cells_ >= static_cast<size_t>(cluster) * 2 * 40000)
     cluster *= 2;
   return cluster;
 }
@@ -467,7 +475,7 @@ void DeviceFitter::queue_account(long long ticket, int gene, Tally* tally) const
   if (r.status != 0) return;
   const uint64_t sw = static_cast<uint64_t>(r.sweeps);
   tally->sweeps += sw;
-  tally->cell_visits += sw * (n_cells_ + gene_nnz_[static_cast<size_t>(gene)]);
+  tally->cell_visits += sw * (dense_cells_ + gene_nnz_[static_cast<size_t>(gene)]);
   tally->slot_cycles += static_cast<uint64_t>(r.cycles);
   tally->first_ns = std::min<int64_t>(tally->first_ns, r.start_ns);
   tally->last_ns = std::max<int64_t>(tally->last_ns, r.end_ns);
@@ -604,7 +612,7 @@ std::unique_ptr<Session> create_session(const nb_csr* counts, const uint64_t* su
                [&](size_t g) { ss->genes[g] = positive_indices(ss->prep.counts, ss->prep.kept[g]); });
   ss->ms_prepare = ms_since(t0);
   auto t2 = Clock::now();
-  ss->fitter = std::make_unique<DeviceFitter>(ss->prep, ss->genes, ss->opt.device);
+  ss->fitter = std::make_unique<DeviceFitter>(ss->prep, ss->genes, ss->opt.device, 1, ss->opt.dense_sweep == 0);
   ss->ms_upload = ms_since(t2);
   // stage one (nebula.rs:812-901): every gene's projected Newton at its own
   // pace through one persistent launch of marginal-likelihood cell passes;
@@ -1228,6 +1236,7 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
     stats->ms_prepare = ss.ms_prepare;
     stats->ms_upload = ss.ms_upload;
     stats->ms_busy_span = fitter.busy_span_ms();
+    stats->zero_groups = fitter.tabled_groups();
     stats->ms_stage_one = ss.ms_stage_one;
     stats->ms_stage_two = ms_stage_two;
     stats->ms_stage_three = ms_stage_three;

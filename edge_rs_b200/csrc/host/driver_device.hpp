@@ -27,7 +27,9 @@ class DeviceFitter {
   static constexpr int kDefaultLanes = 8;
   static constexpr int kMaxLanes = 64;
 
-  DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& genes, int device, int lanes = 1);
+  // tables: use the zero-count tables where they apply (zero_tables.hpp)
+  DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& genes, int device, int lanes = 1,
+               bool tables = true);
   ~DeviceFitter();
   DeviceFitter(const DeviceFitter&) = delete;
   DeviceFitter& operator=(const DeviceFitter&) = delete;
@@ -135,6 +137,8 @@ class DeviceFitter {
   std::vector<Lane> lanes_;
   std::vector<uint64_t> gene_nnz_;
   size_t n_cells_ = 0;
+  size_t dense_cells_ = 0;  // cells a sweep's dense part visits
+  size_t sweep_cells_ = 0;  // dense cells plus an average gene's positive entries
   device::GeneData data_{};
   device::FitControl ctl_{};
   std::vector<void*> pooled_;

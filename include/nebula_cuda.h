@@ -131,6 +131,10 @@ typedef struct nb_options {
   double warm_radius;    /* warm start only: the search's initial BOBYQA trust
                             radius as a fraction of NLopt's (the final radius
                             stays NLopt's); 0 = the library default, 1 = NLopt's */
+  int32_t dense_sweep;   /* 1: every sweep visits every cell even where the
+                            zero-count tables (src/sc/zeros.rs) apply; 0 = use
+                            them for categorical designs, as the reference's
+                            CPU path does */
 } nb_options;
 
 /* Counters of one call (timings in milliseconds of host wall clock, device
@@ -154,6 +158,8 @@ typedef struct nb_stats {
   double ms_upload;         /* host wall time of the device upload */
   double ms_busy_span;      /* device time from the first fit's start to the
                                last fit's end in stages two and three */
+  uint64_t zero_groups;     /* zero-count groups looked up instead of swept
+                               (0: every sweep visits every cell) */
 } nb_stats;
 
 void nb_params_default(nb_params* params);

@@ -57,3 +57,30 @@ def test_device_tabled_fit_differs_from_dense_only_in_rounding():
         assert dev[q]["log_likelihood"] == pytest.approx(dense["log_likelihood"], rel=1e-13)
         assert dev[q]["log_det"] == pytest.approx(dense["log_det"], rel=1e-12)
         np.testing.assert_allclose(dev[q]["beta"], dense["beta"], rtol=1e-6)
+
+
+def test_categorical_fit_uses_the_tables_and_matches_the_dense_sweep():
+    """nebula_sparse_cuda on a categorical design (intercept and a
+    subject-level binary): one tabled group per subject, and the fits agree
+    with the same call sweeping every cell within the search's resolution
+    (the objective differs in its last digits, so BOBYQA may stop at a
+    different point within its final radius)."""
+    from edge_rs_b200 import NebulaParams, nebula_sparse_cuda, workloads
+    w = workloads.make("c0", seed=3, n_genes=24, n_cells=5000, n_subjects=10)
+    params = NebulaParams(method="HL")
+    tabled = nebula_sparse_cuda(w.csr, w.subject, w.design, w.n_coef, w.offset, params)
+    dense = nebula_sparse_cuda(w.csr, w.subject, w.design, w.n_coef, w.offset, params, dense_sweep=True)
+    assert tabled.stats["zero_groups"] == 10 and dense.stats["zero_groups"] == 0
+    assert tabled.stats["cell_visits"] < 0.5 * dense.stats["cell_visits"]
+    assert np.array_equal(tabled.gene_index, dense.gene_index)
+    rel = lambda a, b: np.abs(a - b) / np.maximum(np.abs(b), 1e-12)
+    assert np.median(rel(tabled.coefficients, dense.coefficients)) < 1e-6
+    assert np.median(rel(tabled.subject_overdispersion, dense.subject_overdispersion)) < 1e-4
+    assert np.median(rel(tabled.cell_overdispersion, dense.cell_overdispersion)) < 1e-4
+
+
+def test_continuous_design_builds_no_tables():
+    from edge_rs_b200 import NebulaParams, nebula_sparse_cuda, workloads
+    w = workloads.make("c1", seed=3, n_genes=8, n_cells=4000, n_subjects=8)
+    fit = nebula_sparse_cuda(w.csr, w.subject, w.design, w.n_coef, w.offset, NebulaParams(method="HL"))
+    assert fit.stats["zero_groups"] == 0
