@@ -6,14 +6,37 @@
 // LN->HL override (nebula.rs:612-617) and the expression filter
 // (nebula.rs:621-639).
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <sstream>
+#include <thread>
 #include <unordered_map>
 #include <unordered_set>
+#include <vector>
 
 #include "common.hpp"
 
 namespace nebula {
+namespace {
+
+// Runs f(begin, end) over [0, n) in contiguous blocks on the host's threads
+// when `parallel` (else as one block); true when every block returned true.
+template <typename F>
+bool all_blocks(size_t n, bool parallel, F&& f) {
+  const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t blocks = parallel ? std::min<size_t>({hw, 64, std::max<size_t>(n, 1)}) : 1;
+  if (blocks == 1) return f(size_t{0}, n);
+  std::atomic<bool> ok{true};
+  std::vector<std::thread> pool;
+  for (size_t b = 0; b < blocks; ++b)
+    pool.emplace_back([&, b] {
+      if (!f(n * b / blocks, n * (b + 1) / blocks)) ok.store(false);
+    });
+  for (auto& t : pool) t.join();
+  return ok.load();
+}
+
+}  // namespace
 
 void fail(int32_t code, const std::string& message) { throw NbError{code, message}; }
 
@@ -67,8 +90,12 @@ void validate_csr(const nb_csr* c) {
     if (c->indptr[g + 1] < c->indptr[g]) fail(NB_ERR_MALFORMED_SPARSE, "indptr is not non-decreasing");
   if (c->indptr[c->n_genes] != c->nnz)
     fail(NB_ERR_MALFORMED_SPARSE, "indptr does not end at the number of stored values");
-  for (uint64_t i = 0; i < c->nnz; ++i)
-    if (c->indices[i] >= c->n_cells) fail(NB_ERR_MALFORMED_SPARSE, "cell index out of range");
+  const bool in_range = all_blocks(c->nnz, c->nnz >= (size_t{1} << 20), [&](size_t a, size_t b) {
+    for (size_t i = a; i < b; ++i)
+      if (c->indices[i] >= c->n_cells) return false;
+    return true;
+  });
+  if (!in_range) fail(NB_ERR_MALFORMED_SPARSE, "cell index out of range");
 }
 
 }  // namespace
@@ -82,11 +109,14 @@ Prepared prepare(const nb_csr* counts, const uint64_t* subject_id, const double*
   const size_t n_genes = counts->n_genes;
   if (n_cells < 2) fail(NB_ERR_INVALID_ARGUMENT, "NEBULA needs more than one cell in the count matrix.");
   if (n_coef == 0) fail(NB_ERR_MUST_BE_POSITIVE, "n_coef must be positive");
-  for (uint64_t i = 0; i < counts->nnz; ++i) {
-    double v = counts->data[i];
-    if (!(std::isfinite(v) && v >= 0.0))
-      fail(NB_ERR_INVALID_ARGUMENT, "The counts hold a value that is not a non-negative finite number.");
-  }
+  const bool finite = all_blocks(counts->nnz, counts->nnz >= (size_t{1} << 20), [&](size_t a, size_t b) {
+    for (size_t i = a; i < b; ++i) {
+      const double v = counts->data[i];
+      if (!(std::isfinite(v) && v >= 0.0)) return false;
+    }
+    return true;
+  });
+  if (!finite) fail(NB_ERR_INVALID_ARGUMENT, "The counts hold a value that is not a non-negative finite number.");
   if (!design) fail(NB_ERR_SHAPE_MISMATCH, "design is null");
   if (!subject_id) fail(NB_ERR_LENGTH_MISMATCH, "subject_id is null");
 
@@ -203,13 +233,17 @@ Prepared prepare(const nb_csr* counts, const uint64_t* subject_id, const double*
   for (int s = 0; s < k; ++s)
     for (size_t i = sh.fid[s]; i < sh.fid[s + 1]; ++i) subject_of[i] = s;
   out.totals.assign(n_genes * k, 0.0);
-  for (size_t g = 0; g < n_genes; ++g) {
-    double* row = &out.totals[g * k];
-    for (uint32_t e = counts->indptr[g]; e < counts->indptr[g + 1]; ++e) {
-      double v = counts->data[e];
-      if (v > 0.0) row[subject_of[counts->indices[e]]] += v;
+  // each gene's row on its own, in entry order; blocks of genes run in parallel
+  all_blocks(n_genes, counts->nnz >= (size_t{1} << 20), [&](size_t a, size_t b) {
+    for (size_t g = a; g < b; ++g) {
+      double* row = &out.totals[g * k];
+      for (uint32_t e = counts->indptr[g]; e < counts->indptr[g + 1]; ++e) {
+        double v = counts->data[e];
+        if (v > 0.0) row[subject_of[counts->indices[e]]] += v;
+      }
     }
-  }
+    return true;
+  });
 
   sh.cells_per_subject = static_cast<double>(n_cells) / static_cast<double>(k);
   sh.method = sh.cells_per_subject < 30.0 ? NB_METHOD_HL : params.method;
