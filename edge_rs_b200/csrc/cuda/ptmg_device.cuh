@@ -20,9 +20,11 @@ struct alignas(16) PtmgRequest {
 
 // Per request the kernel writes (2 + ptmg_width_of(n_coef)) * n_subjects
 // doubles: cumsumxtb (K), ylin (K), then K rows of the pass-two sums.
-size_t ptmg_smem_bytes(int n_subjects);
 int ptmg_width_of(int n_coef);
-size_t ptmg_scratch_doubles(int n_subjects, int n_coef);  // per CTA
+// Scratch doubles per CTA, and CTAs per SM, for n_coef columns of which
+// n_varying vary within subjects (GeneData.n_varying).
+size_t ptmg_scratch_doubles(int n_subjects, int n_coef, int n_varying);
+int ptmg_blocks_per_sm(int n_subjects, int n_coef, int n_varying);
 
 // Streaming mode for stage one: the request-ring protocol of FitQueue
 // (pml_device.cuh) with PtmgRequests and results of result_stride doubles

@@ -1,0 +1,484 @@
+// Stage one's cell passes on the device: per-subject sums of the Poisson-gamma
+// marginal likelihood (src/sc/ptmg.rs linear_predictor 661-708, the cell loop
+// of evaluate 926-966 and hessian_subject 1381-1428) for a stream of
+// (gene, [beta, sigma, phi]) requests. The host assembles value, gradient and
+// Hessian from them (stage_one.cpp ptmg_assemble). Instantiated per design
+// width NB and count NV of the columns that vary within subjects
+// (ptmg_nb<NB>.cu); ptmg_eval.cu dispatches.
+//
+// Pass one sums exp(eta) per subject over every cell and y eta over the
+// positive ones (two accumulators, so the dense and sparse halves stay apart).
+// Pass two, with ym = (cumsumy + alpha) / (cumsumxtb + lambda) per subject,
+// sums the nine scalars, the x-weighted vectors and the two triangles of
+// stage_one.hpp, split into the value at a count of zero (dense, every cell)
+// plus what each positive count adds (sparse); every per-cell term is affine
+// in the count.
+//
+// The cells' sums run over the NV varying columns only. eta starts from the
+// offset plus the subject's constant share (the subject-constant columns
+// times beta, once per subject and request), and pass two keeps, beside the
+// nine scalars, sum e and sum e q (dense and sparse q alike) and the vector
+// sum x e q over the varying columns: a constant column a's sums are then its
+// value times a scalar sum (sum x_a e = x_a sum e, sum x_a gg e = x_a acc[6],
+// ...), and the subject's full row of stage_one.hpp is expanded before it is
+// written (expand_two).
+//
+// The summation tree, the exp/log (nbmath.hpp) and the fused multiply-adds
+// (written explicitly; compiled with -fmad=false) are those of the CPU oracle
+// (oracle/ptmg_cpu.cpp), so the two agree bit for bit. One persistent launch
+// serves the whole stage: each CTA claims the next ticket of the device
+// request ring, waits (bounded) for the host to post it, and writes its
+// result to host-mapped memory; the warp slots and the subjects' reduced
+// sums live in a per-CTA global scratch region (L2-resident).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../host/nbmath.hpp"
+#include "ptmg_device.cuh"
+#include "ptmg_ops.cuh"
+
+namespace nebula {
+namespace device {
+namespace {
+
+// The full per-subject row of pass two (stage_one.hpp).
+template <int NB>
+struct PDims {
+  static constexpr int T = NB * (NB + 1) / 2;
+  static constexpr int W = 9 + 4 * NB + 2 * T;
+  static constexpr int kXf = 9, kD41 = kXf + NB, kT1 = kD41 + NB, kT2 = kT1 + NB, kBp = kT2 + NB, kBq = kBp + T;
+};
+
+// The reduced row over NV varying columns: the nine scalars, sum e, sum e q,
+// the vectors Xf, D41, T1, T2, Eq and the triangles Bp, Bq.
+template <int NV>
+struct RDims {
+  static constexpr int T = NV * (NV + 1) / 2;
+  static constexpr int kE = 9, kEq = 10;
+  static constexpr int kXf = 11, kD41 = kXf + NV, kT1 = kD41 + NV, kT2 = kT1 + NV, kQv = kT2 + NV;
+  static constexpr int kBp = kQv + NV, kBq = kBp + T;
+  static constexpr int W = kBq + T;
+};
+
+constexpr int ptmg_min_blocks(int nb, int nv) { return nb <= 4 && nv <= 1 ? 2 : 1; }
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  return v;
+}
+
+template <int N>
+__device__ __forceinline__ void reduce_to(const double* acc, double* slot, int lane) {
+#pragma unroll
+  for (int v = 0; v < N; ++v) {
+    double s = warp_sum(acc[v]);
+    if (lane == 0) slot[v] = s;
+  }
+}
+
+__device__ __forceinline__ int subject_of(const uint32_t* fid, int K, int c) {
+  int lo = 0, hi = K;
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (fid[mid] <= static_cast<uint32_t>(c)) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// The varying design values of cell r and eta over them from `start`.
+template <int NB, int NV>
+__device__ __forceinline__ void varying_row(const double* __restrict__ design, const int* vc, int r, double* x) {
+  const double* row = design + static_cast<size_t>(r) * NB;
+#pragma unroll
+  for (int j = 0; j < NV; ++j) x[j] = __ldg(row + vc[j]);
+}
+
+template <int NV>
+__device__ __forceinline__ double eta_from(const double* x, const double* beta, double start) {
+  double eta = start;
+#pragma unroll
+  for (int j = 0; j < NV; ++j) eta = nb_fma(x[j], beta[j], eta);
+  return eta;
+}
+
+// Pass two's dense (count zero) contribution of one cell.
+template <int NV>
+__device__ __forceinline__ void dense_two(double* acc, const double* x, double e, double ym, double gamma) {
+  using D = RDims<NV>;
+  const double we = ym * e;
+  const double w = we + gamma;
+  const double lw = nb_log(w);
+  const double iw = 1.0 / w;
+  const double gg = gamma * iw;
+  const double gt = gg * iw;
+  const double gte = gt * e;
+  acc[0] += we;
+  acc[1] += lw;
+  acc[2] = nb_fma(gamma, lw, acc[2]);
+  acc[3] += gg;
+  acc[4] += iw;
+  acc[5] += gt;
+  acc[6] = nb_fma(gg, e, acc[6]);
+  acc[7] += gte - e * iw;
+  acc[8] = nb_fma(gte, e, acc[8]);
+  const double f1 = gt - iw;
+  const double q = ym * (ym * gte - gg);
+  acc[D::kE] += e;
+  acc[D::kEq] = nb_fma(e, q, acc[D::kEq]);
+  int t = 0;
+#pragma unroll
+  for (int a = 0; a < NV; ++a) {
+    const double xe = x[a] * e;
+    acc[D::kXf + a] += xe;
+    acc[D::kD41 + a] = nb_fma(gg, xe, acc[D::kD41 + a]);
+    acc[D::kT1 + a] = nb_fma(xe, f1, acc[D::kT1 + a]);
+    acc[D::kT2 + a] = nb_fma(xe, gte, acc[D::kT2 + a]);
+    acc[D::kQv + a] = nb_fma(xe, q, acc[D::kQv + a]);
+#pragma unroll
+    for (int b = a; b < NV; ++b) {
+      const double c = xe * x[b];
+      acc[D::kBp + t] += c;
+      acc[D::kBq + t] = nb_fma(c, q, acc[D::kBq + t]);
+      ++t;
+    }
+  }
+}
+
+// What a positive count y adds to a cell's pass-two contribution.
+template <int NV>
+__device__ __forceinline__ void sparse_two(double* acc, const double* x, double e, double y, double ym,
+                                           double gamma) {
+  using D = RDims<NV>;
+  const double w = ym * e + gamma;
+  const double lw = nb_log(w);
+  const double iw = 1.0 / w;
+  const double gg = y * iw;
+  const double gt = gg * iw;
+  const double gte = gt * e;
+  acc[2] = nb_fma(y, lw, acc[2]);
+  acc[3] += gg;
+  acc[5] += gt;
+  acc[6] = nb_fma(gg, e, acc[6]);
+  acc[7] += gte;
+  acc[8] = nb_fma(gte, e, acc[8]);
+  const double q = ym * (ym * gte - gg);
+  acc[D::kEq] = nb_fma(e, q, acc[D::kEq]);
+  int t = 0;
+#pragma unroll
+  for (int a = 0; a < NV; ++a) {
+    const double xe = x[a] * e;
+    acc[D::kD41 + a] = nb_fma(gg, xe, acc[D::kD41 + a]);
+    acc[D::kT1 + a] = nb_fma(xe, gt, acc[D::kT1 + a]);
+    acc[D::kT2 + a] = nb_fma(xe, gte, acc[D::kT2 + a]);
+    acc[D::kQv + a] = nb_fma(xe, q, acc[D::kQv + a]);
+#pragma unroll
+    for (int b = a; b < NV; ++b) {
+      const double cc = xe * x[b];
+      acc[D::kBq + t] = nb_fma(cc, q, acc[D::kBq + t]);
+      ++t;
+    }
+  }
+}
+
+// Shared-memory and scratch views of one stage-one CTA.
+struct PtmgCta {
+  double* ym;        // K
+  double* p1;        // K x 2: cumsumxtb, ylin
+  double* cs;        // K: the constant columns' share of eta for this request
+  uint32_t* fid;     // K + 1
+  uint32_t* wcells;  // kWarps + 1
+  int32_t* vpos;     // kMaxCoef: each column's index among the varying ones, or -1
+  double* slots;     // this CTA's scratch: warp and subject pieces
+  double* reduced;   // this CTA's scratch: K reduced pass-two rows
+};
+
+// One pass through the tree: dense pieces into slots[(s + warp) * stride],
+// sparse pieces into slots[(K + kWarps + s) * stride], then per subject
+// out[s * out_stride + v] = 0 + dense pieces (warp order) + sparse piece.
+// Lanes take two cells (r, r + 32) or entries per iteration; each lane's
+// partials still take them in its sequential order.
+template <int NB, int NV, int PASS, int N>
+__device__ void tree_pass(const GeneData& d, const PtmgCta& c, int gene, const double* beta, double gamma,
+                          const int* vc, int stride, double* out, int out_stride) {
+  const int K = d.n_subjects;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int NX = NV > 0 ? NV : 1;
+  const int c_begin = static_cast<int>(c.wcells[warp]), c_end = static_cast<int>(c.wcells[warp + 1]);
+  if (c_begin < c_end) {
+    int s = subject_of(c.fid, K, c_begin);
+    for (int c0 = c_begin; c0 < c_end; ++s) {
+      const int s_end = min(c_end, static_cast<int>(c.fid[s + 1]));
+      double acc[N];
+#pragma unroll
+      for (int v = 0; v < N; ++v) acc[v] = 0.0;
+      const double yms = PASS == 2 ? c.ym[s] : 0.0;
+      const double cs = c.cs[s];
+      for (int r = c0 + lane; r < s_end; r += 64) {
+        const bool has_b = r + 32 < s_end;
+        const int rb = has_b ? r + 32 : r;
+        double xa[NX], xb[NX];
+        varying_row<NB, NV>(d.design, vc, r, xa);
+        varying_row<NB, NV>(d.design, vc, rb, xb);
+        const double ea = nb_exp(eta_from<NV>(xa, beta, __ldg(d.log_offset + r) + cs));
+        const double eb = nb_exp(eta_from<NV>(xb, beta, __ldg(d.log_offset + rb) + cs));
+        if constexpr (PASS == 1) {
+          acc[0] += ea;
+          if (has_b) acc[0] += eb;
+        } else {
+          dense_two<NV>(acc, xa, ea, yms, gamma);
+          if (has_b) dense_two<NV>(acc, xb, eb, yms, gamma);
+        }
+      }
+      reduce_to<N>(acc, c.slots + (s + warp) * stride, lane);
+      c0 = s_end;
+    }
+  }
+  const uint64_t* runs = d.runs + static_cast<size_t>(gene) * (K + 1);
+  for (int s = warp; s < K; s += kWarps) {
+    const uint64_t p0 = runs[s], p1 = runs[s + 1];
+    double acc[N];
+#pragma unroll
+    for (int v = 0; v < N; ++v) acc[v] = 0.0;
+    const double yms = PASS == 2 ? c.ym[s] : 0.0;
+    const double cs = c.cs[s];
+    for (uint64_t p = p0 + lane; p < p1; p += 64) {
+      const bool has_b = p + 32 < p1;
+      const uint64_t pb = has_b ? p + 32 : p;
+      const int ca = static_cast<int>(__ldg(d.cells + p)), cb = static_cast<int>(__ldg(d.cells + pb));
+      const double ya = __ldg(d.counts + p), yb = __ldg(d.counts + pb);
+      double xa[NX], xb[NX];
+      varying_row<NB, NV>(d.design, vc, ca, xa);
+      varying_row<NB, NV>(d.design, vc, cb, xb);
+      const double eta_a = eta_from<NV>(xa, beta, __ldg(d.log_offset + ca) + cs);
+      const double eta_b = eta_from<NV>(xb, beta, __ldg(d.log_offset + cb) + cs);
+      if constexpr (PASS == 1) {
+        acc[1] = nb_fma(eta_a, ya, acc[1]);
+        if (has_b) acc[1] = nb_fma(eta_b, yb, acc[1]);
+      } else {
+        sparse_two<NV>(acc, xa, nb_exp(eta_a), ya, yms, gamma);
+        if (has_b) sparse_two<NV>(acc, xb, nb_exp(eta_b), yb, yms, gamma);
+      }
+    }
+    reduce_to<N>(acc, c.slots + (K + kWarps + s) * stride, lane);
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < K * N; idx += blockDim.x) {
+    const int s = idx / N, v = idx - s * N;
+    const uint32_t a0 = c.fid[s], a1 = c.fid[s + 1];
+    double total = 0.0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w)
+      if (c.wcells[w] < a1 && c.wcells[w + 1] > a0) total += c.slots[(s + w) * stride + v];
+    total += c.slots[(K + kWarps + s) * stride + v];
+    out[s * out_stride + v] = total;
+  }
+  __syncthreads();
+}
+
+// Subject s's full pass-two row (PDims<NB>) from its reduced one, element x.
+template <int NB, int NV>
+__device__ __forceinline__ double expand_two(const double* R, const double* X, const int32_t* vpos, int x) {
+  using F = PDims<NB>;
+  using D = RDims<NV>;
+  if (x < F::kXf) return R[x];
+  if (x < F::kBp) {
+    const int part = (x - F::kXf) / NB, a = (x - F::kXf) - part * NB, va = vpos[a];
+    const int from[4] = {D::kXf, D::kD41, D::kT1, D::kT2};
+    const int scalar[4] = {D::kE, 6, 7, 8};
+    return va >= 0 ? R[from[part] + va] : X[a] * R[scalar[part]];
+  }
+  const bool q = x >= F::kBq;
+  int a = 0, rem = x - (q ? F::kBq : F::kBp);
+  while (rem >= NB - a) {
+    rem -= NB - a;
+    ++a;
+  }
+  const int b = a + rem, va = vpos[a], vb = vpos[b];
+  const int vec = q ? D::kQv : D::kXf;
+  if (va >= 0 && vb >= 0) return R[(q ? D::kBq : D::kBp) + va * NV - va * (va - 1) / 2 + (vb - va)];
+  if (vb >= 0) return X[a] * R[vec + vb];
+  if (va >= 0) return X[b] * R[vec + va];
+  return X[a] * (X[b] * R[q ? D::kEq : D::kE]);
+}
+
+template <int NB, int NV>
+__device__ PtmgCta ptmg_setup(const GeneData& d, double* smem, double* scratch) {
+  const int K = d.n_subjects;
+  PtmgCta c;
+  c.ym = smem;
+  c.p1 = c.ym + K;
+  c.cs = c.p1 + 2 * K;
+  c.fid = reinterpret_cast<uint32_t*>(c.cs + K);
+  c.wcells = c.fid + K + 1;
+  c.vpos = reinterpret_cast<int32_t*>(c.wcells + kWarps + 1);
+  for (int i = threadIdx.x; i <= K; i += blockDim.x) c.fid[i] = d.fid[i];
+  if (threadIdx.x <= kWarps) c.wcells[threadIdx.x] = d.warp_cells[threadIdx.x];
+  if (threadIdx.x < NB) {
+    int pos = -1;
+    for (int j = 0; j < NV; ++j)
+      if (d.varying[j] == static_cast<int>(threadIdx.x)) pos = j;
+    c.vpos[threadIdx.x] = pos;
+  }
+  const size_t per_cta = static_cast<size_t>(2 * K + kWarps) * RDims<NV>::W + static_cast<size_t>(K) * RDims<NV>::W;
+  c.slots = scratch + static_cast<size_t>(blockIdx.x) * per_cta;
+  c.reduced = c.slots + static_cast<size_t>(2 * K + kWarps) * RDims<NV>::W;
+  return c;
+}
+
+// Both passes of one request into `out` ((2 + W) K doubles).
+template <int NB, int NV>
+__device__ void ptmg_one(const GeneData& d, const PtmgCta& c, const PtmgRequest& req, double* beta_sm, double* out) {
+  using F = PDims<NB>;
+  using D = RDims<NV>;
+  constexpr int NX = NV > 0 ? NV : 1;
+  const int K = d.n_subjects;
+  const int tid = threadIdx.x;
+  if (tid < NB) beta_sm[tid] = req.beta[tid];
+  __syncthreads();
+  // the constant columns' share of eta per subject, in column order
+  for (int s = tid; s < K; s += blockDim.x) {
+    double v = 0.0;
+    if (c.fid[s] < c.fid[s + 1]) {
+      const double* row = d.design + static_cast<size_t>(c.fid[s]) * NB;
+#pragma unroll
+      for (int a = 0; a < NB; ++a)
+        if (c.vpos[a] < 0) v = nb_fma(__ldg(row + a), beta_sm[a], v);
+    }
+    c.cs[s] = v;
+  }
+  int vc[NX];
+  double beta[NX];
+#pragma unroll
+  for (int j = 0; j < NV; ++j) {
+    vc[j] = d.varying[j];
+    beta[j] = beta_sm[vc[j]];
+  }
+  __syncthreads();
+  tree_pass<NB, NV, 1, 2>(d, c, req.gene, beta, req.gamma, vc, D::W, c.p1, 2);
+  const double* tot = d.totals + static_cast<size_t>(req.gene) * K;
+  for (int s = tid; s < K; s += blockDim.x) {
+    c.ym[s] = (__ldg(tot + s) + req.alpha) / (c.p1[2 * s] + req.lambda);
+    out[s] = c.p1[2 * s];          // cumsumxtb
+    out[K + s] = c.p1[2 * s + 1];  // ylin
+  }
+  __syncthreads();
+  tree_pass<NB, NV, 2, D::W>(d, c, req.gene, beta, req.gamma, vc, D::W, c.reduced, D::W);
+  // every subject's full row, the constant columns' sums from the scalars
+  for (int idx = tid; idx < K * F::W; idx += blockDim.x) {
+    const int s = idx / F::W, x = idx - s * F::W;
+    double X[NB];
+    const bool has = c.fid[s] < c.fid[s + 1];
+    const double* row = d.design + static_cast<size_t>(has ? c.fid[s] : 0) * NB;
+#pragma unroll
+    for (int a = 0; a < NB; ++a) X[a] = has ? __ldg(row + a) : 0.0;
+    out[2 * K + idx] = expand_two<NB, NV>(c.reduced + static_cast<size_t>(s) * D::W, X, c.vpos, x);
+  }
+}
+
+__device__ __forceinline__ long long global_ns() {
+  long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Streaming mode: one persistent launch for stage one, the request-ring
+// protocol of FitQueue (pml_device.cuh) with one CTA per request.
+template <int NB, int NV>
+__global__ void __launch_bounds__(kThreads, ptmg_min_blocks(NB, NV))
+    ptmg_queue_kernel(GeneData d, PtmgQueue qu, double* scratch) {
+  extern __shared__ __align__(16) double smem[];
+  const PtmgCta c = ptmg_setup<NB, NV>(d, smem, scratch);
+  __shared__ long long next_ticket;
+  __shared__ double beta_sm[kMaxCoef];
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const long long t = static_cast<long long>(atomicAdd(qu.taken, 1ull));
+      const volatile long long* seq = qu.seq + (t & qu.mask);
+      const volatile int* stop = qu.stop;
+      const long long t0 = global_ns();
+      unsigned int pause = 128;
+      long long got = -1;
+      for (;;) {
+        if (*seq == t) {
+          got = t;
+          break;
+        }
+        if (*stop != 0) break;
+        if (global_ns() - t0 > qu.idle_ns) {
+          atomicExch(qu.status, 1);
+          break;
+        }
+        __nanosleep(pause);
+        if (pause < 2048) pause *= 2;
+      }
+      next_ticket = got;
+    }
+    __syncthreads();
+    const long long t = next_ticket;
+    if (t < 0) break;
+    PtmgRequest req;
+    {
+      const int4* src = reinterpret_cast<const int4*>(qu.ring + (t & qu.mask));
+      int4* dst = reinterpret_cast<int4*>(&req);
+#pragma unroll
+      for (int i = 0; i < static_cast<int>(sizeof(PtmgRequest) / 16); ++i) dst[i] = __ldcg(src + i);
+    }
+    ptmg_one<NB, NV>(d, c, req, beta_sm, qu.results + (t & qu.mask) * qu.result_stride);
+    // every thread's result writes reach host memory before the flag
+    __threadfence_system();
+    __syncthreads();
+    if (threadIdx.x == 0) reinterpret_cast<volatile long long*>(qu.done)[t & qu.mask] = t + 1;
+  }
+}
+
+inline size_t smem_bytes(int K) {
+  return static_cast<size_t>(4 * K) * 8 + (K + 1 + kWarps + 1 + kMaxCoef) * 4 + 16;
+}
+
+template <int NB, int NV>
+int launch_queue_nb(const GeneData& d, const PtmgQueue& qu, double* scratch, int grid, cudaStream_t stream) {
+  const size_t smem = smem_bytes(d.n_subjects);
+  cudaError_t e = cudaFuncSetAttribute(ptmg_queue_kernel<NB, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  ptmg_queue_kernel<NB, NV><<<grid, kThreads, smem, stream>>>(d, qu, scratch);
+  return cudaGetLastError();
+}
+
+template <int NB, int NV>
+int blocks_nb(int K) {
+  const size_t smem = smem_bytes(K);
+  if (cudaFuncSetAttribute(ptmg_queue_kernel<NB, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(smem)) != cudaSuccess)
+    return 0;
+  int blocks = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, ptmg_queue_kernel<NB, NV>, kThreads, smem) !=
+      cudaSuccess)
+    return 0;
+  return blocks;
+}
+
+template <int NB, int NV>
+size_t scratch_nb(int K) {
+  return static_cast<size_t>(3 * K + kWarps) * RDims<NV>::W;
+}
+
+template <int NB, int NV = 0>
+PtmgOps ptmg_ops_for(int n_varying) {
+  if constexpr (NV > NB) {
+    return PtmgOps{};
+  } else {
+    if (n_varying == NV) return PtmgOps{&launch_queue_nb<NB, NV>, &blocks_nb<NB, NV>, &scratch_nb<NB, NV>};
+    return ptmg_ops_for<NB, NV + 1>(n_varying);
+  }
+}
+
+}  // namespace
+}  // namespace device
+}  // namespace nebula

@@ -276,9 +276,13 @@ void DeviceFitter::ensure_ptmg_scratch() {
   int sms = 0, dev = 0;
   cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
   cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute");
-  pgrid_ = sms;  // one CTA per SM (the kernel is bound to one resident block)
-  d_scratch_ = pool_alloc<double>(static_cast<size_t>(pgrid_) * device::ptmg_scratch_doubles(K, data_.n_coef),
-                                   stream_, &pooled_);
+  const int per_sm = device::ptmg_blocks_per_sm(K, data_.n_coef, data_.n_varying);
+  if (per_sm <= 0)
+    fail(NB_ERR_UNSUPPORTED, "the stage-one kernel cannot be resident with " + std::to_string(K) + " subjects");
+  pgrid_ = per_sm * sms;
+  d_scratch_ = pool_alloc<double>(
+      static_cast<size_t>(pgrid_) * device::ptmg_scratch_doubles(K, data_.n_coef, data_.n_varying), stream_,
+      &pooled_);
 }
 
 size_t DeviceFitter::ptmg_stride() const {
@@ -306,7 +310,7 @@ void DeviceFitter::ptmg_queue_start(size_t capacity) {
   ++launches_;
 }
 
-long long DeviceFitter::ptmg_post(const device::PtmgRequest* reqs, size_t n) { return ptmgq_->try_post(reqs, n); }
+long long DeviceFitter::ptmg_post(const device::PtmgRequest* reqs, size_t n) { return ptmgq_->post(reqs, n); }
 void DeviceFitter::ptmg_consumed(long long ticket) { ptmgq_->consumed(ticket); }
 bool DeviceFitter::ptmg_done(long long ticket) const { return ptmgq_->done(ticket); }
 const double* DeviceFitter::ptmg_result(long long ticket) const {
@@ -644,15 +648,66 @@ std::unique_ptr<Session> create_session(const nb_csr* counts, const uint64_t* su
     for (int j = 0; j < nb; ++j) r.beta[j] = x[j];
     return r;
   };
+  // Workers queue their genes' next requests here; one poster thread posts
+  // each drain as one batch (the workers never wait on the copies, and the
+  // batches grow while a post is under way), as in stages two and three.
+  std::mutex queue_mu;
+  std::vector<device::PtmgRequest> queued;
+  std::vector<size_t> queued_genes;
+  std::atomic<int> workers_left{workers};
+  auto poster = [&]() {
+    std::vector<device::PtmgRequest> batch;
+    std::vector<size_t> genes;
+    try {
+      while (!abort.load(std::memory_order_relaxed)) {
+        bool idle = false;
+        {
+          std::lock_guard<std::mutex> lock(queue_mu);
+          batch.swap(queued);
+          genes.swap(queued_genes);
+          idle = batch.empty() && workers_left.load() == 0;
+        }
+        if (idle) return;
+        if (batch.empty()) {
+          std::this_thread::yield();
+          continue;
+        }
+        // chunks of at most a quarter of the ring; the owning workers read the
+        // tickets with acquire loads
+        for (size_t at = 0; at < batch.size();) {
+          const size_t n = std::min(batch.size() - at, capacity / 4);
+          const long long first = ss->fitter->ptmg_post(batch.data() + at, n);
+          for (size_t k = 0; k < n; ++k)
+            std::atomic_ref<long long>(ticket[genes[at + k]]).store(first + static_cast<long long>(k),
+                                                                    std::memory_order_release);
+          at += n;
+        }
+        batch.clear();
+        genes.clear();
+      }
+    } catch (const NbError& e) {
+      std::lock_guard<std::mutex> lock(err_mu);
+      if (!first_err) first_err = e;
+      abort.store(true);
+    } catch (const std::exception& e) {
+      std::lock_guard<std::mutex> lock(err_mu);
+      if (!first_err) first_err = NbError{NB_ERR_GPU, e.what()};
+      abort.store(true);
+    }
+  };
   auto worker = [&](int w) {
+    struct Leave {
+      std::atomic<int>& left;
+      ~Leave() { left.fetch_sub(1); }
+    } leave{workers_left};
     try {
       std::vector<size_t> waiting, owners;
       std::vector<device::PtmgRequest> box;
       auto post = [&]() {
         if (box.empty()) return;
-        const long long first = ss->fitter->ptmg_post(box.data(), box.size());
-        if (first < 0) return;  // a slot's previous result is unread: retry after this worker's next pass
-        for (size_t k = 0; k < owners.size(); ++k) ticket[owners[k]] = first + static_cast<long long>(k);
+        std::lock_guard<std::mutex> lock(queue_mu);
+        queued.insert(queued.end(), box.begin(), box.end());
+        queued_genes.insert(queued_genes.end(), owners.begin(), owners.end());
         box.clear();
         owners.clear();
       };
@@ -664,16 +719,15 @@ std::unique_ptr<Session> create_session(const nb_csr* counts, const uint64_t* su
         box.push_back(request_of(g));
         owners.push_back(g);
         waiting.push_back(g);
-        if (box.size() >= 64) post();
+        post();
       }
-      post();
       std::vector<double> grad(np), hess(static_cast<size_t>(np) * np), x(np);
       auto last_progress = Clock::now();
       while (!waiting.empty() && !abort.load(std::memory_order_relaxed)) {
         bool progressed = false;
         for (size_t i = 0; i < waiting.size();) {
           const size_t g = waiting[i];
-          if (!ss->fitter->ptmg_done(ticket[g])) {
+          if (!ss->fitter->ptmg_done(std::atomic_ref<long long>(ticket[g]).load(std::memory_order_acquire))) {
             ++i;
             continue;
           }
@@ -724,10 +778,12 @@ std::unique_ptr<Session> create_session(const nb_csr* counts, const uint64_t* su
       ~QueueGuard() { f.ptmg_abort(); }
     } guard{*ss->fitter};
     ss->fitter->ptmg_queue_start(capacity);
+    std::thread post_thread(poster);
     std::vector<std::thread> pool;
     for (int w = 1; w < workers; ++w) pool.emplace_back(worker, w);
     worker(0);
     for (auto& th : pool) th.join();
+    post_thread.join();
     if (first_err) throw *first_err;
     ss->fitter->ptmg_stop();
   }

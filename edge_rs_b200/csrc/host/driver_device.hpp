@@ -78,7 +78,7 @@ class DeviceFitter {
   // Stage one in streaming mode (device::PtmgQueue), the same protocol as
   // the fit queue below; a result is ptmg_stride() doubles.
   void ptmg_queue_start(size_t capacity);
-  // -1 (nothing posted) while a slot's previous result is unread (try_post)
+  // Posts from a thread that reads no results (RequestQueue::post).
   long long ptmg_post(const device::PtmgRequest* reqs, size_t n);
   void ptmg_consumed(long long ticket);
   bool ptmg_done(long long ticket) const;

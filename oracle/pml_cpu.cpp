@@ -69,21 +69,11 @@ std::vector<size_t> positive_runs(const PmlData& d) {
   return run;
 }
 
-namespace {
-
-// Slot layout of a per-subject partial: resid, weight, sum ln t, sum y eta,
-// sum y ln t, X'd (nb), sum p x (nb), sum p x x' (upper triangle).
-enum { kResid = 0, kWeight = 1, kSumLog = 2, kLinear = 3, kWlog = 4, kScore = 5 };
-
 // The design columns that take more than one value within some subject (the
 // reference's cell_level_columns, ptmg.rs:1962-2005), increasing; vpos[a] is
 // column a's index among them, or -1 for a column constant within every
 // subject. A sweep sums only the varying columns per cell and applies each
 // constant column's share per subject.
-struct Split {
-  std::vector<int> varying, vpos;
-};
-
 Split split_columns(const PmlData& d) {
   Split sp;
   sp.vpos.assign(d.n_beta, -1);
@@ -139,6 +129,12 @@ double varying_eta(const Split& sp, const double* x, const std::vector<double>& 
   for (size_t j = 0; j < sp.varying.size(); ++j) eta = nebula::nb_fma(x[j], beta[sp.varying[j]], eta);
   return eta;
 }
+
+namespace {
+
+// Slot layout of a per-subject partial: resid, weight, sum ln t, sum y eta,
+// sum y ln t, X'd (nb), sum p x (nb), sum p x x' (upper triangle).
+enum { kResid = 0, kWeight = 1, kSumLog = 2, kLinear = 3, kWlog = 4, kScore = 5 };
 
 // The fold of pml.rs:1469-1489 over the varying columns (nb of them): d
 // into the gradient, p into the curvature.

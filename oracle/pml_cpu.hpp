@@ -33,6 +33,18 @@ struct PmlData {
   const nebula::zero::Tables* zeros = nullptr;
 };
 
+// The design columns that vary within some subject (increasing) and each
+// column's index among them (-1 for one constant within every subject); the
+// sweeps sum only the varying columns per cell (pml_cpu.cpp, ptmg_cpu.cpp).
+struct Split {
+  std::vector<int> varying, vpos;
+};
+Split split_columns(const PmlData& d);
+// Subject s's design row (zeros for a subject without cells).
+std::vector<double> subject_row(const PmlData& d, int s);
+// Cell r's varying design values into x; returns how many.
+int varying_row(const PmlData& d, const Split& sp, size_t r, double* x);
+
 struct PmlParams {
   bool reml = false;
   double eps = 1e-6;

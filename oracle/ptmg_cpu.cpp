@@ -21,24 +21,44 @@ using nebula::nb_exp;
 using nebula::nb_fma;
 using nebula::nb_log;
 
-double eta_at(const PmlData& d, const double* beta, size_t r) {
-  const double* row = d.design + r * d.n_beta;
-  double eta = d.offset[r];
-  for (int j = 0; j < d.n_beta; ++j) eta = nb_fma(row[j], beta[j], eta);
-  return eta;
-}
 
 }  // namespace
 
 nebula::PtmgSums ptmg_sums(const PmlData& d, const double* beta, double alpha, double lambda, double gamma) {
   const int nb = d.n_beta, k = d.k, T = nb * (nb + 1) / 2, W = nebula::ptmg_width(nb);
   const int kXf = 9, kD41 = kXf + nb, kT1 = kD41 + nb, kT2 = kT1 + nb, kBp = kT2 + nb, kBq = kBp + T;
+  // the per-cell sums run over the varying columns (ptmg_impl.cuh): the
+  // reduced row holds the nine scalars, sum e, sum e q, the vectors Xf, D41,
+  // T1, T2, Eq over the varying columns and the triangles Bp, Bq
+  const Split sp = split_columns(d);
+  const int nv = static_cast<int>(sp.varying.size()), tv = nv * (nv + 1) / 2;
+  const int rE = 9, rEq = 10, rXf = 11, rD41 = rXf + nv, rT1 = rD41 + nv, rT2 = rT1 + nv, rQv = rT2 + nv;
+  const int rBp = rQv + nv, rBq = rBp + tv, RW = rBq + tv;
+  std::vector<double> cs(k), bv(nv);
+  for (int j = 0; j < nv; ++j) bv[j] = beta[sp.varying[j]];
+  for (int s = 0; s < k; ++s) {  // the constant columns' share of eta, in column order
+    const std::vector<double> row = subject_row(d, s);
+    double c = 0.0;
+    for (int a = 0; a < nb; ++a)
+      if (sp.vpos[a] < 0) c = nb_fma(row[a], beta[a], c);
+    cs[s] = c;
+  }
+  auto eta_at = [&](size_t r, int s, double* x) {
+    varying_row(d, sp, r, x);
+    double eta = d.offset[r] + cs[s];
+    for (int j = 0; j < nv; ++j) eta = nb_fma(x[j], bv[j], eta);
+    return eta;
+  };
   const std::vector<size_t> run = positive_runs(d);
   nebula::PtmgSums out;
   // pass one: sum e over every cell, sum y eta over the positive ones
-  auto dense1 = [&](double* acc, size_t r, int) { acc[0] += nb_exp(eta_at(d, beta, r)); };
-  auto sparse1 = [&](double* acc, size_t i, int) {
-    acc[1] = nb_fma(eta_at(d, beta, d.cells[i]), d.counts[i], acc[1]);
+  auto dense1 = [&](double* acc, size_t r, int s) {
+    double x[8];
+    acc[0] += nb_exp(eta_at(r, s, x));
+  };
+  auto sparse1 = [&](double* acc, size_t i, int s) {
+    double x[8];
+    acc[1] = nb_fma(eta_at(d.cells[i], s, x), d.counts[i], acc[1]);
   };
   std::vector<double> p1 = tree_sums(d, run, 2, dense1, sparse1);
   out.cumsumxtb.resize(k);
@@ -51,8 +71,8 @@ nebula::PtmgSums ptmg_sums(const PmlData& d, const double* beta, double alpha, d
   }
   // pass two
   auto dense2 = [&](double* acc, size_t r, int s) {
-    const double* x = d.design + r * nb;
-    const double e = nb_exp(eta_at(d, beta, r));
+    double x[8];
+    const double e = nb_exp(eta_at(r, s, x));
     const double yms = ym[s];
     const double we = yms * e;
     const double w = we + gamma;
@@ -72,26 +92,28 @@ nebula::PtmgSums ptmg_sums(const PmlData& d, const double* beta, double alpha, d
     acc[8] = nb_fma(gte, e, acc[8]);
     const double f1 = gt - iw;
     const double q = yms * (yms * gte - gg);
+    acc[rE] += e;
+    acc[rEq] = nb_fma(e, q, acc[rEq]);
     int t = 0;
-    for (int a = 0; a < nb; ++a) {
+    for (int a = 0; a < nv; ++a) {
       const double xe = x[a] * e;
-      acc[kXf + a] += xe;
-      acc[kD41 + a] = nb_fma(gg, xe, acc[kD41 + a]);
-      acc[kT1 + a] = nb_fma(xe, f1, acc[kT1 + a]);
-      acc[kT2 + a] = nb_fma(xe, gte, acc[kT2 + a]);
-      for (int b = a; b < nb; ++b) {
+      acc[rXf + a] += xe;
+      acc[rD41 + a] = nb_fma(gg, xe, acc[rD41 + a]);
+      acc[rT1 + a] = nb_fma(xe, f1, acc[rT1 + a]);
+      acc[rT2 + a] = nb_fma(xe, gte, acc[rT2 + a]);
+      acc[rQv + a] = nb_fma(xe, q, acc[rQv + a]);
+      for (int b = a; b < nv; ++b) {
         const double c = xe * x[b];
-        acc[kBp + t] += c;
-        acc[kBq + t] = nb_fma(c, q, acc[kBq + t]);
+        acc[rBp + t] += c;
+        acc[rBq + t] = nb_fma(c, q, acc[rBq + t]);
         ++t;
       }
     }
   };
   auto sparse2 = [&](double* acc, size_t i, int s) {
-    const size_t c = d.cells[i];
-    const double* x = d.design + c * nb;
+    double x[8];
     const double y = d.counts[i];
-    const double e = nb_exp(eta_at(d, beta, c));
+    const double e = nb_exp(eta_at(d.cells[i], s, x));
     const double yms = ym[s];
     const double w = yms * e + gamma;
     const double lw = nb_log(w);
@@ -106,20 +128,51 @@ nebula::PtmgSums ptmg_sums(const PmlData& d, const double* beta, double alpha, d
     acc[7] += gte;
     acc[8] = nb_fma(gte, e, acc[8]);
     const double q = yms * (yms * gte - gg);
+    acc[rEq] = nb_fma(e, q, acc[rEq]);
     int t = 0;
-    for (int a = 0; a < nb; ++a) {
+    for (int a = 0; a < nv; ++a) {
       const double xe = x[a] * e;
-      acc[kD41 + a] = nb_fma(gg, xe, acc[kD41 + a]);
-      acc[kT1 + a] = nb_fma(xe, gt, acc[kT1 + a]);
-      acc[kT2 + a] = nb_fma(xe, gte, acc[kT2 + a]);
-      for (int b = a; b < nb; ++b) {
+      acc[rD41 + a] = nb_fma(gg, xe, acc[rD41 + a]);
+      acc[rT1 + a] = nb_fma(xe, gt, acc[rT1 + a]);
+      acc[rT2 + a] = nb_fma(xe, gte, acc[rT2 + a]);
+      acc[rQv + a] = nb_fma(xe, q, acc[rQv + a]);
+      for (int b = a; b < nv; ++b) {
         const double cc = xe * x[b];
-        acc[kBq + t] = nb_fma(cc, q, acc[kBq + t]);
+        acc[rBq + t] = nb_fma(cc, q, acc[rBq + t]);
         ++t;
       }
     }
   };
-  out.sums = tree_sums(d, run, W, dense2, sparse2);
+  const std::vector<double> red = tree_sums(d, run, RW, dense2, sparse2);
+  // every subject's full row: a constant column's sums are its value times a
+  // scalar sum (sum x_a e = x_a sum e, sum x_a gg e = x_a acc[6], ...)
+  out.sums.assign(static_cast<size_t>(k) * W, 0.0);
+  for (int s = 0; s < k; ++s) {
+    const double* R = &red[static_cast<size_t>(s) * RW];
+    const std::vector<double> X = subject_row(d, s);
+    double* F = &out.sums[static_cast<size_t>(s) * W];
+    for (int x = 0; x < kXf; ++x) F[x] = R[x];
+    const int from[4] = {rXf, rD41, rT1, rT2}, scalar[4] = {rE, 6, 7, 8}, block[4] = {kXf, kD41, kT1, kT2};
+    for (int part = 0; part < 4; ++part)
+      for (int a = 0; a < nb; ++a) {
+        const int va = sp.vpos[a];
+        F[block[part] + a] = va >= 0 ? R[from[part] + va] : X[a] * R[scalar[part]];
+      }
+    for (int qpart = 0; qpart < 2; ++qpart) {
+      const int base = qpart ? rBq : rBp, vec = qpart ? rQv : rXf, sc = qpart ? rEq : rE;
+      int t = 0;
+      for (int a = 0; a < nb; ++a)
+        for (int b = a; b < nb; ++b, ++t) {
+          const int va = sp.vpos[a], vb = sp.vpos[b];
+          double v;
+          if (va >= 0 && vb >= 0) v = R[base + va * nv - va * (va - 1) / 2 + (vb - va)];
+          else if (vb >= 0) v = X[a] * R[vec + vb];
+          else if (va >= 0) v = X[b] * R[vec + va];
+          else v = X[a] * (X[b] * R[sc]);
+          F[(qpart ? kBq : kBp) + t] = v;
+        }
+    }
+  }
   return out;
 }
 
