@@ -240,7 +240,7 @@ __device__ __forceinline__ void fold(double* acc, const double* x, double d, dou
 // The four per-cell Laplace sums (pml.rs:1842-1856, 1863-1868, 1893-1899),
 // each term scaled by gamma (dense) or the count (sparse).
 __device__ __forceinline__ void laplace_terms(double* acc, double e, double t, double gamma, double scale) {
-  const double inv = 1.0 / t;
+  const double inv = nb_recip(t);
   const double p2 = (e * inv) * inv, p3 = p2 * inv, p4 = p3 * inv, p5 = p4 * inv, e2 = e * e;
   acc[0] += scale * p2;
   acc[1] += scale * (p3 * (gamma - e));
@@ -366,7 +366,7 @@ __device__ void sweep_sums(const GeneData& d, Smem<NB, NV>& sm, const double* be
           const double ta = ea + gamma, tb = eb + gamma;
           if (MODE == 0) {
             const double la = nb_log_tab(ta, tab), lb = nb_log_tab(tb, tab);
-            const double inva = 1.0 / ta, invb = 1.0 / tb;
+            const double inva = nb_recip(ta), invb = nb_recip(tb);
             const double ua = ea * inva, ub = eb * invb;
             acc[kSumLog] += la;
             fold<NV>(acc, xa, -gamma * ua, (gamma * ua) * inva);
@@ -421,7 +421,7 @@ __device__ void sweep_sums(const GeneData& d, Smem<NB, NV>& sm, const double* be
           const double ta = ea + gamma, tb = eb + gamma;
           if (MODE == 0) {
             const double la = nb_log_tab(ta, tab), lb = nb_log_tab(tb, tab);
-            const double inva = 1.0 / ta, invb = 1.0 / tb;
+            const double inva = nb_recip(ta), invb = nb_recip(tb);
             const double ua = ea * inva, ub = eb * invb;
             acc[kSumLog] += la;
             fold<NV>(acc, xa, -gamma * ua, (gamma * ua) * inva);
@@ -454,7 +454,7 @@ __device__ void sweep_sums(const GeneData& d, Smem<NB, NV>& sm, const double* be
         const double ta = ea + gamma, tb = eb + gamma;
         if (MODE == 0) {
           const double la = nb_log_tab(ta, tab), lb = nb_log_tab(tb, tab);
-          const double inva = 1.0 / ta, invb = 1.0 / tb;
+          const double inva = nb_recip(ta), invb = nb_recip(tb);
           const double ua = ea * inva, ub = eb * invb;
           acc[kLinear] = nb_fma(eta_a, ya, acc[kLinear]);
           acc[kWlog] = nb_fma(ya, la, acc[kWlog]);

@@ -113,7 +113,7 @@ __device__ __forceinline__ void dense_two(double* acc, const double* x, double e
   const double we = ym * e;
   const double w = we + gamma;
   const double lw = nb_log(w);
-  const double iw = 1.0 / w;
+  const double iw = nb_recip(w);
   const double gg = gamma * iw;
   const double gt = gg * iw;
   const double gte = gt * e;
@@ -156,7 +156,7 @@ __device__ __forceinline__ void sparse_two(double* acc, const double* x, double 
   using D = RDims<NV>;
   const double w = ym * e + gamma;
   const double lw = nb_log(w);
-  const double iw = 1.0 / w;
+  const double iw = nb_recip(w);
   const double gg = y * iw;
   const double gt = gg * iw;
   const double gte = gt * e;

@@ -77,6 +77,15 @@ NB_HD double nb_from_bits(uint64_t u) {
 // 2^k for -1022 <= k <= 1023
 NB_HD double nb_pow2(int k) { return nb_from_bits(static_cast<uint64_t>(k + 1023) << 52); }
 
+// 1/x correctly rounded (the same double as 1.0 / x).
+NB_HD double nb_recip(double x) {
+#ifdef __CUDA_ARCH__
+  return __drcp_rn(x);
+#else
+  return 1.0 / x;
+#endif
+}
+
 NB_HD double nb_rint(double x) {
   // round to nearest (ties to even) for |x| < 2^51
   const double shifter = 6755399441055744.0;  // 1.5 * 2^52
@@ -174,12 +183,30 @@ inline constexpr NbTableData kNbTables = {
 };
 
 NB_HD double nb_exp_tab(double x, const NbTableData* t) {
-  if (!(x == x)) return x;                      // NaN
-  if (x > 709.782712893384) return 1.0 / 0.0;  // overflow
-  if (x < -745.1332191019412) return 0.0;      // underflow
   const double inv_l = 0x1.71547652b82fep+8;    // 256 / ln 2
   const double l_hi = 0x1.62e42fef80000p-9;     // ln 2 / 256, 34 bits
   const double l_lo = 0x1.1cf79abc9e3b4p-44;
+  if (x > -707.0 && x < 707.0) {
+    // The common range (NaN fails the test): the same steps as below with
+    // the special cases left out. n = rint(x * inv_l) is read from the
+    // shifter's low word instead of a conversion, (n - n mod 256) / 256 is an
+    // arithmetic shift, and 2^m stays normal (|m| <= 1020).
+    const double shifted = x * inv_l + 6755399441055744.0;  // 1.5 * 2^52
+    const double n = shifted - 6755399441055744.0;
+    double r = nb_fma(-n, l_hi, x);
+    r = nb_fma(-n, l_lo, r);
+    double p = nb_fma(r, 1.0 / 120.0, 1.0 / 24.0);
+    p = nb_fma(p, r, 1.0 / 6.0);
+    p = nb_fma(p, r, 0.5);
+    const double q = nb_fma(r * r, p, r);
+    const int ni = static_cast<int>(static_cast<uint32_t>(nb_bits(shifted)));
+    const NbPair s = t->exp2_frac[ni & 255];
+    const double er = s.a + nb_fma(s.a, q, s.b);
+    return er * nb_pow2(ni >> 8);
+  }
+  if (!(x == x)) return x;                      // NaN
+  if (x > 709.782712893384) return 1.0 / 0.0;  // overflow
+  if (x < -745.1332191019412) return 0.0;      // underflow
   const double n = nb_rint(x * inv_l);
   double r = nb_fma(-n, l_hi, x);
   r = nb_fma(-n, l_lo, r);
@@ -198,6 +225,36 @@ NB_HD double nb_exp_tab(double x, const NbTableData* t) {
 }
 
 NB_HD double nb_log_tab(double x, const NbTableData* t) {
+  const double ln2_hi = 0x1.62e42fee00000p-1;  // 32 bits: e ln2_hi is exact
+  const double ln2_lo = 0x1.a39ef35793c76p-33;
+  if (x >= 2.2250738585072014e-308 && x < 1.0 / 0.0) {
+    // The common range (positive, normal, finite; NaN fails the test): the
+    // same steps as below with the special cases left out, and e converted
+    // to a double through the shifter.
+    const uint64_t u = nb_bits(x);
+    int e = static_cast<int>(u >> 52) - 1023;
+    const uint64_t f = u & 0x000fffffffffffffULL;
+    double m = nb_from_bits(f | 0x3ff0000000000000ULL);  // [1, 2)
+    int j = static_cast<int>((f + (1ULL << 43)) >> 44);
+    if (j == 256) {
+      j = 0;
+      e += 1;
+      m *= 0.5;
+    }
+    const NbPair c = t->log_inv_hi[j];
+    const double r = nb_fma(m, c.a, -1.0);
+    double p = nb_fma(r, 1.0 / 7.0, -1.0 / 6.0);
+    p = nb_fma(p, r, 0.2);
+    p = nb_fma(p, r, -0.25);
+    p = nb_fma(p, r, 1.0 / 3.0);
+    p = nb_fma(p, r, -0.5);
+    const double l1p = nb_fma(r * r, p, r);
+    const double ed =
+        nb_from_bits(0x4338000000000000ULL + static_cast<uint64_t>(static_cast<int64_t>(e))) - 6755399441055744.0;
+    const double hi = nb_fma(ed, ln2_hi, c.b);
+    const double lo = nb_fma(ed, ln2_lo, t->log_lo[j]);
+    return hi + (lo + l1p);
+  }
   if (!(x == x)) return x;         // NaN
   if (x < 0.0) return 0.0 / 0.0;   // NaN
   if (x == 0.0) return -1.0 / 0.0;
@@ -225,8 +282,6 @@ NB_HD double nb_log_tab(double x, const NbTableData* t) {
   p = nb_fma(p, r, 1.0 / 3.0);
   p = nb_fma(p, r, -0.5);
   const double l1p = nb_fma(r * r, p, r);
-  const double ln2_hi = 0x1.62e42fee00000p-1;  // 32 bits: e ln2_hi is exact
-  const double ln2_lo = 0x1.a39ef35793c76p-33;
   const double ed = static_cast<double>(e);
   const double hi = nb_fma(ed, ln2_hi, c.b);
   const double lo = nb_fma(ed, ln2_lo, t->log_lo[j]);
