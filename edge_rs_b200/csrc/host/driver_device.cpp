@@ -85,6 +85,48 @@ void keep_pool_memory() {
   cuda_check(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "memory pool threshold");
 }
 
+// Pinned host buffers for the upload's staging, kept in a process-wide pool:
+// pinned memory is slow to allocate and free, and a copy from it runs
+// asynchronously at the link's speed (a pageable source goes through the
+// driver's bounce buffers). A call takes one buffer (grown when too small)
+// and returns it once its copies have completed. Held until the process exits.
+class PinnedStage {
+ public:
+  explicit PinnedStage(size_t bytes) {
+    {
+      std::lock_guard<std::mutex> lock(mu());
+      if (!pool().empty()) {
+        buf_ = pool().back();
+        pool().pop_back();
+      }
+    }
+    if (buf_.second < bytes) {
+      if (buf_.first) cudaFreeHost(buf_.first);
+      buf_ = {nullptr, 0};
+      cuda_check(cudaMallocHost(&buf_.first, bytes), "cudaMallocHost");
+      buf_.second = bytes;
+    }
+  }
+  ~PinnedStage() {
+    std::lock_guard<std::mutex> lock(mu());
+    pool().push_back(buf_);
+  }
+  PinnedStage(const PinnedStage&) = delete;
+  PinnedStage& operator=(const PinnedStage&) = delete;
+  char* data() const { return static_cast<char*>(buf_.first); }
+
+ private:
+  static std::mutex& mu() {
+    static std::mutex m;
+    return m;
+  }
+  static std::vector<std::pair<void*, size_t>>& pool() {
+    static auto* p = new std::vector<std::pair<void*, size_t>>();
+    return *p;
+  }
+  std::pair<void*, size_t> buf_{nullptr, 0};
+};
+
 template <typename T>
 T* pool_alloc(size_t n, cudaStream_t stream, std::vector<void*>* pooled) {
   T* d = nullptr;
@@ -118,16 +160,18 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
   std::vector<uint64_t> gene_ptr(G + 1, 0);
   for (size_t g = 0; g < G; ++g) gene_ptr[g + 1] = gene_ptr[g] + genes[g].cells.size();
   const size_t nnz = gene_ptr[G];
-  // the kept genes' entries, concatenated on all host threads (the buffers
-  // are left uninitialised: every element is written once)
-  std::unique_ptr<uint32_t[]> cells(new uint32_t[std::max<size_t>(nnz, 1)]);
-  std::unique_ptr<double[]> counts(new double[std::max<size_t>(nnz, 1)]);
+  // the kept genes' entries, concatenated on all host threads straight into
+  // pinned staging (every element is written once)
+  const size_t nz = std::max<size_t>(nnz, 1);
+  PinnedStage stage(nz * (sizeof(double) + sizeof(uint32_t)));
+  double* const counts_h = reinterpret_cast<double*>(stage.data());
+  uint32_t* const cells_h = reinterpret_cast<uint32_t*>(stage.data() + nz * sizeof(double));
   std::vector<double> totals(G * K);
   std::vector<uint64_t> runs(G * (K + 1));
   parallel_for(G, 0, [&](size_t g) {
     const GeneCounts& gc = genes[g];
-    std::copy(gc.cells.begin(), gc.cells.end(), cells.get() + gene_ptr[g]);
-    std::copy(gc.counts.begin(), gc.counts.end(), counts.get() + gene_ptr[g]);
+    std::copy(gc.cells.begin(), gc.cells.end(), cells_h + gene_ptr[g]);
+    std::copy(gc.counts.begin(), gc.counts.end(), counts_h + gene_ptr[g]);
     std::copy(prep.totals.begin() + prep.kept[g] * K, prep.totals.begin() + (prep.kept[g] + 1) * K,
               totals.begin() + g * K);
     // positive_runs (pml.rs:1155-1160) as absolute positions
@@ -164,8 +208,8 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
   data_.log_offset = device_copy(sh.log_offset.data(), sh.log_offset.size(), stream_, &pooled_);
   data_.fid = device_copy(fid.data(), fid.size(), stream_, &pooled_);
   data_.gene_ptr = device_copy(gene_ptr.data(), gene_ptr.size(), stream_, &pooled_);
-  data_.cells = device_copy(cells.get(), nnz, stream_, &pooled_);
-  data_.counts = device_copy(counts.get(), nnz, stream_, &pooled_);
+  data_.cells = device_copy(cells_h, nnz, stream_, &pooled_);
+  data_.counts = device_copy(counts_h, nnz, stream_, &pooled_);
   data_.runs = device_copy(runs.data(), runs.size(), stream_, &pooled_);
   data_.totals = device_copy(totals.data(), totals.size(), stream_, &pooled_);
   data_.warp_cells = device_copy(wcells.data(), wcells.size(), stream_, &pooled_);
@@ -229,6 +273,8 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
     queue_clusters_[c] = device::fit_queue_max_clusters(K, sh.n_coef, data_.n_varying, c);
   cuda_check(cudaEventCreate(&step0_), "event");
   cuda_check(cudaEventCreate(&step1_), "event");
+  // the pinned staging goes back to its pool when this returns
+  cuda_check(cudaStreamSynchronize(stream_), "upload");
 }
 
 void DeviceFitter::reset_counters() {
