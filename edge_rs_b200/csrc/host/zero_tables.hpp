@@ -179,12 +179,17 @@ inline bool build_tables(const double* design, const double* log_offset, const u
                          int n_coef, Tables* out, int threads = 0) {
   const size_t n_cells = static_cast<size_t>(fid[n_subjects]);
   // A cell can sit in a tabled group only if its value in every column occurs
-  // at least kMinGroupCells times; counting the values of each column bounds
-  // the tabled cells from above, and a continuous column ends the build here
-  // without grouping the rows.
+  // at least kMinGroupCells times; counting the values of the columns that
+  // vary within some subject bounds the tabled cells from above, and a
+  // continuous column ends the build here without grouping the rows.
   {
     std::vector<uint64_t> bits(n_cells);
     for (int j = 0; j < n_coef; ++j) {
+      bool varies = false;
+      for (int s = 0; s < n_subjects && !varies; ++s)
+        for (uint64_t r = fid[s] + 1; r < fid[s + 1] && !varies; ++r)
+          varies = std::memcmp(&design[r * n_coef + j], &design[fid[s] * n_coef + j], sizeof(double)) != 0;
+      if (!varies) continue;
       for (size_t r = 0; r < n_cells; ++r) std::memcpy(&bits[r], &design[r * n_coef + j], sizeof(double));
       std::sort(bits.begin(), bits.end());
       size_t coverable = 0;
