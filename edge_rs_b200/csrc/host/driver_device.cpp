@@ -243,9 +243,6 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
                     lpos.size() * sizeof(uint64_t);
     }
   }
-  // cells a sweep of an average gene visits: the dense part (every cell, or
-  // the loose ones under zero-count tables) and the positive entries
-  sweep_cells_ = dense_cells_ + (G ? nnz / G : 0);
   data_.n_cells = static_cast<int32_t>(sh.n_cells);
   data_.n_subjects = K;
   data_.n_coef = sh.n_coef;
@@ -473,14 +470,16 @@ int DeviceFitter::cluster_for(size_t requests) const {
   // Spread each fit over more CTAs while (a) the fits in flight times the
   // cluster stay within about four times the resident CTA slots, so the
   // searches that finish last still find the SMs busy, and (b) each CTA keeps
-  // at least ~40,000 cell visits per sweep (the dense cells, only the loose
-  // ones under zero-count tables, plus a gene's positive entries), so a
-  // sweep's fixed costs (the cluster barrier, the combine, the Newton step
-  // every CTA repeats) stay small.
+  // at least ~40,000 cells per sweep, so a sweep's fixed costs (the cluster
+  // barrier, the combine, the Newton step every CTA repeats) stay small. The
+  // count is the design's cells even under zero-count tables, whose sweeps
+  // visit far fewer: their steps are bound by the chains of evaluations, and
+  // a fit spread wider ends sooner (500 genes x 100,000 cells, categorical:
+  // 77 ms a step at 4 CTAs per fit, 92 at 2, 119 at 1).
   int cluster = 1;
   while (cluster < device::kMaxCluster && queue_clusters_[cluster * 2] > 0 &&
          requests * static_cast<size_t>(cluster) * 2 <= 4 * static_cast<size_t>(grid_) &&
-         sweep_cells_ >= static_cast<size_t>(cluster) * 2 * 40000)
+         n_cells_ >= static_cast<size_t>(cluster) * 2 * 40000)
     cluster *= 2;
   return cluster;
 }

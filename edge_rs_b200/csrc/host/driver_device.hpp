@@ -138,7 +138,6 @@ class DeviceFitter {
   std::vector<uint64_t> gene_nnz_;
   size_t n_cells_ = 0;
   size_t dense_cells_ = 0;  // cells a sweep's dense part visits
-  size_t sweep_cells_ = 0;  // dense cells plus an average gene's positive entries
   device::GeneData data_{};
   device::FitControl ctl_{};
   std::vector<void*> pooled_;
