@@ -182,28 +182,6 @@ inline constexpr NbTableData kNbTables = {
 #include "nbmath_tables.inc"
 };
 
-// exp(r) - 1 for |r| <= ln2/512: r + r^2 (1/2 + r/6 + r^2 (1/24 + r/120)),
-// the inner polynomial by Estrin's scheme (pairs of terms side by side, then
-// combined with r^2), three dependent steps instead of four.
-NB_HD double exp_poly(double r) {
-  const double r2 = r * r;
-  const double a = nb_fma(r, 1.0 / 6.0, 0.5);
-  const double b = nb_fma(r, 1.0 / 120.0, 1.0 / 24.0);
-  return nb_fma(r2, nb_fma(r2, b, a), r);
-}
-
-// log1p(r) for |r| <= 2^-8: r + r^2 (-1/2 + r/3 - r^2/4 + r^3/5 - r^4/6 +
-// r^5/7), the inner polynomial by Estrin's scheme (three pairs, combined with
-// r^2 and r^4), four dependent steps instead of six.
-NB_HD double log1p_poly(double r) {
-  const double r2 = r * r;
-  const double r4 = r2 * r2;
-  const double a = nb_fma(r, 1.0 / 3.0, -0.5);
-  const double b = nb_fma(r, 0.2, -0.25);
-  const double c = nb_fma(r, 1.0 / 7.0, -1.0 / 6.0);
-  return nb_fma(r2, nb_fma(r4, c, nb_fma(r2, b, a)), r);
-}
-
 NB_HD double nb_exp_tab(double x, const NbTableData* t) {
   const double inv_l = 0x1.71547652b82fep+8;    // 256 / ln 2
   const double l_hi = 0x1.62e42fef80000p-9;     // ln 2 / 256, 34 bits
@@ -213,11 +191,14 @@ NB_HD double nb_exp_tab(double x, const NbTableData* t) {
     // the special cases left out. n = rint(x * inv_l) is read from the
     // shifter's low word instead of a conversion, (n - n mod 256) / 256 is an
     // arithmetic shift, and 2^m stays normal (|m| <= 1020).
-    const double shifted = nb_fma(x, inv_l, 6755399441055744.0);  // 1.5 * 2^52
+    const double shifted = x * inv_l + 6755399441055744.0;  // 1.5 * 2^52
     const double n = shifted - 6755399441055744.0;
     double r = nb_fma(-n, l_hi, x);
     r = nb_fma(-n, l_lo, r);
-    const double q = exp_poly(r);
+    double p = nb_fma(r, 1.0 / 120.0, 1.0 / 24.0);
+    p = nb_fma(p, r, 1.0 / 6.0);
+    p = nb_fma(p, r, 0.5);
+    const double q = nb_fma(r * r, p, r);
     const int ni = static_cast<int>(static_cast<uint32_t>(nb_bits(shifted)));
     const NbPair s = t->exp2_frac[ni & 255];
     const double er = s.a + nb_fma(s.a, q, s.b);
@@ -226,11 +207,13 @@ NB_HD double nb_exp_tab(double x, const NbTableData* t) {
   if (!(x == x)) return x;                      // NaN
   if (x > 709.782712893384) return 1.0 / 0.0;  // overflow
   if (x < -745.1332191019412) return 0.0;      // underflow
-  // |x| < 746 here, so the shifter rounds x inv_l as in the common range
-  const double n = nb_fma(x, inv_l, 6755399441055744.0) - 6755399441055744.0;
+  const double n = nb_rint(x * inv_l);
   double r = nb_fma(-n, l_hi, x);
   r = nb_fma(-n, l_lo, r);
-  const double q = exp_poly(r);
+  double p = nb_fma(r, 1.0 / 120.0, 1.0 / 24.0);
+  p = nb_fma(p, r, 1.0 / 6.0);
+  p = nb_fma(p, r, 0.5);
+  const double q = nb_fma(r * r, p, r);
   const int ni = static_cast<int>(n);
   const int j = ni & 255;
   const int m = (ni - j) / 256;
@@ -260,7 +243,12 @@ NB_HD double nb_log_tab(double x, const NbTableData* t) {
     }
     const NbPair c = t->log_inv_hi[j];
     const double r = nb_fma(m, c.a, -1.0);
-    const double l1p = log1p_poly(r);
+    double p = nb_fma(r, 1.0 / 7.0, -1.0 / 6.0);
+    p = nb_fma(p, r, 0.2);
+    p = nb_fma(p, r, -0.25);
+    p = nb_fma(p, r, 1.0 / 3.0);
+    p = nb_fma(p, r, -0.5);
+    const double l1p = nb_fma(r * r, p, r);
     const double ed =
         nb_from_bits(0x4338000000000000ULL + static_cast<uint64_t>(static_cast<int64_t>(e))) - 6755399441055744.0;
     const double hi = nb_fma(ed, ln2_hi, c.b);
@@ -288,7 +276,12 @@ NB_HD double nb_log_tab(double x, const NbTableData* t) {
   }
   const NbPair c = t->log_inv_hi[j];
   const double r = nb_fma(m, c.a, -1.0);
-  const double l1p = log1p_poly(r);
+  double p = nb_fma(r, 1.0 / 7.0, -1.0 / 6.0);
+  p = nb_fma(p, r, 0.2);
+  p = nb_fma(p, r, -0.25);
+  p = nb_fma(p, r, 1.0 / 3.0);
+  p = nb_fma(p, r, -0.5);
+  const double l1p = nb_fma(r * r, p, r);
   const double ed = static_cast<double>(e);
   const double hi = nb_fma(ed, ln2_hi, c.b);
   const double lo = nb_fma(ed, ln2_lo, t->log_lo[j]);
