@@ -161,14 +161,29 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
   for (size_t g = 0; g < G; ++g) gene_ptr[g + 1] = gene_ptr[g] + genes[g].cells.size();
   const size_t nnz = gene_ptr[G];
   // the kept genes' entries, concatenated on all host threads straight into
-  // pinned staging (every element is written once)
+  // pinned staging (every element is written once), and the design and
+  // offsets beside them, so that every large copy runs asynchronously
   const size_t nz = std::max<size_t>(nnz, 1);
-  PinnedStage stage(nz * (sizeof(double) + sizeof(uint32_t)));
+  const size_t nd = sh.design.size(), no = sh.log_offset.size();
+  PinnedStage stage((nz + nd + no) * sizeof(double) + nz * sizeof(uint32_t));
   double* const counts_h = reinterpret_cast<double*>(stage.data());
-  uint32_t* const cells_h = reinterpret_cast<uint32_t*>(stage.data() + nz * sizeof(double));
+  double* const design_h = counts_h + nz;
+  double* const offset_h = design_h + nd;
+  uint32_t* const cells_h = reinterpret_cast<uint32_t*>(offset_h + no);
   std::vector<double> totals(G * K);
   std::vector<uint64_t> runs(G * (K + 1));
-  parallel_for(G, 0, [&](size_t g) {
+  // the sweep's fixed cell ranges and, per gene, the first positive entry at
+  // or after each range boundary (absolute positions)
+  constexpr int R = device::kRanges;
+  std::vector<uint32_t> rcells(R + 1);
+  for (int v = 0; v <= R; ++v) rcells[v] = static_cast<uint32_t>(sh.n_cells * static_cast<size_t>(v) / R);
+  std::vector<uint64_t> rpos(G * (R + 1));
+  parallel_for(G + 1, 0, [&](size_t g) {
+    if (g == G) {
+      std::copy(sh.design.begin(), sh.design.end(), design_h);
+      std::copy(sh.log_offset.begin(), sh.log_offset.end(), offset_h);
+      return;
+    }
     const GeneCounts& gc = genes[g];
     std::copy(gc.cells.begin(), gc.cells.end(), cells_h + gene_ptr[g]);
     std::copy(gc.counts.begin(), gc.counts.end(), counts_h + gene_ptr[g]);
@@ -181,6 +196,10 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
                                  [](uint32_t c, uint64_t v) { return c < v; });
       runs[g * (K + 1) + s] = gene_ptr[g] + static_cast<uint64_t>(it - gc.cells.begin());
     }
+    for (int v = 0; v <= R; ++v) {
+      auto it = std::lower_bound(gc.cells.begin(), gc.cells.end(), rcells[v]);
+      rpos[g * (R + 1) + v] = gene_ptr[g] + static_cast<uint64_t>(it - gc.cells.begin());
+    }
   });
   gene_nnz_.resize(G);
   for (size_t g = 0; g < G; ++g) gene_nnz_[g] = genes[g].cells.size();
@@ -190,31 +209,21 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
   std::vector<uint32_t> wcells(device::kWarps + 1);
   for (int w = 0; w <= device::kWarps; ++w)
     wcells[w] = static_cast<uint32_t>(sh.n_cells * static_cast<size_t>(w) / device::kWarps);
-  // the sweep's fixed cell ranges and, per gene, the first positive entry at
-  // or after each range boundary (absolute positions)
-  constexpr int R = device::kRanges;
-  std::vector<uint32_t> rcells(R + 1);
-  for (int v = 0; v <= R; ++v) rcells[v] = static_cast<uint32_t>(sh.n_cells * static_cast<size_t>(v) / R);
-  std::vector<uint64_t> rpos(G * (R + 1));
-  for (size_t g = 0; g < G; ++g) {
-    const GeneCounts& gc = genes[g];
-    for (int v = 0; v <= R; ++v) {
-      auto it = std::lower_bound(gc.cells.begin(), gc.cells.end(), rcells[v]);
-      rpos[g * (R + 1) + v] = gene_ptr[g] + static_cast<uint64_t>(it - gc.cells.begin());
-    }
-  }
 
-  data_.design = device_copy(sh.design.data(), sh.design.size(), stream_, &pooled_);
-  data_.log_offset = device_copy(sh.log_offset.data(), sh.log_offset.size(), stream_, &pooled_);
+  // the small pageable arrays first: a copy from pageable memory returns only
+  // once the stream's earlier copies are done, so issued after the large
+  // pinned ones it would wait for them
   data_.fid = device_copy(fid.data(), fid.size(), stream_, &pooled_);
   data_.gene_ptr = device_copy(gene_ptr.data(), gene_ptr.size(), stream_, &pooled_);
-  data_.cells = device_copy(cells_h, nnz, stream_, &pooled_);
-  data_.counts = device_copy(counts_h, nnz, stream_, &pooled_);
   data_.runs = device_copy(runs.data(), runs.size(), stream_, &pooled_);
   data_.totals = device_copy(totals.data(), totals.size(), stream_, &pooled_);
   data_.warp_cells = device_copy(wcells.data(), wcells.size(), stream_, &pooled_);
   data_.range_cells = device_copy(rcells.data(), rcells.size(), stream_, &pooled_);
   data_.range_pos = device_copy(rpos.data(), rpos.size(), stream_, &pooled_);
+  data_.design = device_copy(design_h, nd, stream_, &pooled_);
+  data_.log_offset = device_copy(offset_h, no, stream_, &pooled_);
+  data_.cells = device_copy(cells_h, nnz, stream_, &pooled_);
+  data_.counts = device_copy(counts_h, nnz, stream_, &pooled_);
   h2d_bytes_ = (sh.design.size() + sh.log_offset.size() + nnz + totals.size()) * sizeof(double) +
                (fid.size() + nnz + wcells.size() + rcells.size()) * sizeof(uint32_t) +
                (gene_ptr.size() + runs.size() + rpos.size()) * sizeof(uint64_t);

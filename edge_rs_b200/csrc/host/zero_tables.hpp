@@ -118,6 +118,30 @@ inline bool fit_panel(const std::vector<std::pair<double, double>>& distinct, do
   return ok;
 }
 
+// Sorts 64-bit keys (least significant 16-bit digit first; a pass whose
+// digit is the same in every key is skipped). The table bound only needs
+// equal keys next to each other; a comparison sort of 100,000 keys took
+// 5 ms of a call.
+inline void radix_sort(std::vector<uint64_t>& keys, std::vector<uint64_t>& tmp) {
+  const size_t n = keys.size();
+  if (n < 2) return;
+  tmp.resize(n);
+  std::vector<size_t> count(size_t{1} << 16);
+  for (int shift = 0; shift < 64; shift += 16) {
+    std::fill(count.begin(), count.end(), 0);
+    for (uint64_t k : keys) ++count[(k >> shift) & 0xffff];
+    if (count[(keys[0] >> shift) & 0xffff] == n) continue;
+    size_t sum = 0;
+    for (size_t& c : count) {
+      const size_t t = c;
+      c = sum;
+      sum += t;
+    }
+    for (uint64_t k : keys) tmp[count[(k >> shift) & 0xffff]++] = k;
+    keys.swap(tmp);
+  }
+}
+
 // One group's sums and panels; its base panels' (first, depth) entries use
 // panel numbers local to the group (0, 1, ...).
 struct Built {
@@ -183,7 +207,7 @@ inline bool build_tables(const double* design, const double* log_offset, const u
   // vary within some subject bounds the tabled cells from above, and a
   // continuous column ends the build here without grouping the rows.
   {
-    std::vector<uint64_t> bits(n_cells);
+    std::vector<uint64_t> bits(n_cells), tmp;
     for (int j = 0; j < n_coef; ++j) {
       bool varies = false;
       for (int s = 0; s < n_subjects && !varies; ++s)
@@ -191,7 +215,7 @@ inline bool build_tables(const double* design, const double* log_offset, const u
           varies = std::memcmp(&design[r * n_coef + j], &design[fid[s] * n_coef + j], sizeof(double)) != 0;
       if (!varies) continue;
       for (size_t r = 0; r < n_cells; ++r) std::memcpy(&bits[r], &design[r * n_coef + j], sizeof(double));
-      std::sort(bits.begin(), bits.end());
+      detail::radix_sort(bits, tmp);
       size_t coverable = 0;
       for (size_t a = 0, b; a < n_cells; a = b) {
         for (b = a + 1; b < n_cells && bits[b] == bits[a];) ++b;
