@@ -60,7 +60,7 @@ struct GeneData {
   const double* counts;      // positive counts
   const uint64_t* runs;      // n_genes x (n_subjects + 1): first positive entry of each subject
   const double* totals;      // n_genes x n_subjects count totals
-  const uint32_t* warp_cells;  // kWarps + 1 boundaries of stage one's warp ranges
+  const uint32_t* warp_cells;  // ptmg_warps + 1 boundaries of stage one's warp ranges
   const uint32_t* range_cells; // kRanges + 1 boundaries of the sweep's cell ranges
   const uint64_t* range_pos;   // n_genes x (kRanges + 1): first positive entry at or after each boundary
   double* warm_state;          // n_genes x 2 x (n_coef + n_subjects), or null

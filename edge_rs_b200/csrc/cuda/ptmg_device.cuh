@@ -18,6 +18,17 @@ struct alignas(16) PtmgRequest {
   double beta[kMaxCoef];
 };
 
+// Warps of a stage-one CTA, and so the ranges of its summation tree (the
+// cells cut into this many equal contiguous ranges, warp_cells): 16 (one
+// 512-thread CTA per SM) for designs of at most 4 columns with at most one
+// varying within subjects, whose per-thread state fits in 128 registers;
+// otherwise 8 (256 threads), where a thread needs up to 224. An SM holds 16
+// or 8 warps either way, but with 16 in one CTA each request is served by
+// twice the warps, so a gene's chain of Newton points runs about twice as
+// fast; stage one is bound by its longest chain.
+constexpr int ptmg_warps(int n_coef, int n_varying) { return n_coef <= 4 && n_varying <= 1 ? 16 : 8; }
+constexpr int kMaxPtmgWarps = 16;
+
 // Per request the kernel writes (2 + ptmg_width_of(n_coef)) * n_subjects
 // doubles: cumsumxtb (K), ylin (K), then K rows of the pass-two sums.
 int ptmg_width_of(int n_coef);

@@ -63,7 +63,7 @@ struct RDims {
   static constexpr int W = kBq + T;
 };
 
-constexpr int ptmg_min_blocks(int nb, int nv) { return nb <= 4 && nv <= 1 ? 2 : 1; }
+constexpr int ptmg_threads(int nb, int nv) { return ptmg_warps(nb, nv) * 32; }
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -191,14 +191,14 @@ struct PtmgCta {
   double* p1;        // K x 2: cumsumxtb, ylin
   double* cs;        // K: the constant columns' share of eta for this request
   uint32_t* fid;     // K + 1
-  uint32_t* wcells;  // kWarps + 1
+  uint32_t* wcells;  // ptmg_warps + 1
   int32_t* vpos;     // kMaxCoef: each column's index among the varying ones, or -1
   double* slots;     // this CTA's scratch: warp and subject pieces
   double* reduced;   // this CTA's scratch: K reduced pass-two rows
 };
 
 // One pass through the tree: dense pieces into slots[(s + warp) * stride],
-// sparse pieces into slots[(K + kWarps + s) * stride], then per subject
+// sparse pieces into slots[(K + W + s) * stride] (W = ptmg_warps), then per subject
 // out[s * out_stride + v] = 0 + dense pieces (warp order) + sparse piece.
 // Lanes take two cells (r, r + 32) or entries per iteration; each lane's
 // partials still take them in its sequential order.
@@ -206,6 +206,7 @@ template <int NB, int NV, int PASS, int N>
 __device__ void tree_pass(const GeneData& d, const PtmgCta& c, int gene, const double* beta, double gamma,
                           const int* vc, int stride, double* out, int out_stride) {
   const int K = d.n_subjects;
+  constexpr int W = ptmg_warps(NB, NV);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   constexpr int NX = NV > 0 ? NV : 1;
   const int c_begin = static_cast<int>(c.wcells[warp]), c_end = static_cast<int>(c.wcells[warp + 1]);
@@ -239,7 +240,7 @@ __device__ void tree_pass(const GeneData& d, const PtmgCta& c, int gene, const d
     }
   }
   const uint64_t* runs = d.runs + static_cast<size_t>(gene) * (K + 1);
-  for (int s = warp; s < K; s += kWarps) {
+  for (int s = warp; s < K; s += W) {
     const uint64_t p0 = runs[s], p1 = runs[s + 1];
     double acc[N];
 #pragma unroll
@@ -264,7 +265,7 @@ __device__ void tree_pass(const GeneData& d, const PtmgCta& c, int gene, const d
         if (has_b) sparse_two<NV>(acc, xb, nb_exp(eta_b), yb, yms, gamma);
       }
     }
-    reduce_to<N>(acc, c.slots + (K + kWarps + s) * stride, lane);
+    reduce_to<N>(acc, c.slots + (K + W + s) * stride, lane);
   }
   __syncthreads();
   for (int idx = threadIdx.x; idx < K * N; idx += blockDim.x) {
@@ -272,9 +273,9 @@ __device__ void tree_pass(const GeneData& d, const PtmgCta& c, int gene, const d
     const uint32_t a0 = c.fid[s], a1 = c.fid[s + 1];
     double total = 0.0;
 #pragma unroll
-    for (int w = 0; w < kWarps; ++w)
+    for (int w = 0; w < W; ++w)
       if (c.wcells[w] < a1 && c.wcells[w + 1] > a0) total += c.slots[(s + w) * stride + v];
-    total += c.slots[(K + kWarps + s) * stride + v];
+    total += c.slots[(K + W + s) * stride + v];
     out[s * out_stride + v] = total;
   }
   __syncthreads();
@@ -309,24 +310,25 @@ __device__ __forceinline__ double expand_two(const double* R, const double* X, c
 template <int NB, int NV>
 __device__ PtmgCta ptmg_setup(const GeneData& d, double* smem, double* scratch) {
   const int K = d.n_subjects;
+  constexpr int W = ptmg_warps(NB, NV);
   PtmgCta c;
   c.ym = smem;
   c.p1 = c.ym + K;
   c.cs = c.p1 + 2 * K;
   c.fid = reinterpret_cast<uint32_t*>(c.cs + K);
   c.wcells = c.fid + K + 1;
-  c.vpos = reinterpret_cast<int32_t*>(c.wcells + kWarps + 1);
+  c.vpos = reinterpret_cast<int32_t*>(c.wcells + W + 1);
   for (int i = threadIdx.x; i <= K; i += blockDim.x) c.fid[i] = d.fid[i];
-  if (threadIdx.x <= kWarps) c.wcells[threadIdx.x] = d.warp_cells[threadIdx.x];
+  if (threadIdx.x <= W) c.wcells[threadIdx.x] = d.warp_cells[threadIdx.x];
   if (threadIdx.x < NB) {
     int pos = -1;
     for (int j = 0; j < NV; ++j)
       if (d.varying[j] == static_cast<int>(threadIdx.x)) pos = j;
     c.vpos[threadIdx.x] = pos;
   }
-  const size_t per_cta = static_cast<size_t>(2 * K + kWarps) * RDims<NV>::W + static_cast<size_t>(K) * RDims<NV>::W;
+  const size_t per_cta = static_cast<size_t>(2 * K + W) * RDims<NV>::W + static_cast<size_t>(K) * RDims<NV>::W;
   c.slots = scratch + static_cast<size_t>(blockIdx.x) * per_cta;
-  c.reduced = c.slots + static_cast<size_t>(2 * K + kWarps) * RDims<NV>::W;
+  c.reduced = c.slots + static_cast<size_t>(2 * K + W) * RDims<NV>::W;
   return c;
 }
 
@@ -389,7 +391,7 @@ __device__ __forceinline__ long long global_ns() {
 // Streaming mode: one persistent launch for stage one, the request-ring
 // protocol of FitQueue (pml_device.cuh) with one CTA per request.
 template <int NB, int NV>
-__global__ void __launch_bounds__(kThreads, ptmg_min_blocks(NB, NV))
+__global__ void __launch_bounds__(ptmg_threads(NB, NV), 1)
     ptmg_queue_kernel(GeneData d, PtmgQueue qu, double* scratch) {
   extern __shared__ __align__(16) double smem[];
   const PtmgCta c = ptmg_setup<NB, NV>(d, smem, scratch);
@@ -438,7 +440,7 @@ __global__ void __launch_bounds__(kThreads, ptmg_min_blocks(NB, NV))
 }
 
 inline size_t smem_bytes(int K) {
-  return static_cast<size_t>(4 * K) * 8 + (K + 1 + kWarps + 1 + kMaxCoef) * 4 + 16;
+  return static_cast<size_t>(4 * K) * 8 + (K + 1 + kMaxPtmgWarps + 1 + kMaxCoef) * 4 + 16;
 }
 
 template <int NB, int NV>
@@ -447,7 +449,7 @@ int launch_queue_nb(const GeneData& d, const PtmgQueue& qu, double* scratch, int
   cudaError_t e = cudaFuncSetAttribute(ptmg_queue_kernel<NB, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;
-  ptmg_queue_kernel<NB, NV><<<grid, kThreads, smem, stream>>>(d, qu, scratch);
+  ptmg_queue_kernel<NB, NV><<<grid, ptmg_threads(NB, NV), smem, stream>>>(d, qu, scratch);
   return cudaGetLastError();
 }
 
@@ -458,7 +460,7 @@ int blocks_nb(int K) {
                            static_cast<int>(smem)) != cudaSuccess)
     return 0;
   int blocks = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, ptmg_queue_kernel<NB, NV>, kThreads, smem) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, ptmg_queue_kernel<NB, NV>, ptmg_threads(NB, NV), smem) !=
       cudaSuccess)
     return 0;
   return blocks;
@@ -466,7 +468,7 @@ int blocks_nb(int K) {
 
 template <int NB, int NV>
 size_t scratch_nb(int K) {
-  return static_cast<size_t>(3 * K + kWarps) * RDims<NV>::W;
+  return static_cast<size_t>(3 * K + ptmg_warps(NB, NV)) * RDims<NV>::W;
 }
 
 template <int NB, int NV = 0>

@@ -206,9 +206,11 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
   n_cells_ = sh.n_cells;
   dense_cells_ = sh.n_cells;
   std::vector<uint32_t> fid(sh.fid.begin(), sh.fid.end());
-  std::vector<uint32_t> wcells(device::kWarps + 1);
-  for (int w = 0; w <= device::kWarps; ++w)
-    wcells[w] = static_cast<uint32_t>(sh.n_cells * static_cast<size_t>(w) / device::kWarps);
+  data_.n_varying = device::varying_columns(sh.design.data(), sh.n_coef, sh.fid.data(), K, data_.varying);
+  // stage one's warp ranges, as many as its CTA has warps
+  const int pw = device::ptmg_warps(sh.n_coef, data_.n_varying);
+  std::vector<uint32_t> wcells(static_cast<size_t>(pw) + 1);
+  for (int w = 0; w <= pw; ++w) wcells[w] = static_cast<uint32_t>(sh.n_cells * static_cast<size_t>(w) / pw);
 
   // the small pageable arrays first: a copy from pageable memory returns only
   // once the stream's earlier copies are done, so issued after the large
@@ -255,7 +257,6 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
   data_.n_cells = static_cast<int32_t>(sh.n_cells);
   data_.n_subjects = K;
   data_.n_coef = sh.n_coef;
-  data_.n_varying = device::varying_columns(sh.design.data(), sh.n_coef, sh.fid.data(), K, data_.varying);
   {
     // per gene two (beta, log_w) slots for warm inner starts
     const size_t doubles = std::max<size_t>(G, 1) * 2 * static_cast<size_t>(sh.n_coef + K);

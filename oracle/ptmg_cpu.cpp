@@ -34,6 +34,7 @@ nebula::PtmgSums ptmg_sums(const PmlData& d, const double* beta, double alpha, d
   const int nv = static_cast<int>(sp.varying.size()), tv = nv * (nv + 1) / 2;
   const int rE = 9, rEq = 10, rXf = 11, rD41 = rXf + nv, rT1 = rD41 + nv, rT2 = rT1 + nv, rQv = rT2 + nv;
   const int rBp = rQv + nv, rBq = rBp + tv, RW = rBq + tv;
+  const int warps = stage_one_warps(nb, nv);  // the kernel's warp ranges
   std::vector<double> cs(k), bv(nv);
   for (int j = 0; j < nv; ++j) bv[j] = beta[sp.varying[j]];
   for (int s = 0; s < k; ++s) {  // the constant columns' share of eta, in column order
@@ -60,7 +61,7 @@ nebula::PtmgSums ptmg_sums(const PmlData& d, const double* beta, double alpha, d
     double x[8];
     acc[1] = nb_fma(eta_at(d.cells[i], s, x), d.counts[i], acc[1]);
   };
-  std::vector<double> p1 = tree_sums(d, run, 2, dense1, sparse1);
+  std::vector<double> p1 = tree_sums(d, run, 2, warps, dense1, sparse1);
   out.cumsumxtb.resize(k);
   out.ylin.resize(k);
   std::vector<double> ym(k);
@@ -143,7 +144,7 @@ nebula::PtmgSums ptmg_sums(const PmlData& d, const double* beta, double alpha, d
       }
     }
   };
-  const std::vector<double> red = tree_sums(d, run, RW, dense2, sparse2);
+  const std::vector<double> red = tree_sums(d, run, RW, warps, dense2, sparse2);
   // every subject's full row: a constant column's sums are its value times a
   // scalar sum (sum x_a e = x_a sum e, sum x_a gg e = x_a acc[6], ...)
   out.sums.assign(static_cast<size_t>(k) * W, 0.0);

@@ -13,14 +13,19 @@ namespace oracle {
 
 // The summation tree of stage one's per-subject sums, so that the oracle and
 // the CUDA kernel agree bit for bit. Dense part: the cells
-// are cut into kWarps equal contiguous ranges; within a range each subject
+// are cut into `warps` equal contiguous ranges, as many as the kernel's CTA has
+// warps (stage_one_warps); within a range each subject
 // piece is summed by kLanes strided partial sums (lane l takes cells
 // c0 + l, c0 + l + kLanes, ...), which are then combined by the butterfly
 // v[l] += v[l ^ off] for off = 16, 8, 4, 2, 1 (lane 0's value is kept).
 // Sparse part: each subject's positive entries the same way. A subject's total
 // is 0 + its dense pieces in range order + its sparse piece.
-constexpr int kWarps = 8;
 constexpr int kLanes = 32;
+
+// Warps of the stage-one kernel's CTA (ptmg_warps, ptmg_device.cuh): 16 for
+// designs of at most 4 columns with at most one varying within subjects,
+// else 8.
+inline int stage_one_warps(int n_beta, int n_varying) { return n_beta <= 4 && n_varying <= 1 ? 16 : 8; }
 
 struct Tree {
   int nv;
@@ -42,7 +47,9 @@ struct Tree {
   }
 };
 
-inline size_t warp_start(const PmlData& d, int w) { return d.n_cells * static_cast<size_t>(w) / kWarps; }
+inline size_t warp_start(const PmlData& d, int w, int warps) {
+  return d.n_cells * static_cast<size_t>(w) / static_cast<size_t>(warps);
+}
 
 inline int subject_of(const PmlData& d, size_t c) {
   int s = 0;
@@ -54,13 +61,13 @@ inline int subject_of(const PmlData& d, size_t c) {
 // over every positive entry (sparse) through the tree; returns per-subject
 // totals, K x nv.
 template <typename Dense, typename Sparse>
-std::vector<double> tree_sums(const PmlData& d, const std::vector<size_t>& run, int nv, Dense cell,
+std::vector<double> tree_sums(const PmlData& d, const std::vector<size_t>& run, int nv, int warps, Dense cell,
                               Sparse pos) {
   const int k = d.k;
-  std::vector<double> dense(static_cast<size_t>(k + kWarps) * nv, 0.0), sparse(static_cast<size_t>(k) * nv, 0.0);
+  std::vector<double> dense(static_cast<size_t>(k + warps) * nv, 0.0), sparse(static_cast<size_t>(k) * nv, 0.0);
   Tree tree(nv);
-  for (int w = 0; w < kWarps; ++w) {
-    const size_t c_begin = warp_start(d, w), c_end = warp_start(d, w + 1);
+  for (int w = 0; w < warps; ++w) {
+    const size_t c_begin = warp_start(d, w, warps), c_end = warp_start(d, w + 1, warps);
     if (c_begin >= c_end) continue;
     int s = subject_of(d, c_begin);
     for (size_t c0 = c_begin; c0 < c_end; ++s) {
@@ -82,8 +89,8 @@ std::vector<double> tree_sums(const PmlData& d, const std::vector<size_t>& run, 
   for (int s = 0; s < k; ++s) {
     for (int v = 0; v < nv; ++v) {
       double t = 0.0;
-      for (int w = 0; w < kWarps; ++w)
-        if (warp_start(d, w) < d.subject_start[s + 1] && warp_start(d, w + 1) > d.subject_start[s])
+      for (int w = 0; w < warps; ++w)
+        if (warp_start(d, w, warps) < d.subject_start[s + 1] && warp_start(d, w + 1, warps) > d.subject_start[s])
           t += dense[static_cast<size_t>(s + w) * nv + v];
       t += sparse[static_cast<size_t>(s) * nv + v];
       total[static_cast<size_t>(s) * nv + v] = t;
