@@ -14,16 +14,19 @@
 // zero plus what the positive counts add (every per-cell term is affine in
 // the count), and the reference's three x x' e blocks enter the Hessian only
 // as bp ymm_d - bg ym + bgte ym^2 per subject, so the cell pass sums
-// x x' e and x x' e ym (ym g e/w - g) directly. Every design, categorical or
-// not, takes the exact-Hessian projected Newton (the reference switches
-// tabled designs to L-BFGS-B, nebula.rs:1141-1169); a Newton search that
-// fails keeps its start, as descend_marginal does when L-BFGS-B fails too.
+// x x' e and x x' e ym (ym g e/w - g) directly. A descent is the reference's:
+// the exact-Hessian projected Newton on a dense run, L-BFGS-B (lbfgsb.hpp)
+// where the run is tabled or the Newton stalls or does not improve, and the
+// start kept when that fails too (nebula.rs:1132-1170). Its value and
+// gradient come from the dense sums even on a tabled run, where the
+// reference reads its zero-count tables; the two agree to rounding.
 #include "stage_one.hpp"
 
 #include <algorithm>
 #include <cmath>
 #include <limits>
 
+#include "lbfgsb.hpp"
 #include "special.hpp"
 
 namespace nebula {
@@ -42,6 +45,8 @@ constexpr int kMaxHalvings = 40;               // nebula.rs:140
 constexpr double kShift = 1e-8;                // nebula.rs:145
 constexpr int kRestarts = 3;                   // nebula.rs:153
 constexpr double kRestartGain = 1e-6;          // nebula.rs:161
+constexpr int kLbfgsbMaxIter = 300;            // nebula.rs:164
+constexpr int kLbfgsbMaxLineSearch = 40;       // nebula.rs:167
 constexpr int kUnrolled = 8;                   // pml.rs:1165
 
 struct GammaTerms {
@@ -350,9 +355,9 @@ bool cholesky_solve(const std::vector<double>& a, int n, const std::vector<doubl
 // minimise_marginal as a coroutine (nebula.rs:1075-1325)
 
 MarginalSearch::MarginalSearch(std::vector<double> start, std::vector<double> lower, std::vector<double> upper,
-                               int nb)
+                               int nb, bool tabled)
     : start_(std::move(start)), lower_(std::move(lower)), upper_(std::move(upper)),
-      n_(static_cast<int>(start_.size())), nb_(nb) {
+      n_(static_cast<int>(start_.size())), nb_(nb), tabled_(tabled) {
   g_.assign(n_, 0.0);
   h_.assign(static_cast<size_t>(n_) * n_, 0.0);
   task_ = run();
@@ -401,14 +406,17 @@ MarginalSearch::Task MarginalSearch::run() {
       xs = x1;
       fs = f_;
     }
-    // descend_marginal: projected Newton from (xs, fs) (nebula.rs:1132-1170, 1225-1325)
-    int status = 0;  // 0 running, 1 converged, 2 stalled
-    x = xs;
-    co_await evaluate(x);
-    f = f_;
-    g = g_;
-    h = h_;
-    if (!all_finite(f, g, h)) status = 2;
+    // descend_marginal (nebula.rs:1132-1170): projected Newton from (xs, fs)
+    // on a dense run (1225-1325), L-BFGS-B where that is not taken or fails
+    int status = tabled_ ? 2 : 0;  // 0 running, 1 converged, 2 stalled or not run
+    if (!tabled_) {
+      x = xs;
+      co_await evaluate(x);
+      f = f_;
+      g = g_;
+      h = h_;
+      if (!all_finite(f, g, h)) status = 2;
+    }
     for (int it = 0; status == 0 && it < kNewtonMaxIter; ++it) {
       double projected = 0.0;
       for (int i = 0; i < n; ++i)
@@ -490,6 +498,25 @@ MarginalSearch::Task MarginalSearch::run() {
     if (status == 1 && f < fs) {
       xd = x;
       fd = f;
+    } else {
+      // the quasi-Newton, its ftol relative to the start's objective so that
+      // its stop is nebula's absolute eps (nebula.rs:1146-1168)
+      LbfgsbParams lp;
+      lp.ftol = kFtolAbs / std::fmax(std::fabs(fs), 1.0);
+      lp.pgtol = kPgtol;
+      lp.max_iter = kLbfgsbMaxIter;
+      lp.max_line_search = kLbfgsbMaxLineSearch;
+      Lbfgsb quasi(xs, lower_, upper_, lp);
+      std::vector<double> xq(n);
+      while (const double* q = quasi.ask()) {
+        xq.assign(q, q + n);
+        co_await evaluate(xq);
+        quasi.tell(f_, g_.data());
+      }
+      if (quasi.f() < fs) {
+        xd = quasi.x();
+        fd = quasi.f();
+      }
     }
     if (attempt == 0) {
       best = xd;

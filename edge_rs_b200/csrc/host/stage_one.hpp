@@ -1,7 +1,8 @@
 // Stage one: the Poisson-gamma marginal likelihood over [beta, sigma, phi]
-// (src/sc/ptmg.rs) and its projected-Newton minimiser (src/sc/nebula.rs
-// minimise_marginal 1075-1112, newton_marginal 1225-1325), then the plan for
-// stage two (plan_gene 812-901).
+// (src/sc/ptmg.rs) and its minimiser, the projected Newton with L-BFGS-B
+// behind it (src/sc/nebula.rs minimise_marginal 1075-1112, descend_marginal
+// 1132-1170, newton_marginal 1225-1325), then the plan for stage two
+// (plan_gene 812-901).
 //
 // An evaluation is split in two: per-subject sums over the cells (on the
 // device for the product, on the CPU for the oracle, both with the same
@@ -58,10 +59,14 @@ double ptmg_assemble(const MarginalGene& g, const double* params, const PtmgSums
 
 // Reverse-communication minimise_marginal: ask() gives the point to evaluate
 // (null when done), tell() its value, gradient and Hessian (any may be
-// non-finite).
+// non-finite). `tabled`: the run has zero-count tables (the reference's
+// `zeros` is Some), so every descent is the quasi-Newton L-BFGS-B; otherwise
+// the projected Newton runs first and L-BFGS-B takes over where it fails or
+// does not improve (descend_marginal, nebula.rs:1132-1170).
 class MarginalSearch {
  public:
-  MarginalSearch(std::vector<double> start, std::vector<double> lower, std::vector<double> upper, int nb);
+  MarginalSearch(std::vector<double> start, std::vector<double> lower, std::vector<double> upper, int nb,
+                 bool tabled = false);
   ~MarginalSearch();
   MarginalSearch(const MarginalSearch&) = delete;
   MarginalSearch& operator=(const MarginalSearch&) = delete;
@@ -95,6 +100,7 @@ class MarginalSearch {
 
   std::vector<double> start_, lower_, upper_;
   int n_, nb_;
+  bool tabled_;
   std::vector<double> x_;
   double f_ = 0.0;
   std::vector<double> g_, h_;

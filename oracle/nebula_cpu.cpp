@@ -43,7 +43,7 @@ GeneOutcome fit_gene_cpu(const Shared& sh, const CsrView& csr, const std::vector
   const double* tot = &totals[g * k];
   GeneCounts gc = positive_indices(csr, g);
   int marginal_evaluations = 0;
-  GenePlan plan = oracle::plan_gene(sh, gc, tot, &marginal_evaluations);
+  GenePlan plan = oracle::plan_gene(sh, gc, tot, &marginal_evaluations, zeros != nullptr);
   oracle::PmlData data = pml_view(sh, gc, tot, zeros);
   std::optional<std::optional<std::pair<std::vector<double>, bool>>> refit;
   if (plan.refit != Refit::None) {

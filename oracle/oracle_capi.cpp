@@ -1,7 +1,10 @@
 // ORACLE — test infrastructure only. C-ABI the tests and the CPU-baseline leg
 // of bench.py load with ctypes. Never linked by the product library.
 #include <cstdint>
+#include <vector>
 
+#include "common.hpp"
+#include "lbfgsb.hpp"
 #include "nbmath.hpp"
 #include "pml_cpu.hpp"
 
@@ -108,4 +111,55 @@ ORACLE_API int32_t oracle_zero_groups(const double* design, const double* log_of
   for (size_t i = 0; i < t.loose.size(); ++i) loose_out[i] = t.loose[i];
   *n_loose = t.loose.size();
   return static_cast<int32_t>(t.groups.size());
+}
+
+// The stage-one quasi-Newton (lbfgsb.hpp) on an objective the caller
+// evaluates: fg(x, n, grad_out, ctx) returns the value at x and writes the
+// gradient. x_out (n) and *f_out receive the result, ints_out its status
+// (LbfgsbStatus), iterations and evaluations. Returns 0, or the NB_ERR_* code
+// of a rejected argument (its message into err).
+typedef double (*oracle_fg)(const double* x, uint32_t n, double* grad, void* ctx);
+ORACLE_API int32_t oracle_lbfgsb(oracle_fg fg, void* ctx, const double* x0, uint32_t n, const double* lower,
+                                 uint32_t n_lower, const double* upper, uint32_t n_upper, int32_t memory,
+                                 double ftol, double pgtol, int32_t max_iter, int32_t max_line_search,
+                                 double* x_out, double* f_out, int32_t* ints_out, char* err, uint64_t err_len) {
+  try {
+    nebula::LbfgsbParams p;
+    p.memory = memory;
+    p.ftol = ftol;
+    p.pgtol = pgtol;
+    p.max_iter = max_iter;
+    p.max_line_search = max_line_search;
+    nebula::Lbfgsb search(std::vector<double>(x0, x0 + n), std::vector<double>(lower, lower + n_lower),
+                          std::vector<double>(upper, upper + n_upper), p);
+    std::vector<double> g(n);
+    while (const double* x = search.ask()) {
+      const double f = fg(x, n, g.data(), ctx);
+      search.tell(f, g.data());
+    }
+    for (uint32_t i = 0; i < n; ++i) x_out[i] = search.x()[i];
+    *f_out = search.f();
+    ints_out[0] = static_cast<int32_t>(search.status());
+    ints_out[1] = search.iterations();
+    ints_out[2] = search.evaluations();
+    return 0;
+  } catch (const nebula::NbError& e) {
+    if (err && err_len) {
+      const size_t m = std::min<size_t>(err_len - 1, e.message.size());
+      for (size_t i = 0; i < m; ++i) err[i] = e.message[i];
+      err[m] = 0;
+    }
+    return e.code;
+  }
+}
+
+// solve_dense of the quasi-Newton (lbfgsb.rs:317-361); returns 0, or 1 when a
+// pivot underflows.
+ORACLE_API int32_t oracle_lbfgsb_solve_dense(const double* a, const double* b, uint32_t dim, double* x_out) {
+  std::vector<double> x;
+  if (!nebula::lbfgsb_solve_dense(std::vector<double>(a, a + dim * dim), std::vector<double>(b, b + dim),
+                                  static_cast<int>(dim), &x))
+    return 1;
+  for (uint32_t i = 0; i < dim; ++i) x_out[i] = x[i];
+  return 0;
 }

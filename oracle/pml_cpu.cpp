@@ -168,7 +168,7 @@ void sweep(const PmlData& d, const std::vector<double>& beta, const std::vector<
   std::vector<double> cs, csl;
   constant_shares(d, sp, beta, log_w, &cs, &csl);
   auto dense = [&](double* acc, size_t r, int s) {
-    double x[8];
+    double x[kMaxRow];
     varying_row(d, sp, r, x);
     double e = nebula::nb_exp_tab(varying_eta(sp, x, beta, d.offset[r] + csl[s]), &nebula::kNbTables);
     double t = e + gamma;
@@ -180,7 +180,7 @@ void sweep(const PmlData& d, const std::vector<double>& beta, const std::vector<
   auto sparse = [&](double* acc, size_t i, int s) {
     size_t c = d.cells[i];
     double y = d.counts[i];
-    double x[8];
+    double x[kMaxRow];
     varying_row(d, sp, c, x);
     double eta = varying_eta(sp, x, beta, d.offset[c] + cs[s]);
     double e = nebula::nb_exp_tab(eta + log_w[s], &nebula::kNbTables);
@@ -200,7 +200,7 @@ void sweep(const PmlData& d, const std::vector<double>& beta, const std::vector<
       double* R = &red[static_cast<size_t>(s) * nsr];
       for (uint32_t g = d.zeros->subject_groups[s]; g < d.zeros->subject_groups[s + 1]; ++g) {
         const nebula::zero::Group& G = d.zeros->groups[g];
-        double x[8];
+        double x[kMaxRow];
         varying_row(d, sp, static_cast<size_t>(G.row), x);
         const double log_tau = varying_eta(sp, x, beta, csl[s] - ln_gamma);
         double f[3];
@@ -366,12 +366,12 @@ double laplace_correction(const PmlData& d, const std::vector<double>& beta, con
   std::vector<double> cs, csl;
   constant_shares(d, sp, beta, log_w, &cs, &csl);
   auto dense = [&](double* acc, size_t r, int s) {
-    double x[8];
+    double x[kMaxRow];
     varying_row(d, sp, r, x);
     terms(nebula::nb_exp_tab(varying_eta(sp, x, beta, d.offset[r] + csl[s]), &nebula::kNbTables), gamma, acc);
   };
   auto sparse = [&](double* acc, size_t i, int s) {
-    double x[8];
+    double x[kMaxRow];
     varying_row(d, sp, d.cells[i], x);
     const double eta = varying_eta(sp, x, beta, d.offset[d.cells[i]] + cs[s]);
     terms(nebula::nb_exp_tab(eta + log_w[s], &nebula::kNbTables), d.counts[i], acc);
@@ -383,7 +383,7 @@ double laplace_correction(const PmlData& d, const std::vector<double>& beta, con
     for (int s = 0; s < d.k; ++s) {
       for (uint32_t g = d.zeros->subject_groups[s]; g < d.zeros->subject_groups[s + 1]; ++g) {
         const nebula::zero::Group& G = d.zeros->groups[g];
-        double x[8];
+        double x[kMaxRow];
         varying_row(d, sp, static_cast<size_t>(G.row), x);
         const double log_tau = varying_eta(sp, x, beta, csl[s] - ln_gamma);
         double f[4];
@@ -483,6 +483,7 @@ bool opt_pml(const PmlData& d, const double* beta_init, const double* log_w_init
     pen.alpha = subject;
   }
   if (!(std::isfinite(gamma) && gamma > 0.0)) return false;
+  if (d.n_beta < 1 || d.n_beta > kMaxRow) return false;
   const int nb = d.n_beta, k = d.k;
   std::vector<double> beta(beta_init, beta_init + nb);
   std::vector<double> log_w(k, 0.0);

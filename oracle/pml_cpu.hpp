@@ -17,6 +17,10 @@
 
 namespace oracle {
 
+// Widest design the oracle's per-cell row buffers hold (the reference's CPU
+// path has no width cap; its e2e sets reach 13 columns).
+constexpr int kMaxRow = 64;
+
 // One gene in the layout of PmlData (pml.rs:122-136).
 struct PmlData {
   const double* design;  // row-major n_cells x n_beta

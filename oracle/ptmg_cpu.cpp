@@ -54,11 +54,11 @@ nebula::PtmgSums ptmg_sums(const PmlData& d, const double* beta, double alpha, d
   nebula::PtmgSums out;
   // pass one: sum e over every cell, sum y eta over the positive ones
   auto dense1 = [&](double* acc, size_t r, int s) {
-    double x[8];
+    double x[kMaxRow];
     acc[0] += nb_exp(eta_at(r, s, x));
   };
   auto sparse1 = [&](double* acc, size_t i, int s) {
-    double x[8];
+    double x[kMaxRow];
     acc[1] = nb_fma(eta_at(d.cells[i], s, x), d.counts[i], acc[1]);
   };
   std::vector<double> p1 = tree_sums(d, run, 2, warps, dense1, sparse1);
@@ -72,7 +72,7 @@ nebula::PtmgSums ptmg_sums(const PmlData& d, const double* beta, double alpha, d
   }
   // pass two
   auto dense2 = [&](double* acc, size_t r, int s) {
-    double x[8];
+    double x[kMaxRow];
     const double e = nb_exp(eta_at(r, s, x));
     const double yms = ym[s];
     const double we = yms * e;
@@ -112,7 +112,7 @@ nebula::PtmgSums ptmg_sums(const PmlData& d, const double* beta, double alpha, d
     }
   };
   auto sparse2 = [&](double* acc, size_t i, int s) {
-    double x[8];
+    double x[kMaxRow];
     const double y = d.counts[i];
     const double e = nb_exp(eta_at(d.cells[i], s, x));
     const double yms = ym[s];
@@ -178,14 +178,14 @@ nebula::PtmgSums ptmg_sums(const PmlData& d, const double* beta, double alpha, d
 }
 
 nebula::GenePlan plan_gene(const nebula::Shared& sh, const nebula::GeneCounts& gc, const double* totals,
-                           int* evaluations) {
+                           int* evaluations, bool tabled) {
   PmlData d{sh.design.data(), sh.log_offset.data(), sh.n_cells, sh.n_coef, gc.counts.data(), gc.cells.data(),
             gc.counts.size(), sh.fid.data(), sh.n_subjects, totals};
   const std::vector<double> xy = nebula::positive_xy(sh, gc);
   nebula::MarginalGene mg{&sh, &gc, totals, xy.data()};
   std::vector<double> start, lower, upper;
   nebula::marginal_box(sh, gc, &start, &lower, &upper);
-  nebula::MarginalSearch search(start, lower, upper, sh.n_coef);
+  nebula::MarginalSearch search(start, lower, upper, sh.n_coef, tabled);
   const int np = sh.n_coef + 2;
   std::vector<double> g(np), h(static_cast<size_t>(np) * np);
   while (const double* x = search.ask()) {

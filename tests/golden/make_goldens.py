@@ -1,13 +1,14 @@
 """Writes the golden fixtures the parity tests read.
 
-Run in a container that has the edge-rs 0.4.0 sources at REF (read-only):
+Run where the edge-rs 0.4.0 sources are checked out (read-only), naming
+their root on the command line or in EDGE_RS_REFERENCE:
 
-    python tests/golden/make_goldens.py
+    python tests/golden/make_goldens.py <edge-rs root>
 
 1. Copies the reference's committed R-derived CSV fixtures (produced by its
    tests/r/generate_fixtures.R from nebula 1.5.8/1.5.9 and nloptr 2.2.1) into
    tests/golden/data/: the BOBYQA traces, the 8-gene x 150-cell NEBULA golden
-   and the NEBULA-HL end-to-end datasets.
+   and the end-to-end datasets (NEBULA-HL and NEBULA-LN).
 2. Writes tests/golden/inline_goldens.json: the literal expected values the
    reference keeps inside its unit tests (R's 17-digit prints), transcribed
    here with the file:line each comes from.
@@ -18,8 +19,8 @@ script writes.
 import json
 import os
 import shutil
+import sys
 
-REF = "/root/reference"
 HERE = os.path.dirname(os.path.abspath(__file__))
 DATA = os.path.join(HERE, "data")
 
@@ -27,7 +28,7 @@ DATA = os.path.join(HERE, "data")
 # cells per subject, which the driver turns into HL), plus the LN ones kept for
 # the LN path.
 E2E_HL = ["sc_small", "sc_k2", "sc_intercept", "sc_wide", "sc_high", "sc_cat_hl", "sc_cat_sparse"]
-E2E_LN = ["sc_blocks", "sc_cat_ln"]
+E2E_LN = ["sc_blocks", "sc_cat_ln", "sc", "sc_xwide"]
 BOBYQA = ["rosen", "rosen_edge", "corner", "chain3", "rescue", "roundoff"]
 
 # --- opt_pml goldens, src/sc/pml.rs:2149-2700 (nebula:::opt_pml, nebula 1.5.8) ---
@@ -225,17 +226,20 @@ PTMG_CASES = [
 
 
 def main():
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("EDGE_RS_REFERENCE")
+    if not ref or not os.path.isdir(os.path.join(ref, "tests", "data")):
+        sys.exit("usage: make_goldens.py <edge-rs root> (or set EDGE_RS_REFERENCE)")
     os.makedirs(DATA, exist_ok=True)
     files = [f"e2e/bobyqa_{t}.csv" for t in BOBYQA]
     for tag in E2E_HL + E2E_LN:
         for part in ("counts", "meta", "design", "nebula", "covariance"):
             p = f"e2e/{tag}_{part}.csv"
-            if os.path.exists(os.path.join(REF, "tests", "data", p)):
+            if os.path.exists(os.path.join(ref, "tests", "data", p)):
                 files.append(p)
     files += ["e2e/scalars.csv"]
     files += [f"nebula_{p}.csv" for p in ("counts", "design", "expected", "covariance")]
     for f in files:
-        shutil.copyfile(os.path.join(REF, "tests", "data", f), os.path.join(DATA, os.path.basename(f)))
+        shutil.copyfile(os.path.join(ref, "tests", "data", f), os.path.join(DATA, os.path.basename(f)))
     inline = {"pml_fixture_a": PML_FIXTURE_A, "pml_fixture_b": PML_FIXTURE_B, "pml_cases": PML_CASES,
               "pml_gradient": PML_GRADIENT, "ptmg_fixtures": PTMG_FIXTURES, "ptmg_cases": PTMG_CASES,
               "e2e_hl": E2E_HL, "e2e_ln": E2E_LN, "bobyqa": BOBYQA}

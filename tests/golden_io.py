@@ -54,12 +54,14 @@ def dense_to_csr(dense):
 
 # tests/e2e_nebula.rs:288-398: (method, has_offset, n_coef, design_file)
 E2E = {
+    "sc": ("LN", True, 3, False),
     "sc_small": ("LN", True, 3, False),
     "sc_k2": ("HL", True, 3, True),
     "sc_blocks": ("LN", True, 3, True),
     "sc_intercept": ("HL", False, 1, True),
     "sc_wide": ("HL", True, 8, True),
     "sc_high": ("HL", True, 3, True),
+    "sc_xwide": ("LN", True, 13, True),
     "sc_cat_ln": ("LN", True, 4, True),
     "sc_cat_hl": ("HL", True, 4, True),
     "sc_cat_sparse": ("HL", True, 3, True),

@@ -99,3 +99,46 @@ def mlp_predict(params, features):
     out = np.zeros((x.shape[0], 3))
     lib().oracle_mlp_predict(_p(p), _p(x), ctypes.c_uint64(x.shape[0]), _p(out))
     return out
+
+
+_FG = ctypes.CFUNCTYPE(ctypes.c_double, ctypes.POINTER(ctypes.c_double), ctypes.c_uint32,
+                       ctypes.POINTER(ctypes.c_double), ctypes.c_void_p)
+
+
+def lbfgsb(fg, x0, lower, upper, memory=10, ftol=1e-6, pgtol=1e-5, max_iter=200, max_line_search=20):
+    """The stage-one quasi-Newton (csrc/host/lbfgsb.cpp) on fg(x) -> (value,
+    gradient). Returns (x, f, status, iterations, evaluations); a rejected
+    argument raises NebulaError with the EdgeErrors code."""
+    x0 = np.ascontiguousarray(x0, np.float64)
+    lo = np.ascontiguousarray(lower, np.float64)
+    hi = np.ascontiguousarray(upper, np.float64)
+    n = x0.size
+
+    def cb(x, m, grad, _ctx):
+        xv = np.ctypeslib.as_array(x, shape=(m,)).copy()
+        f, g = fg(xv)
+        gv = np.ctypeslib.as_array(grad, shape=(m,))
+        gv[:] = g
+        return float(f)
+
+    callback = _FG(cb)
+    out = np.zeros(max(n, 1))
+    f = ctypes.c_double(0.0)
+    ints = np.zeros(3, np.int32)
+    err = ctypes.create_string_buffer(256)
+    rc = lib().oracle_lbfgsb(callback, None, _p(x0), ctypes.c_uint32(n), _p(lo), ctypes.c_uint32(lo.size), _p(hi),
+                             ctypes.c_uint32(hi.size), ctypes.c_int32(memory), ctypes.c_double(ftol),
+                             ctypes.c_double(pgtol), ctypes.c_int32(max_iter), ctypes.c_int32(max_line_search),
+                             _p(out), ctypes.byref(f), _p(ints), err, ctypes.c_uint64(len(err)))
+    if rc != 0:
+        raise NebulaError(rc, err.value.decode(errors="replace"))
+    return out[:n], f.value, int(ints[0]), int(ints[1]), int(ints[2])
+
+
+def lbfgsb_solve_dense(a, b):
+    """solve_dense of the quasi-Newton; None when singular."""
+    a = np.ascontiguousarray(a, np.float64)
+    b = np.ascontiguousarray(b, np.float64)
+    x = np.zeros(b.size)
+    rc = lib().oracle_lbfgsb_solve_dense(_p(a), _p(b), ctypes.c_uint32(b.size), _p(x))
+    return None if rc != 0 else x
