@@ -352,6 +352,8 @@ def ours_arm(args, world, rank, local, dist):
                    # device time from the first fit's start to the last fit's end, and
                    # the step's device time outside it (start-up and the drain)
                    "busy_span_ms": stats[-1]["ms_busy_span"],
+                   # summed over the fits: device time clusters waited for their tickets
+                   "ticket_wait_ms": stats[-1]["ms_ticket_wait"],
                    "outside_span_ms": stats[-1]["ms_step_device"] - stats[-1]["ms_busy_span"]},
     }
     print(json.dumps(line), flush=True)

@@ -70,7 +70,8 @@ class NbStats(ctypes.Structure):
                 ("audited", ctypes.c_uint64), ("refit_cold", ctypes.c_uint64),
                 ("fit_slots", ctypes.c_uint64), ("slot_cycles", ctypes.c_uint64),
                 ("cluster", ctypes.c_uint64), ("ms_upload", ctypes.c_double),
-                ("ms_busy_span", ctypes.c_double), ("zero_groups", ctypes.c_uint64)]
+                ("ms_busy_span", ctypes.c_double), ("zero_groups", ctypes.c_uint64),
+                ("ms_ticket_wait", ctypes.c_double)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

@@ -40,7 +40,7 @@ struct alignas(16) FitResult {
   int32_t iterations, backtracks, sweeps, status;  // status 0 ok, 1 rejected arguments
   int64_t cycles;  // SM clock cycles the request held its CTAs (summed over the cluster)
   int64_t start_ns, end_ns;  // global timer when the fit began and ended
-  int64_t pad;
+  int64_t wait_ns;  // streaming mode: how long the cluster waited for this ticket's request
 };
 
 // FitRequest.flags: start the Newton loop from the gene's stored (beta,
@@ -129,24 +129,40 @@ int launch_fit(const GeneData& data, const FitControl& ctl, const FitRequest* re
                int cluster, void* stream);
 
 // Streaming mode: one persistent launch serves requests the host posts while
-// it runs. Ticket t's request is ring[t & mask] in device memory; the host
-// copies it there and then, by a later copy on the same stream, seq[t & mask]
-// = t. A cluster takes the next ticket off `taken`, polls seq[t & mask]
-// (backing off, at most idle_ns by the global timer), runs the fit, writes
-// the result into results[t & mask] (host memory mapped into the device's
-// address space) and then done[t & mask] = t + 1. *stop != 0 tells clusters
-// waiting on a ticket nobody will post to exit; a wait that runs out sets
-// *status = 1 and exits too. Nothing else waits.
-struct FitQueue {
-  const FitRequest* ring;
-  const long long* seq;
-  const int* stop;
-  unsigned long long* taken;
-  FitResult* results;
-  long long* done;
-  int* status;
-  long long mask;
+// it runs, through a request ring (ring_device.cuh).
+// - The host stores ticket t's request in host_ring[t & mask] and then
+//   releases `posted` = t + 1 (tickets are posted in order). Both are host
+//   memory mapped into the device's address space, so posting needs no copy
+//   engine and works while launches are serialised.
+// - A cluster takes the next ticket off words[kTaken] and waits until
+//   words[kForwarded] > t, polling L2 only. One waiting warp at a time (the
+//   holder of words[kLock]) reads `posted` across the bus and forwards the
+//   newly posted requests into the device ring; the rest never touch host
+//   memory, so a hundred idle clusters add no bus traffic that the result
+//   writes and their fences would queue behind.
+// - The cluster reads its request from the device ring, runs it, writes the
+//   result into results[t & mask] (mapped) and then done[t & mask] = t + 1.
+// - *stop != 0 (mapped) means nothing more will be posted: the lock holder
+//   that has forwarded everything sets words[kStopped], and clusters waiting
+//   on a ticket nobody will post exit. A wait that runs out (idle_ns by the
+//   global timer) sets *status = 1 (mapped) and exits too.
+struct RingView {
+  const char* host_ring;             // mapped: requests as posted
+  const unsigned long long* posted;  // mapped: tickets below it are posted
+  const int* stop;                   // mapped
+  int* status;                       // mapped
+  char* ring;                        // device: forwarded requests
+  unsigned long long* words;         // device: kRingWords counters, zeroed before the launch
+  long long mask;                    // ring capacity - 1 (a power of two)
   long long idle_ns;
+  int request_bytes;                 // a multiple of 8
+};
+constexpr int kTaken = 0, kForwarded = 1, kLock = 2, kStopped = 3, kRingWords = 4;
+
+struct FitQueue {
+  RingView ring;
+  FitResult* results;  // mapped
+  long long* done;     // mapped
 };
 
 int launch_fit_queue(const GeneData& data, const FitControl& ctl, const FitQueue& queue, int grid, int cluster,

@@ -38,6 +38,7 @@
 #include "nbmath_device.cuh"
 #include "pml_device.cuh"
 #include "pml_fit_ops.cuh"
+#include "ring_device.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -1061,55 +1062,41 @@ __global__ void __launch_bounds__(kThreads, min_blocks(NB, NV)) fit_queue_kernel
   const Cluster cl = setup_cta<NB, NV>(d, sm);
   const int tid = threadIdx.x;
   __shared__ long long next_ticket;  // the ticket to run, or -1 to exit
+  __shared__ FitRequest next_req;    // its request
   int parity = 0;
+  long long wait_ns = 0;             // rank 0's thread 0: the last ticket's wait
 
   for (;;) {
+    // rank 0's first warp takes a ticket, waits for its request and hands
+    // ticket and request to every CTA of the cluster; the first barrier keeps
+    // it from overwriting what a CTA has not read yet
     cluster_barrier(cl);
-    if (cl.rank == 0 && tid == 0) {
-      const long long t = static_cast<long long>(atomicAdd(qu.taken, 1ull));
-      const volatile long long* seq = qu.seq + (t & qu.mask);
-      const volatile int* stop = qu.stop;
-      const long long t0 = global_ns();
-      unsigned int pause = 128;
-      long long got = -1;
-      for (;;) {
-        if (*seq == t) {
-          got = t;
-          break;
-        }
-        if (*stop != 0) break;
-        if (global_ns() - t0 > qu.idle_ns) {
-          atomicExch(qu.status, 1);
-          break;
-        }
-        __nanosleep(pause);
-        if (pause < 2048) pause *= 2;
-      }
-      if (cl.size == 1) {
+    if (cl.rank == 0 && tid < 32) {
+      long long waited = 0;
+      const long long got = ring_next(qu.ring, &next_req, &waited);
+      if (tid == 0) {
+        wait_ns = waited;
         next_ticket = got;
-      } else {
+      }
+      if (cl.size > 1) {
         cg::cluster_group cluster = cg::this_cluster();
-        for (int r = 0; r < cl.size; ++r) *cluster.map_shared_rank(&next_ticket, r) = got;
+        constexpr int kWords = static_cast<int>(sizeof(FitRequest) / 8);
+        const unsigned long long* mine = reinterpret_cast<const unsigned long long*>(&next_req);
+        for (int r = 1; r < cl.size; ++r) {
+          if (tid == 0) *cluster.map_shared_rank(&next_ticket, r) = got;
+          if (tid < kWords && got >= 0)
+            cluster.map_shared_rank(reinterpret_cast<unsigned long long*>(&next_req), r)[tid] = mine[tid];
+        }
       }
     }
     cluster_barrier(cl);
     const long long t = next_ticket;
     if (t < 0) break;
-    // the request, read past L1: the host's copy landed in L2 before the
-    // sequence number this cluster saw
-    FitRequest req;
-    {
-      const int4* src = reinterpret_cast<const int4*>(qu.ring + (t & qu.mask));
-      int4* dst = reinterpret_cast<int4*>(&req);
-#pragma unroll
-      for (int i = 0; i < static_cast<int>(sizeof(FitRequest) / 16); ++i) dst[i] = __ldcg(src + i);
-    }
-    fit_one<NB, NV>(d, ctl, sm, req, qu.results + (t & qu.mask), cl, parity, clock64());
-    if (cl.rank == 0) {
-      // every thread's result writes reach host memory before the flag
-      __threadfence_system();
-      __syncthreads();
-      if (tid == 0) reinterpret_cast<volatile long long*>(qu.done)[t & qu.mask] = t + 1;
+    const FitRequest req = next_req;
+    fit_one<NB, NV>(d, ctl, sm, req, qu.results + (t & qu.ring.mask), cl, parity, clock64());
+    if (cl.rank == 0) {  // rank 0 wrote the result
+      if (tid == 0) qu.results[t & qu.ring.mask].wait_ns = wait_ns;
+      ring_publish(qu.done + (t & qu.ring.mask), t);
     }
   }
 }

@@ -42,16 +42,10 @@ int ptmg_blocks_per_sm(int n_subjects, int n_coef, int n_varying);
 // each in host-mapped memory; one CTA per request, `grid` CTAs each owning
 // its row of `scratch`.
 struct PtmgQueue {
-  const PtmgRequest* ring;
-  const long long* seq;
-  const int* stop;
-  unsigned long long* taken;
+  RingView ring;
   double* results;
   long long result_stride;
   long long* done;
-  int* status;
-  long long mask;
-  long long idle_ns;
 };
 
 int launch_ptmg_queue(const GeneData& d, const PtmgQueue& queue, double* scratch, int grid, void* stream);

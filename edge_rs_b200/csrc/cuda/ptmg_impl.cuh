@@ -26,9 +26,9 @@
 // The summation tree, the exp/log (nbmath.hpp) and the fused multiply-adds
 // (written explicitly; compiled with -fmad=false) are those of the CPU oracle
 // (oracle/ptmg_cpu.cpp), so the two agree bit for bit. One persistent launch
-// serves the whole stage: each CTA claims the next ticket of the device
-// request ring, waits (bounded) for the host to post it, and writes its
-// result to host-mapped memory; the warp slots and the subjects' reduced
+// serves the whole stage: each CTA claims the next ticket of the request
+// ring (host memory mapped into the device), waits (bounded) for the host to
+// post it, and writes its result to host-mapped memory; the warp slots and the subjects' reduced
 // sums live in a per-CTA global scratch region (L2-resident).
 #pragma once
 
@@ -39,6 +39,7 @@
 #include "../host/nbmath.hpp"
 #include "ptmg_device.cuh"
 #include "ptmg_ops.cuh"
+#include "ring_device.cuh"
 
 namespace nebula {
 namespace device {
@@ -382,12 +383,6 @@ __device__ void ptmg_one(const GeneData& d, const PtmgCta& c, const PtmgRequest&
   }
 }
 
-__device__ __forceinline__ long long global_ns() {
-  long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
 // Streaming mode: one persistent launch for stage one, the request-ring
 // protocol of FitQueue (pml_device.cuh) with one CTA per request.
 template <int NB, int NV>
@@ -396,46 +391,20 @@ __global__ void __launch_bounds__(ptmg_threads(NB, NV), 1)
   extern __shared__ __align__(16) double smem[];
   const PtmgCta c = ptmg_setup<NB, NV>(d, smem, scratch);
   __shared__ long long next_ticket;
+  __shared__ PtmgRequest next_req;
   __shared__ double beta_sm[kMaxCoef];
   for (;;) {
     __syncthreads();
-    if (threadIdx.x == 0) {
-      const long long t = static_cast<long long>(atomicAdd(qu.taken, 1ull));
-      const volatile long long* seq = qu.seq + (t & qu.mask);
-      const volatile int* stop = qu.stop;
-      const long long t0 = global_ns();
-      unsigned int pause = 128;
-      long long got = -1;
-      for (;;) {
-        if (*seq == t) {
-          got = t;
-          break;
-        }
-        if (*stop != 0) break;
-        if (global_ns() - t0 > qu.idle_ns) {
-          atomicExch(qu.status, 1);
-          break;
-        }
-        __nanosleep(pause);
-        if (pause < 2048) pause *= 2;
-      }
-      next_ticket = got;
+    if (threadIdx.x < 32) {  // the first warp takes a ticket and waits for its request
+      const long long got = ring_next(qu.ring, &next_req, nullptr);
+      if (threadIdx.x == 0) next_ticket = got;
     }
     __syncthreads();
     const long long t = next_ticket;
     if (t < 0) break;
-    PtmgRequest req;
-    {
-      const int4* src = reinterpret_cast<const int4*>(qu.ring + (t & qu.mask));
-      int4* dst = reinterpret_cast<int4*>(&req);
-#pragma unroll
-      for (int i = 0; i < static_cast<int>(sizeof(PtmgRequest) / 16); ++i) dst[i] = __ldcg(src + i);
-    }
-    ptmg_one<NB, NV>(d, c, req, beta_sm, qu.results + (t & qu.mask) * qu.result_stride);
-    // every thread's result writes reach host memory before the flag
-    __threadfence_system();
-    __syncthreads();
-    if (threadIdx.x == 0) reinterpret_cast<volatile long long*>(qu.done)[t & qu.mask] = t + 1;
+    const PtmgRequest req = next_req;
+    ptmg_one<NB, NV>(d, c, req, beta_sm, qu.results + (t & qu.ring.mask) * qu.result_stride);
+    ring_publish(qu.done + (t & qu.ring.mask), t);
   }
 }
 

@@ -232,8 +232,11 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
   // zero-count tables (the reference's ZeroCells, nebula.rs:641): built once
   // for the call when enough cells share their subject's design rows
   {
+    // whether the run is tabled decides stage one's descent (L-BFGS-B), so
+    // it is found even when the sweeps are asked to visit every cell
     zero::Tables zt;
-    if (tables && zero::build_tables(sh.design.data(), sh.log_offset.data(), sh.fid.data(), K, sh.n_coef, &zt)) {
+    design_tabled_ = zero::build_tables(sh.design.data(), sh.log_offset.data(), sh.fid.data(), K, sh.n_coef, &zt);
+    if (tables && design_tabled_) {
       std::vector<uint64_t> lpos(R + 1);
       for (int v = 0; v <= R; ++v)
         lpos[v] = static_cast<uint64_t>(std::lower_bound(zt.loose.begin(), zt.loose.end(), rcells[v]) -
@@ -289,6 +292,7 @@ void DeviceFitter::reset_counters() {
   launches_ = requests_ = sweeps_ = cell_visits_ = slot_cycles_ = h2d_bytes_ = d2h_bytes_ = 0;
   first_ns_ = INT64_MAX;
   last_ns_ = INT64_MIN;
+  wait_ns_ = 0;
 }
 
 void DeviceFitter::begin_step() {
@@ -342,25 +346,27 @@ size_t DeviceFitter::ptmg_stride() const {
   return static_cast<size_t>(2 + device::ptmg_width_of(data_.n_coef)) * static_cast<size_t>(data_.n_subjects);
 }
 
-void DeviceFitter::ptmg_queue_start(size_t capacity) {
+void DeviceFitter::ptmg_queue_prepare(size_t capacity) {
   ensure_ptmg_scratch();
   if (!ptmgq_ || ptmgq_->capacity() != capacity)
     ptmgq_ = std::make_unique<RequestQueue>(sizeof(device::PtmgRequest), ptmg_stride() * sizeof(double), capacity);
-  ptmgq_->start(stream_, [&](const RequestQueue::View& v) {
+  ptmgq_->prepare(stream_);
+}
+
+void DeviceFitter::ptmg_queue_launch() {
+  ptmgq_->launch(stream_, [&](const RequestQueue::View& v) {
     device::PtmgQueue pq{};
-    pq.ring = static_cast<const device::PtmgRequest*>(v.ring);
-    pq.seq = v.seq;
-    pq.stop = v.stop;
-    pq.taken = v.taken;
+    pq.ring = v.ring;
     pq.results = static_cast<double*>(v.results);
     pq.result_stride = static_cast<long long>(ptmg_stride());
     pq.done = v.done;
-    pq.status = v.status;
-    pq.mask = v.mask;
-    pq.idle_ns = v.idle_ns;
     return static_cast<cudaError_t>(device::launch_ptmg_queue(data_, pq, d_scratch_, pgrid_, stream_));
   });
   ++launches_;
+}
+
+void DeviceFitter::ptmg_request_stop() noexcept {
+  if (ptmgq_) ptmgq_->request_stop();
 }
 
 long long DeviceFitter::ptmg_post(const device::PtmgRequest* reqs, size_t n) { return ptmgq_->post(reqs, n); }
@@ -494,21 +500,17 @@ int DeviceFitter::cluster_for(size_t requests) const {
   return cluster;
 }
 
-void DeviceFitter::queue_start(int cluster) {
+void DeviceFitter::queue_prepare() { fitq_.prepare(stream_); }
+
+void DeviceFitter::queue_launch(int cluster) {
   if (cluster < 1 || cluster > device::kMaxCluster || queue_clusters_[cluster] <= 0)
     fail(NB_ERR_GPU, "no resident cluster of " + std::to_string(cluster) + " fit CTAs");
   const int grid = queue_clusters_[cluster] * cluster;
-  fitq_.start(stream_, [&](const RequestQueue::View& v) {
+  fitq_.launch(stream_, [&](const RequestQueue::View& v) {
     device::FitQueue fq{};
-    fq.ring = static_cast<const device::FitRequest*>(v.ring);
-    fq.seq = v.seq;
-    fq.stop = v.stop;
-    fq.taken = v.taken;
+    fq.ring = v.ring;
     fq.results = static_cast<device::FitResult*>(v.results);
     fq.done = v.done;
-    fq.status = v.status;
-    fq.mask = v.mask;
-    fq.idle_ns = v.idle_ns;
     return static_cast<cudaError_t>(device::launch_fit_queue(data_, ctl_, fq, grid, cluster, stream_));
   });
   ++launches_;
@@ -537,6 +539,7 @@ void DeviceFitter::queue_account(long long ticket, int gene, Tally* tally) const
   tally->cell_visits += sw * (dense_cells_ + gene_nnz_[static_cast<size_t>(gene)]);
   tally->slot_cycles += static_cast<uint64_t>(r.cycles);
   tally->first_ns = std::min<int64_t>(tally->first_ns, r.start_ns);
+  tally->wait_ns += r.wait_ns;
   tally->last_ns = std::max<int64_t>(tally->last_ns, r.end_ns);
 }
 
@@ -548,6 +551,7 @@ void DeviceFitter::add_tally(const Tally& t) {
   h2d_bytes_ += t.h2d;
   d2h_bytes_ += t.d2h;
   first_ns_ = std::min(first_ns_, t.first_ns);
+  wait_ns_ += t.wait_ns;
   last_ns_ = std::max(last_ns_, t.last_ns);
 }
 
@@ -711,6 +715,10 @@ std::unique_ptr<Session> create_session(const nb_csr* counts, const uint64_t* su
   std::vector<size_t> queued_genes;
   std::atomic<int> workers_left{workers};
   auto poster = [&]() {
+    struct StopAtEnd {  // every ticket has been read, or the stage failed
+      DeviceFitter& f;
+      ~StopAtEnd() { f.ptmg_request_stop(); }
+    } stop_at_end{*ss->fitter};
     std::vector<device::PtmgRequest> batch;
     std::vector<size_t> genes;
     try {
@@ -769,7 +777,7 @@ std::unique_ptr<Session> create_session(const nb_csr* counts, const uint64_t* su
       for (size_t g = static_cast<size_t>(w); g < G; g += static_cast<size_t>(workers)) {
         std::vector<double> start, lower, upper;
         marginal_box(sh, ss->genes[g], &start, &lower, &upper);
-        search[g] = std::make_unique<MarginalSearch>(start, lower, upper, nb);
+        search[g] = std::make_unique<MarginalSearch>(start, lower, upper, nb, ss->fitter->design_tabled());
         xy[g] = positive_xy(sh, ss->genes[g]);
         box.push_back(request_of(g));
         owners.push_back(g);
@@ -832,11 +840,22 @@ std::unique_ptr<Session> create_session(const nb_csr* counts, const uint64_t* su
       DeviceFitter& f;
       ~QueueGuard() { f.ptmg_abort(); }
     } guard{*ss->fitter};
-    ss->fitter->ptmg_queue_start(capacity);
+    // The ring is ready before the kernel starts and every thread that posts
+    // or reads results runs before the launch: a profiler that serialises
+    // launches returns from it only once the kernel has ended, which the
+    // poster's stop request at the end of the work allows.
+    ss->fitter->ptmg_queue_prepare(capacity);
     std::thread post_thread(poster);
     std::vector<std::thread> pool;
-    for (int w = 1; w < workers; ++w) pool.emplace_back(worker, w);
-    worker(0);
+    for (int w = 0; w < workers; ++w) pool.emplace_back(worker, w);
+    try {
+      ss->fitter->ptmg_queue_launch();
+    } catch (...) {
+      abort.store(true);
+      for (auto& th : pool) th.join();
+      post_thread.join();
+      throw;
+    }
     for (auto& th : pool) th.join();
     post_thread.join();
     if (first_err) throw *first_err;
@@ -1095,6 +1114,10 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
   // worker held the lock for half of the step, one or two requests a post).
   std::atomic<int> workers_left{0};
   auto poster = [&](DeviceFitter::Tally* tally) {
+    struct StopAtEnd {  // every ticket has been read, or the stage failed
+      DeviceFitter& f;
+      ~StopAtEnd() { f.queue_request_stop(); }
+    } stop_at_end{fitter};
     std::vector<device::FitRequest> batch;
     std::vector<std::pair<size_t, size_t>> owners;
     try {
@@ -1309,12 +1332,20 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
       DeviceFitter& f;
       ~QueueGuard() { f.queue_abort(); }
     } guard{fitter};
-    fitter.queue_start(cluster);
+    // as in stage one: the posting and reading threads run before the launch
+    fitter.queue_prepare();
     workers_left.store(workers);
     std::thread post_thread(poster, &tallies[workers]);
     std::vector<std::thread> pool;
-    for (int w = 1; w < workers; ++w) pool.emplace_back(worker, w);
-    worker(0);
+    for (int w = 0; w < workers; ++w) pool.emplace_back(worker, w);
+    try {
+      fitter.queue_launch(cluster);
+    } catch (...) {
+      abort.store(true);
+      for (auto& th : pool) th.join();
+      post_thread.join();
+      throw;
+    }
     for (auto& th : pool) th.join();
     post_thread.join();
     if (first_err) throw *first_err;
@@ -1347,6 +1378,7 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
     stats->ms_prepare = ss.ms_prepare;
     stats->ms_upload = ss.ms_upload;
     stats->ms_busy_span = fitter.busy_span_ms();
+    stats->ms_ticket_wait = fitter.ticket_wait_ms();
     stats->zero_groups = fitter.tabled_groups();
     stats->ms_stage_one = ss.ms_stage_one;
     stats->ms_stage_two = ms_stage_two;

@@ -45,10 +45,13 @@ class DeviceFitter {
   bool ready(int lane);
 
   // Streaming mode: one persistent launch serves requests posted while it
-  // runs (device::FitQueue). queue_start launches it with `cluster` CTAs per
-  // request; queue_post (safe from several host threads, each with its own
-  // `poster` index below kMaxPosters) copies a batch of requests into the
-  // device ring on the poster's stream and returns the first one's ticket;
+  // runs (device::FitQueue). queue_prepare resets the ring (requests may be
+  // posted from then on); queue_launch starts the kernel with `cluster` CTAs
+  // per request (under a profiler that serialises launches it returns only
+  // when the kernel has ended, so the threads that post and read results
+  // run before it and one of them calls queue_request_stop when the work is
+  // done); queue_post (safe from several host threads) stores a batch of
+  // requests into the mapped ring and returns the first one's ticket;
   // queue_done / queue_result read a ticket's result from host memory the
   // kernel writes; queue_stop tells idle clusters to exit, waits for the
   // kernel and reports a timed-out wait as NB_ERR_GPU.
@@ -56,8 +59,11 @@ class DeviceFitter {
   struct Tally {
     uint64_t requests = 0, sweeps = 0, cell_visits = 0, slot_cycles = 0, h2d = 0, d2h = 0;
     int64_t first_ns = INT64_MAX, last_ns = INT64_MIN;  // earliest fit start, latest fit end
+    int64_t wait_ns = 0;  // the clusters' waits for their tickets' requests
   };
-  void queue_start(int cluster);
+  void queue_prepare();
+  void queue_launch(int cluster);
+  void queue_request_stop() noexcept { fitq_.request_stop(); }
   long long queue_post(const device::FitRequest* reqs, size_t n, int poster, Tally* tally);
   bool queue_done(long long ticket) const;
   const device::FitResult& queue_result(long long ticket) const;
@@ -77,7 +83,9 @@ class DeviceFitter {
   int resident_fits(int cluster) const { return queue_clusters_[cluster]; }
   // Stage one in streaming mode (device::PtmgQueue), the same protocol as
   // the fit queue below; a result is ptmg_stride() doubles.
-  void ptmg_queue_start(size_t capacity);
+  void ptmg_queue_prepare(size_t capacity);
+  void ptmg_queue_launch();
+  void ptmg_request_stop() noexcept;
   // Posts from a thread that reads no results (RequestQueue::post).
   long long ptmg_post(const device::PtmgRequest* reqs, size_t n);
   void ptmg_consumed(long long ticket);
@@ -97,8 +105,12 @@ class DeviceFitter {
   uint64_t slot_cycles() const { return slot_cycles_; }
   // Zero-count groups the sweeps look up (0: every cell is swept).
   size_t tabled_groups() const { return tabled_groups_; }
+  // The run has zero-count tables (whether or not the sweeps use them):
+  // stage one then descends by L-BFGS-B alone, as the reference does.
+  bool design_tabled() const { return design_tabled_; }
   // Device time from the first fit's start to the last fit's end since the
   // last reset_counters, in ms (0 before any fit).
+  double ticket_wait_ms() const { return wait_ns_ / 1e6; }
   double busy_span_ms() const { return last_ns_ > first_ns_ ? (last_ns_ - first_ns_) / 1e6 : 0.0; }
   // CTAs the streaming kernel launches with `cluster` CTAs per fit.
   int queue_grid(int cluster) const { return queue_clusters_[cluster] * cluster; }
@@ -140,8 +152,9 @@ class DeviceFitter {
   size_t dense_cells_ = 0;  // cells a sweep's dense part visits
   device::GeneData data_{};
   device::FitControl ctl_{};
-  std::vector<void*> pooled_;
-  size_t tabled_groups_ = 0;  // stream-ordered allocations from the device's memory pool
+  std::vector<void*> pooled_;  // stream-ordered allocations from the device's memory pool
+  size_t tabled_groups_ = 0;
+  bool design_tabled_ = false;
   int grid_ = 0;
   int max_clusters_[device::kMaxCluster + 1] = {};  // resident clusters per cluster size
   // stage-one buffers
@@ -150,6 +163,7 @@ class DeviceFitter {
   double device_ms_ = 0.0;
   uint64_t launches_ = 0, requests_ = 0, sweeps_ = 0, cell_visits_ = 0, slot_cycles_ = 0;
   int64_t first_ns_ = INT64_MAX, last_ns_ = INT64_MIN;
+  int64_t wait_ns_ = 0;
   uint64_t h2d_bytes_ = 0, d2h_bytes_ = 0;
 };
 

@@ -12,7 +12,12 @@
 namespace nebula {
 namespace {
 
-constexpr long long kIdleNs = 30000000000LL;  // longest wait of a cluster for work: 30 s
+// Longest wait of a cluster for its ticket: 5 s. Tickets are posted as
+// results come back, so a cluster waits at most about as long as the
+// longest fit in flight (milliseconds); a ring that stalls fails within
+// seconds instead of holding every SM.
+constexpr long long kIdleNs = 5000000000LL;
+constexpr double kHostWaitMs = 60000.0;  // a post's wait for a slot to be read
 
 void check(cudaError_t e, const char* what) {
   if (e != cudaSuccess) fail(NB_ERR_GPU, std::string(what) + ": " + cudaGetErrorString(e));
@@ -22,25 +27,29 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
-// A ring's buffers, stream and events. Pinned and mapped host memory is slow
-// to allocate and to free, so a ring's set goes back to a process-wide pool
-// when the ring is destroyed and the next ring of the same shape on the same
+template <typename T>
+T* device_view(T* host) {
+  void* p = nullptr;
+  check(cudaHostGetDevicePointer(&p, host, 0), "mapped pointer");
+  return static_cast<T*>(p);
+}
+
+// A ring's buffers and events. Pinned and mapped host memory is slow to
+// allocate and to free, so a ring's set goes back to a process-wide pool when
+// the ring is destroyed and the next ring of the same shape on the same
 // device takes it (the memory is held until the process exits).
 struct RingSet {
   int device;
   size_t request_bytes, result_bytes, capacity;
+  unsigned long long* d_words;
   char* d_ring;
-  long long* d_seq;
-  int* d_stop;
-  unsigned long long* d_taken;
-  int* d_status;
   char* h_ring;
-  long long* h_seq;
-  int* h_one;
+  unsigned long long* h_posted;
+  int* h_stop;
+  int* h_status;
   char* h_results;
   long long* h_done;
-  cudaStream_t post_stream;
-  cudaEvent_t ev0, ev1, ready;
+  cudaEvent_t ev0, ev1;
 };
 
 std::mutex& pool_mutex() {
@@ -52,6 +61,12 @@ std::vector<RingSet>& ring_pool() {
   return *pool;
 }
 
+void* mapped_alloc(size_t bytes) {
+  void* p = nullptr;
+  check(cudaHostAlloc(&p, bytes, cudaHostAllocMapped), "cudaHostAlloc");
+  return p;
+}
+
 }  // namespace
 
 RequestQueue::RequestQueue(size_t request_bytes, size_t result_bytes, size_t capacity)
@@ -59,18 +74,16 @@ RequestQueue::RequestQueue(size_t request_bytes, size_t result_bytes, size_t cap
 
 RequestQueue::~RequestQueue() {
   abort();
-  if (!d_ring_) return;
-  cudaStreamSynchronize(post_stream_);
+  if (!h_ring_) return;
   std::lock_guard<std::mutex> lock(pool_mutex());
-  ring_pool().push_back(RingSet{device_, request_bytes_, result_bytes_, capacity_, d_ring_, d_seq_, d_stop_,
-                                d_taken_, d_status_, h_ring_, h_seq_, h_one_, h_results_, h_done_, post_stream_,
-                                ev0_, ev1_, ready_});
+  ring_pool().push_back(RingSet{device_, request_bytes_, result_bytes_, capacity_, d_words_, d_ring_, h_ring_,
+                                h_posted_, h_stop_, h_status_, h_results_, h_done_, ev0_, ev1_});
 }
 
-void RequestQueue::start(cudaStream_t stream, const std::function<cudaError_t(const View&)>& launch) {
-  if (running_) fail(NB_ERR_GPU, "the work queue is already running");
+void RequestQueue::prepare(cudaStream_t stream) {
+  if (state_.load() != kIdle) fail(NB_ERR_GPU, "the work queue is already running");
   const size_t cap = capacity_;
-  if (!d_ring_) {
+  if (!h_ring_) {
     check(cudaGetDevice(&device_), "cudaGetDevice");
     std::lock_guard<std::mutex> lock(pool_mutex());
     std::vector<RingSet>& pool = ring_pool();
@@ -79,84 +92,66 @@ void RequestQueue::start(cudaStream_t stream, const std::function<cudaError_t(co
       if (r.device != device_ || r.request_bytes != request_bytes_ || r.result_bytes != result_bytes_ ||
           r.capacity != cap)
         continue;
+      d_words_ = r.d_words;
       d_ring_ = r.d_ring;
-      d_seq_ = r.d_seq;
-      d_stop_ = r.d_stop;
-      d_taken_ = r.d_taken;
-      d_status_ = r.d_status;
       h_ring_ = r.h_ring;
-      h_seq_ = r.h_seq;
-      h_one_ = r.h_one;
+      h_posted_ = r.h_posted;
+      h_stop_ = r.h_stop;
+      h_status_ = r.h_status;
       h_results_ = r.h_results;
       h_done_ = r.h_done;
-      post_stream_ = r.post_stream;
       ev0_ = r.ev0;
       ev1_ = r.ev1;
-      ready_ = r.ready;
       pool.erase(pool.begin() + static_cast<long>(i));
       break;
     }
   }
-  if (!d_ring_) {
+  if (!h_ring_) {
     check(cudaEventCreate(&ev0_), "event");
     check(cudaEventCreate(&ev1_), "event");
-    check(cudaEventCreateWithFlags(&ready_, cudaEventDisableTiming), "event");
-    check(cudaStreamCreateWithFlags(&post_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+    check(cudaMalloc(reinterpret_cast<void**>(&d_words_), device::kRingWords * sizeof(unsigned long long)),
+          "cudaMalloc");
     check(cudaMalloc(reinterpret_cast<void**>(&d_ring_), cap * request_bytes_), "cudaMalloc");
-    check(cudaMalloc(reinterpret_cast<void**>(&d_seq_), cap * sizeof(long long)), "cudaMalloc");
-    check(cudaMalloc(reinterpret_cast<void**>(&d_stop_), sizeof(int)), "cudaMalloc");
-    check(cudaMalloc(reinterpret_cast<void**>(&d_taken_), sizeof(unsigned long long)), "cudaMalloc");
-    check(cudaMalloc(reinterpret_cast<void**>(&d_status_), sizeof(int)), "cudaMalloc");
-    check(cudaMallocHost(reinterpret_cast<void**>(&h_ring_), cap * request_bytes_), "cudaMallocHost");
-    check(cudaMallocHost(reinterpret_cast<void**>(&h_seq_), cap * sizeof(long long)), "cudaMallocHost");
-    check(cudaMallocHost(reinterpret_cast<void**>(&h_one_), sizeof(int)), "cudaMallocHost");
-    *h_one_ = 1;
-    check(cudaHostAlloc(reinterpret_cast<void**>(&h_results_), cap * result_bytes_, cudaHostAllocMapped),
-          "cudaHostAlloc");
-    check(cudaHostAlloc(reinterpret_cast<void**>(&h_done_), cap * sizeof(long long), cudaHostAllocMapped),
-          "cudaHostAlloc");
+    h_ring_ = static_cast<char*>(mapped_alloc(cap * request_bytes_));
+    // posted, stop and status, a cache line apart
+    char* words = static_cast<char*>(mapped_alloc(3 * 64));
+    h_posted_ = reinterpret_cast<unsigned long long*>(words);
+    h_stop_ = reinterpret_cast<int*>(words + 64);
+    h_status_ = reinterpret_cast<int*>(words + 128);
+    h_results_ = static_cast<char*>(mapped_alloc(cap * result_bytes_));
+    h_done_ = static_cast<long long*>(mapped_alloc(cap * sizeof(long long)));
   }
-  // tickets restart at zero: no stale sequence number or done flag may match one
+  // tickets restart at zero: no stale done flag may match one (the kernel is
+  // not running, and its launch orders these stores before any of its loads)
   std::memset(h_done_, 0, cap * sizeof(long long));
+  std::atomic_ref<unsigned long long>(*h_posted_).store(0);
+  std::atomic_ref<int>(*h_stop_).store(0);
+  std::atomic_ref<int>(*h_status_).store(0);
   if (!consumed_) consumed_.reset(new std::atomic<long long>[cap]);
   for (size_t i = 0; i < cap; ++i) consumed_[i].store(0);
   next_.store(0);
-  check(cudaMemsetAsync(d_seq_, 0xff, cap * sizeof(long long), stream), "memset");
-  check(cudaMemsetAsync(d_stop_, 0, sizeof(int), stream), "memset");
-  check(cudaMemsetAsync(d_taken_, 0, sizeof(unsigned long long), stream), "memset");
-  check(cudaMemsetAsync(d_status_, 0, sizeof(int), stream), "memset");
-  check(cudaEventRecord(ready_, stream), "event");
-  check(cudaStreamWaitEvent(post_stream_, ready_, 0), "stream wait");  // posts follow the resets
-  View v{};
-  v.ring = d_ring_;
-  v.seq = d_seq_;
-  v.stop = d_stop_;
-  v.taken = d_taken_;
-  void* dev_ptr = nullptr;
-  check(cudaHostGetDevicePointer(&dev_ptr, h_results_, 0), "mapped results");
-  v.results = dev_ptr;
-  check(cudaHostGetDevicePointer(&dev_ptr, h_done_, 0), "mapped flags");
-  v.done = static_cast<long long*>(dev_ptr);
-  v.status = d_status_;
-  v.mask = static_cast<long long>(cap - 1);
-  v.idle_ns = kIdleNs;
-  check(cudaEventRecord(ev0_, stream), "event");
-  check(launch(v), "queue kernel launch");
-  check(cudaEventRecord(ev1_, stream), "event");
-  running_ = true;
+  check(cudaMemsetAsync(d_words_, 0, device::kRingWords * sizeof(unsigned long long), stream), "memset");
+  state_.store(kPrepared);
 }
 
-void RequestQueue::copy_range(void* dst, const void* src, size_t elem, long long first, size_t n) {
-  const long long mask = static_cast<long long>(capacity_ - 1);
-  size_t copied = 0;
-  while (copied < n) {
-    const size_t slot = static_cast<size_t>((first + static_cast<long long>(copied)) & mask);
-    const size_t len = std::min(n - copied, capacity_ - slot);
-    check(cudaMemcpyAsync(static_cast<char*>(dst) + slot * elem, static_cast<const char*>(src) + slot * elem,
-                          len * elem, cudaMemcpyHostToDevice, post_stream_),
-          "queue copy");
-    copied += len;
-  }
+void RequestQueue::launch(cudaStream_t stream, const std::function<cudaError_t(const View&)>& launch_fn) {
+  if (state_.load() != kPrepared) fail(NB_ERR_GPU, "the work queue was not prepared");
+  View v{};
+  v.ring.host_ring = device_view(h_ring_);
+  v.ring.posted = device_view(h_posted_);
+  v.ring.stop = device_view(h_stop_);
+  v.ring.status = device_view(h_status_);
+  v.ring.ring = d_ring_;
+  v.ring.words = d_words_;
+  v.ring.mask = static_cast<long long>(capacity_ - 1);
+  v.ring.idle_ns = kIdleNs;
+  v.ring.request_bytes = static_cast<int>(request_bytes_);
+  v.results = device_view(h_results_);
+  v.done = device_view(h_done_);
+  check(cudaEventRecord(ev0_, stream), "event");
+  check(launch_fn(v), "queue kernel launch");
+  check(cudaEventRecord(ev1_, stream), "event");
+  state_.store(kLaunched);
 }
 
 long long RequestQueue::post(const void* requests, size_t n) { return post_impl(requests, n, true); }
@@ -177,12 +172,9 @@ bool RequestQueue::slot_free(long long t) const {
 long long RequestQueue::post_impl(const void* requests, size_t n, bool wait) {
   if (n == 0) return next_.load();
   if (n > capacity_ / 2) fail(NB_ERR_GPU, "too many requests in one post");
-  // One post at a time through one stream: copies from several streams into
-  // neighbouring ring slots lost updates.
-  std::lock_guard<std::mutex> lock(post_mu_);
+  std::lock_guard<std::mutex> lock(post_mu_);  // tickets are handed out in order
   const long long first = next_.load();
-  const long long cap = static_cast<long long>(capacity_);
-  const long long mask = cap - 1;
+  const long long mask = static_cast<long long>(capacity_) - 1;
   for (size_t i = 0; i < n; ++i) {
     const long long t = first + static_cast<long long>(i);
     if (slot_free(t)) continue;
@@ -191,21 +183,22 @@ long long RequestQueue::post_impl(const void* requests, size_t n, bool wait) {
     const auto t0 = std::chrono::steady_clock::now();
     while (!slot_free(t)) {
       if (!running()) failure("ended with work pending");
-      if (ms_since(t0) > 60000.0) failure("made no progress for 60 s");
+      if (ms_since(t0) > kHostWaitMs) failure("made no progress for 60 s");
       std::this_thread::yield();
     }
   }
   next_.store(first + static_cast<long long>(n));
+  // the requests, then the released count: the warp that acquires `posted`
+  // reads the requests stored before it (the device reads this memory
+  // coherently)
   const char* src = static_cast<const char*>(requests);
   for (size_t i = 0; i < n; ++i) {
     const long long t = first + static_cast<long long>(i);
     std::memcpy(h_ring_ + static_cast<size_t>(t & mask) * request_bytes_, src + i * request_bytes_,
                 request_bytes_);
-    h_seq_[t & mask] = t;
   }
-  // the requests, then (later on the same stream) their sequence numbers
-  copy_range(d_ring_, h_ring_, request_bytes_, first, n);
-  copy_range(d_seq_, h_seq_, sizeof(long long), first, n);
+  std::atomic_ref<unsigned long long>(*h_posted_)
+      .store(static_cast<unsigned long long>(first) + n, std::memory_order_release);
   return first;
 }
 
@@ -220,28 +213,32 @@ const void* RequestQueue::result(long long ticket) const {
 }
 
 bool RequestQueue::running() {
+  const int s = state_.load();
+  if (s == kPrepared) return true;  // launched soon (or now, by another thread)
+  if (s != kLaunched) return false;
   const cudaError_t e = cudaEventQuery(ev1_);
   if (e == cudaErrorNotReady) return true;
   check(e, "queue kernel");
   return false;
 }
 
+void RequestQueue::request_stop() noexcept {
+  if (h_stop_) std::atomic_ref<int>(*h_stop_).store(1, std::memory_order_release);
+}
+
 void RequestQueue::stop_impl(bool check_status) {
-  if (!running_) return;
-  running_ = false;
-  const cudaError_t e1 = cudaMemcpyAsync(d_stop_, h_one_, sizeof(int), cudaMemcpyHostToDevice, post_stream_);
-  const cudaError_t e2 = cudaEventSynchronize(ev1_);
-  int status = 0;
-  const cudaError_t e3 = cudaMemcpy(&status, d_status_, sizeof(int), cudaMemcpyDeviceToHost);
-  cudaStreamSynchronize(post_stream_);
+  const int s = state_.exchange(kIdle);
+  if (s == kIdle) return;
+  request_stop();
+  if (s != kLaunched) return;  // never launched: nothing to wait for
+  const cudaError_t e = cudaEventSynchronize(ev1_);
+  const int status = std::atomic_ref<int>(*h_status_).load(std::memory_order_acquire);
   if (!check_status) return;
-  check(e1, "stop copy");
-  check(e2, "queue kernel");
-  check(e3, "queue status");
+  check(e, "queue kernel");
   float ms = 0.0f;
   check(cudaEventElapsedTime(&ms, ev0_, ev1_), "event time");
   device_ms_ += ms;
-  if (status != 0) fail(NB_ERR_GPU, "a queue cluster waited more than 30 s for work");
+  if (status != 0) fail(NB_ERR_GPU, "a queue cluster waited more than 5 s for work");
 }
 
 void RequestQueue::stop() { stop_impl(true); }
@@ -254,13 +251,15 @@ void RequestQueue::abort() noexcept {
 }
 
 void RequestQueue::failure(const char* what) {
-  int status = -1;
-  cudaMemcpy(&status, d_status_, sizeof(int), cudaMemcpyDeviceToHost);
-  unsigned long long taken = 0;
-  cudaMemcpy(&taken, d_taken_, sizeof(taken), cudaMemcpyDeviceToHost);
+  const int status = h_status_ ? std::atomic_ref<int>(*h_status_).load(std::memory_order_acquire) : 0;
+  std::string taken = "unknown while the kernel runs";
+  if (state_.load() == kLaunched && cudaEventQuery(ev1_) == cudaSuccess) {
+    unsigned long long n = 0;
+    if (cudaMemcpy(&n, d_words_ + device::kTaken, sizeof(n), cudaMemcpyDeviceToHost) == cudaSuccess)
+      taken = std::to_string(n);
+  }
   fail(NB_ERR_GPU, std::string("the queue kernel ") + what + " (tickets posted " + std::to_string(next_.load()) +
-                       ", taken " + std::to_string(taken) +
-                       (status == 1 ? ", a cluster waited more than 30 s for work)" : ")"));
+                       ", taken " + taken + (status == 1 ? ", a cluster waited more than 5 s for work)" : ")"));
 }
 
 }  // namespace nebula

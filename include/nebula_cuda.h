@@ -160,6 +160,9 @@ typedef struct nb_stats {
                                last fit's end in stages two and three */
   uint64_t zero_groups;     /* zero-count groups looked up instead of swept
                                (0: every sweep visits every cell) */
+  double ms_ticket_wait;    /* summed over the fits of stages two and three:
+                               device time a cluster waited for its ticket's
+                               request to be posted and read */
 } nb_stats;
 
 void nb_params_default(nb_params* params);
