@@ -44,17 +44,29 @@ METRIC = "NEBULA-HL genes/s @100k cells, 1 B200: warm-start+batched vs plain; ro
 PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "fit_kernel_traffic.json")
 
 
-def flops_per_visit(nv):
-    """FP64 operations of one cell visit of the fit kernel's sweep, whose
-    per-cell work covers only the nv design columns that vary within
-    subjects (the subject-constant columns' shares are applied per subject).
+def flops_per_visit(nv, sparse=False):
+    """FP64 FLOP of one cell visit of the fit kernel's sweep (pml_fit_impl.cuh,
+    sweep_sums with the table exp/log of nbmath.hpp), counted from the code:
+    an FMA counts two, any other FP64 arithmetic instruction one; compares,
+    integer and bit operations are not counted. nv: the design columns that
+    vary within subjects (the others' shares are applied per subject).
 
-    eta (the offset plus the subject's constant share, then nv FMAs), exp
-    (34), t, log (35), 1/t and the fold scalars (5), the fold: resid and
-    weight (2), per varying column X'd FMA, p x and its sum (4 nv), the p x x'
-    triangle (nv(nv+1) as FMAs); an FMA counts two, a division one.
+    eta: the offset plus the subject's constant share (1) and nv FMAs (2 nv)
+    exp (nb_exp_tab): 20 = x/L and the shifter (2), n (1), the two-part
+        reduction (2 FMA), the degree-5 polynomial (3 FMA), q (3), the table
+        product (3), the scale (1)
+    t = e + gamma (1)
+    log (nb_log_tab): 22 = r (1 FMA), the degree-7 polynomial (5 FMA), l1p (3),
+        the exponent (1), hi and lo (2 FMA), their sum (2)
+    1/t, correctly rounded (1), u = e/t (1)
+    fold: resid and weight (2), per varying column the X'd FMA, p x and its
+        sum (4 nv), the p x x' triangle (nv (nv + 1))
+    a dense (zero-count) cell: sum log t (1), d = -gamma u (1), p = gamma u/t (2)
+    a positive entry: log w_s in eta (1), sum y eta and sum y log t (2 FMA),
+        d = y (1 - u) (2), p = y u/t (2)
     """
-    return 2 * nv + 1 + 34 + 1 + 35 + 5 + 1 + 2 + 4 * nv + nv * (nv + 1)
+    common = 1 + 2 * nv + 20 + 1 + 22 + 1 + 1 + 2 + 4 * nv + nv * (nv + 1)
+    return common + (9 if sparse else 4)
 
 
 def varying_columns(design, subject):
@@ -171,7 +183,7 @@ def run_cpu(work, n_genes, threads):
     fit, _ = oracle_ffi.nebula_sparse(csr, work.subject, work.design, work.n_coef, work.offset,
                                       NebulaParams(method="HL"), threads=threads)
     el = time.perf_counter() - t0
-    return len(fit.gene_index) / el, len(fit.gene_index), el
+    return len(fit.gene_index) / el, len(fit.gene_index), el, fit
 
 
 def reference_arm(args, world, rank, dist):
@@ -181,7 +193,7 @@ def reference_arm(args, world, rank, dist):
     threads = os.cpu_count() or 1
     vals = []
     for i in range(args.warmup + args.steps):
-        v, n, el = run_cpu(work, args.cpu_genes, threads)
+        v, n, el, _ = run_cpu(work, args.cpu_genes, threads)
         if i >= args.warmup:
             vals.append(v)
     value = float(np.mean(vals))
@@ -202,8 +214,9 @@ def l2_flush(buf):
     buf.add_(1.0)
 
 
-def timed_session(args, work, params, flush, dist, warm):
-    """W warm-up and K timed nb_session_fit steps; L2 flushed before each."""
+def timed_session(args, work, params, flush, dist, warm, want_stage_one=False):
+    """W warm-up and K timed nb_session_fit steps; L2 flushed before each.
+    want_stage_one: also return stage one's (sigma, gamma) per kept gene."""
     import torch
     from edge_rs_b200.api import Session
     session = Session(work.csr, work.subject, work.design, work.n_coef, work.offset, params, cluster=args.cluster,
@@ -222,16 +235,61 @@ def timed_session(args, work, params, flush, dist, warm):
         t_wall += time.perf_counter() - t0
         step_ms.append(fit.stats["ms_step_device"])
         stats.append(fit.stats)
+    stage_one = session.features()[1] if want_stage_one else None
     session.close()
-    return step_ms, stats, fit, t_wall
+    return step_ms, stats, fit, t_wall, stage_one
 
 
-def max_rel(a, b):
-    return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-12))) if len(a) else 0.0
+def perturbed_plain(args, work, params, plain_fit, stage_one, delta):
+    """The plain method with its search started from stage one's estimate
+    times (1 + delta) for sigma and (1 - delta) for gamma: NLopt's trust
+    radius, cold inner fits, no audit. Against the plain fit it measures how
+    far two runs of the reference's search land apart from starts that
+    differ by `delta` (the objective is flat to the search's resolution)."""
+    from edge_rs_b200.api import Session
+    points = np.zeros((work.n_genes, 2))
+    points[plain_fit.gene_index, 0] = stage_one[:, 0] * (1.0 + delta)
+    points[plain_fit.gene_index, 1] = stage_one[:, 1] * (1.0 - delta)
+    s = Session(work.csr, work.subject, work.design, work.n_coef, work.offset, params, cluster=args.cluster,
+                warm_start=2, warm_points=points, warm_radius=1.0, audit_percent=0, cold_inner=True)
+    fit = s.fit()
+    s.close()
+    return fit
 
 
-def med_rel(a, b):
-    return float(np.median(np.abs(a - b) / np.maximum(np.abs(b), 1e-12))) if len(a) else 0.0
+def rel_errors(a, b, eps):
+    """Max and median of |a - b| / max(|a|, |b|) over the entries, an entry
+    within eps absolute counting as zero (assert_relative_eq's semantics)."""
+    a = np.asarray(a, np.float64).ravel()
+    b = np.asarray(b, np.float64).ravel()
+    if a.size == 0:
+        return {"max": 0.0, "median": 0.0}
+    diff = np.abs(a - b)
+    scale = np.maximum(np.abs(a), np.abs(b))
+    rel = np.where((diff <= eps) | (a == b), 0.0, diff / np.where(scale > 0, scale, 1.0))
+    return {"max": float(np.max(rel)), "median": float(np.median(rel))}
+
+
+def compare_fits(fit, ref):
+    """Errors of `fit` against `ref` on the genes both kept: beta, sigma^2,
+    phi (relative, eps 1e-9), Wald log p-values of every non-intercept
+    coefficient (relative, eps 1e-6, as the parity tests), and how many
+    convergence codes differ."""
+    from edge_rs_b200 import glm_sc_test
+    common = np.intersect1d(fit.gene_index, ref.gene_index)
+    ia = np.searchsorted(fit.gene_index, common)
+    ib = np.searchsorted(ref.gene_index, common)
+    out = {"genes": int(common.size)}
+    for key, name in (("coefficients", "beta"), ("subject_overdispersion", "sigma2"),
+                      ("cell_overdispersion", "phi")):
+        out[name] = rel_errors(getattr(fit, key)[ia], getattr(ref, key)[ib], 1e-9)
+    la, lb = [], []
+    for coef in range(1, fit.n_coef):
+        la.append(glm_sc_test(fit.coefficients[ia], fit.covariance[ia], coef=coef).log_p_value)
+        lb.append(glm_sc_test(ref.coefficients[ib], ref.covariance[ib], coef=coef).log_p_value)
+    out["log_p"] = rel_errors(np.concatenate(la) if la else [], np.concatenate(lb) if lb else [], 1e-6)
+    out["convergence_differs"] = int(np.sum(fit.convergence[ia] != ref.convergence[ib]))
+    return out
 
 
 def ours_arm(args, world, rank, local, dist):
@@ -242,25 +300,30 @@ def ours_arm(args, world, rank, local, dist):
     params = NebulaParams(method="HL")
     flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > 126 MB L2
     # the plain method (the reference's algorithm, bit-identical to the oracle)
-    plain_ms, plain_stats, plain_fit, _ = timed_session(args, work, params, flush, dist, 0)
+    plain_ms, plain_stats, plain_fit, _, stage_one = timed_session(args, work, params, flush, dist, 0,
+                                                                   want_stage_one=True)
     plain_value = world * len(plain_fit.gene_index) * args.steps / (barrier_max(dist, float(np.sum(plain_ms))) / 1000.0)
     # the headline: warm-started (learned search start, narrowed initial trust
     # radius, warm inner fits) and batched
     sampler = ClockSampler(local)
     sampler.start()
-    step_ms, stats, fit, t_wall = timed_session(args, work, params, flush, dist, args.warm)
+    step_ms, stats, fit, t_wall, _ = timed_session(args, work, params, flush, dist, args.warm)
     clocks = sampler.stop()
     genes = len(fit.gene_index)
     total_ms = barrier_max(dist, float(np.sum(step_ms)))
     value = world * genes * args.steps / (total_ms / 1000.0)
     launches = int(np.sum([s["gpu_launches"] for s in stats]))
     visits = float(np.sum([s["cell_visits"] for s in stats]))
+    sparse_visits = float(np.sum([s["sparse_visits"] for s in stats]))
     kernel_ms = float(np.sum([s["ms_device"] for s in stats]))
     fp64_peak = measure_fp64_tflops(5)
     # the fit kernel is the whole step (one persistent launch serves stages
-    # two and three), so its FLOP are divided by the step's device time
+    # two and three), so its FLOP are divided by the step's device time;
+    # dense (zero-count) and positive visits are counted apart
     n_varying = varying_columns(work.design, work.subject)
-    achieved = visits * flops_per_visit(n_varying) / (float(np.sum(step_ms)) / 1000.0) / 1e12
+    flop = ((visits - sparse_visits) * flops_per_visit(n_varying)
+            + sparse_visits * flops_per_visit(n_varying, sparse=True))
+    achieved = flop / (float(np.sum(step_ms)) / 1000.0) / 1e12
     traffic = None
     if os.path.exists(PROFILE_SUMMARY):
         try:
@@ -287,13 +350,23 @@ def ours_arm(args, world, rank, local, dist):
         e2e_all.append(f2.stats)
     if e2e_vals:  # the breakdown of the median call
         e2e_stats = e2e_all[int(np.argsort(e2e_vals)[len(e2e_vals) // 2])]
+    # the search's reproducibility floor: the plain method from starts
+    # perturbed by 1e-9 and by 1e-3 relative
+    floors = {f"plain_from_start_x(1+-{d:g})": perturbed_plain(args, work, params, plain_fit, stage_one, d)
+              for d in (1e-9, 1e-3)}
     if rank != 0:
         return
-    cpu = None
+    cpu, parity = None, None
     if world == 1 and not args.no_cpu_baseline:
-        cv, n, el = run_cpu(work, args.cpu_genes, os.cpu_count() or 1)
+        cv, n, el, ref = run_cpu(work, args.cpu_genes, os.cpu_count() or 1)
         cpu = {"value": cv, "unit": "genes/s", "cores": os.cpu_count() or 1, "kind": "port",
                "sample": f"first {n} of the workload's genes ({el:.1f} s of CPU work)"}
+        # every arm against the FP64 oracle on the sampled genes, at the
+        # workload's full size
+        parity = {"oracle_sample": f"first {n} genes of the workload, FP64 CPU oracle",
+                  "plain": compare_fits(plain_fit, ref), "warm": compare_fits(fit, ref),
+                  **{k: compare_fits(v, ref) for k, v in floors.items()}}
+    vs_plain = {"warm": compare_fits(fit, plain_fit), **{k: compare_fits(v, plain_fit) for k, v in floors.items()}}
     line = {
         "metric": METRIC, "value": value, "unit": "genes/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -308,24 +381,25 @@ def ours_arm(args, world, rank, local, dist):
                    "step": "stages two and three on device-resident inputs (nb_session_fit)"},
         "plain": {"value": plain_value, "ms_per_step": float(np.sum(plain_ms)) / args.steps,
                   "sweeps_per_step": plain_stats[-1]["sweeps"], "requests_per_step": plain_stats[-1]["requests"],
-                  "parity": "bit-identical to the FP64 CPU oracle (tests/test_gpu_nebula.py)"},
+                  "evaluations_per_gene": float(plain_fit.evaluations.mean())},
         "warm_vs_plain": value / plain_value,
         "warm_start": {"mode": args.warm, "audited": stats[-1]["audited"], "refit_cold": stats[-1]["refit_cold"],
-                       "max_rel_diff_vs_plain": {
-                           "subject_overdispersion": max_rel(fit.subject_overdispersion, plain_fit.subject_overdispersion),
-                           "cell_overdispersion": max_rel(fit.cell_overdispersion, plain_fit.cell_overdispersion),
-                           "coefficients": max_rel(fit.coefficients, plain_fit.coefficients)},
-                       "median_rel_diff_vs_plain": {
-                           "subject_overdispersion": med_rel(fit.subject_overdispersion, plain_fit.subject_overdispersion),
-                           "cell_overdispersion": med_rel(fit.cell_overdispersion, plain_fit.cell_overdispersion),
-                           "coefficients": med_rel(fit.coefficients, plain_fit.coefficients)},
-                       "convergence_differs": int(np.sum(fit.convergence != plain_fit.convergence)),
-                       "evaluations_per_gene": {"plain": float(plain_fit.evaluations.mean()),
-                                                "warm": float(fit.evaluations.mean())}},
+                       "evaluations_per_gene": float(fit.evaluations.mean())},
+        # max / median relative errors (beta, sigma^2, phi: eps 1e-9; Wald log p
+        # of every non-intercept coefficient: eps 1e-6) and differing
+        # convergence codes: each arm against the FP64 oracle on a gene sample,
+        # and against the plain arm on every gene
+        "parity": parity,
+        "vs_plain_all_genes": vs_plain,
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                      "frac": achieved / fp64_peak if fp64_peak > 0 else None, "traffic": traffic,
-                     "kernel": "fit_kernel", "flops_per_visit": flops_per_visit(n_varying),
+                     "kernel": "fit_queue_kernel",
+                     "flops_per_visit": {"dense": flops_per_visit(n_varying),
+                                         "positive": flops_per_visit(n_varying, sparse=True)},
+                     "visits_per_step": {"dense": (visits - sparse_visits) / args.steps,
+                                         "positive": sparse_visits / args.steps},
                      "varying_columns": n_varying,
+                     "flop_counting": "an FMA counts two, other FP64 arithmetic one (bench.py flops_per_visit)",
                      "time": "device time of the step (CUDA events around the persistent launch)",
                      "peak_source": "measured on this GPU: FP64 FMA chains (nb_measure_fp64_tflops)"},
         # the median call: the host's cores are shared with other jobs, and a
@@ -392,13 +466,7 @@ def zero_tables(args):
                                                         f"{work.n_cells} cells, {len(work.truth['sizes'])} subjects, "
                                                         f"{work.n_coef} columns, forced HL, plain method"},
                       **out, "speedup": out["tables"]["genes_per_s"] / out["dense"]["genes_per_s"],
-                      "max_rel_diff": {"subject_overdispersion": max_rel(a.subject_overdispersion,
-                                                                         b.subject_overdispersion),
-                                       "cell_overdispersion": max_rel(a.cell_overdispersion, b.cell_overdispersion),
-                                       "coefficients": max_rel(a.coefficients, b.coefficients)},
-                      "median_rel_diff": {"subject_overdispersion": med_rel(a.subject_overdispersion,
-                                                                            b.subject_overdispersion),
-                                          "coefficients": med_rel(a.coefficients, b.coefficients)}}), flush=True)
+                      "tables_vs_dense": compare_fits(a, b)}), flush=True)
 
 
 def fit_batch(args):

@@ -56,7 +56,8 @@ class NbOptions(ctypes.Structure):
                 ("host_threads", ctypes.c_int32), ("audit_percent", ctypes.c_int32),
                 ("mlp_weights", c_float_p), ("cluster", ctypes.c_int32),
                 ("warm_points", ctypes.POINTER(ctypes.c_double)), ("evaluations", ctypes.POINTER(ctypes.c_int32)),
-                ("warm_radius", ctypes.c_double), ("dense_sweep", ctypes.c_int32)]
+                ("warm_radius", ctypes.c_double), ("dense_sweep", ctypes.c_int32),
+                ("cold_inner", ctypes.c_int32)]
 
 
 class NbStats(ctypes.Structure):
@@ -71,7 +72,7 @@ class NbStats(ctypes.Structure):
                 ("fit_slots", ctypes.c_uint64), ("slot_cycles", ctypes.c_uint64),
                 ("cluster", ctypes.c_uint64), ("ms_upload", ctypes.c_double),
                 ("ms_busy_span", ctypes.c_double), ("zero_groups", ctypes.c_uint64),
-                ("ms_ticket_wait", ctypes.c_double)]
+                ("ms_ticket_wait", ctypes.c_double), ("sparse_visits", ctypes.c_uint64)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

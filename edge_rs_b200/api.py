@@ -122,7 +122,7 @@ def call_nebula(fn, counts, subject_id, design, n_coef, offset, params, extra_ar
 
 
 def _options(device, warm_start, host_threads, audit_percent, cluster, n_genes, warm_points=None,
-             mlp_weights=None, warm_radius=0.0, dense_sweep=False):
+             mlp_weights=None, warm_radius=0.0, dense_sweep=False, cold_inner=False):
     """An NbOptions plus the arrays it points into (kept alive by the caller)."""
     evaluations = np.zeros(max(int(n_genes), 1), np.int32)
     wp = None if warm_points is None else np.ascontiguousarray(warm_points, np.float64).reshape(-1, 2)
@@ -134,13 +134,14 @@ def _options(device, warm_start, host_threads, audit_percent, cluster, n_genes, 
     mode = int(warm_start)
     opts = _ffi.NbOptions(int(device), mode, int(host_threads), int(audit_percent),
                           _ffi.ptr(mw, ctypes.c_float), int(cluster), _ffi.ptr(wp, ctypes.c_double),
-                          _ffi.ptr(evaluations, ctypes.c_int32), float(warm_radius), int(bool(dense_sweep)))
+                          _ffi.ptr(evaluations, ctypes.c_int32), float(warm_radius), int(bool(dense_sweep)),
+                          int(bool(cold_inner)))
     return opts, [evaluations, wp, mw]
 
 
 def nebula_sparse_cuda(counts, subject_id, design, n_coef, offset=None, params: Optional[NebulaParams] = None,
                        warm_start=False, device=-1, host_threads=0, audit_percent=5, cluster=0, warm_points=None,
-                       mlp_weights=None, warm_radius=0.0, dense_sweep=False):
+                       mlp_weights=None, warm_radius=0.0, dense_sweep=False, cold_inner=False):
     """Fits NEBULA per gene with every inner penalised fit on the GPU.
 
     warm_start: False/0 plain (the reference's method). Otherwise every
@@ -154,12 +155,15 @@ def nebula_sparse_cuda(counts, subject_id, design, n_coef, offset=None, params: 
     default; 1: NLopt's); the final radius is NLopt's either way.
     dense_sweep: visit every cell in every sweep even where the zero-count
     tables of a categorical design apply (by default they are used, as the
-    reference's CPU path uses them).
+    reference's CPU path uses them). cold_inner: with a warm start, every
+    inner fit still starts cold, as the plain method's do (with
+    warm_radius=1 and audit_percent=0 the search then differs from the
+    plain one only in where it starts).
     """
     lib = _ffi.product_library()
     n_genes = int(_as_csr(counts).struct.n_genes)
     opts, keep = _options(device, warm_start, host_threads, audit_percent, cluster, n_genes, warm_points,
-                          mlp_weights, warm_radius, dense_sweep)
+                          mlp_weights, warm_radius, dense_sweep, cold_inner)
     fit = call_nebula(lib.nebula_sparse_cuda_ex, counts, subject_id, design, n_coef, offset, params,
                       options=opts, want_stats=True)
     fit.evaluations = keep[0][: len(fit.gene_index)].copy()
@@ -206,7 +210,7 @@ class Session:
 
     def __init__(self, counts, subject_id, design, n_coef, offset=None, params: Optional[NebulaParams] = None,
                  warm_start=False, device=-1, host_threads=0, audit_percent=5, cluster=0, warm_points=None,
-                 mlp_weights=None, warm_radius=0.0, dense_sweep=False):
+                 mlp_weights=None, warm_radius=0.0, dense_sweep=False, cold_inner=False):
         self._lib = _ffi.product_library()
         self._keep = []
         csr = _as_csr(counts)
@@ -217,7 +221,7 @@ class Session:
         self.n_coef = int(n_coef)
         p = (params or NebulaParams()).to_c()
         opts, arrays = _options(device, warm_start, host_threads, audit_percent, cluster, self.n_genes,
-                                warm_points, mlp_weights, warm_radius, dense_sweep)
+                                warm_points, mlp_weights, warm_radius, dense_sweep, cold_inner)
         self._evaluations = arrays[0]
         self._keep = [csr, subject, design, off, p, opts, arrays]
         handle = ctypes.c_void_p()

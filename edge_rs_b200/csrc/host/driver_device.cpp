@@ -289,7 +289,7 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
 
 void DeviceFitter::reset_counters() {
   device_ms_ = 0.0;
-  launches_ = requests_ = sweeps_ = cell_visits_ = slot_cycles_ = h2d_bytes_ = d2h_bytes_ = 0;
+  launches_ = requests_ = sweeps_ = cell_visits_ = sparse_visits_ = slot_cycles_ = h2d_bytes_ = d2h_bytes_ = 0;
   first_ns_ = INT64_MAX;
   last_ns_ = INT64_MIN;
   wait_ns_ = 0;
@@ -473,6 +473,7 @@ const device::FitResult* DeviceFitter::collect(int lane_index) {
     const uint64_t sw = static_cast<uint64_t>(lane.h_res[i].sweeps);
     sweeps_ += sw;
     cell_visits_ += sw * (dense_cells_ + gene_nnz_[lane.h_req[i].gene]);
+    sparse_visits_ += sw * gene_nnz_[lane.h_req[i].gene];
     slot_cycles_ += static_cast<uint64_t>(lane.h_res[i].cycles);
   }
   lane.pending = 0;
@@ -537,6 +538,7 @@ void DeviceFitter::queue_account(long long ticket, int gene, Tally* tally) const
   const uint64_t sw = static_cast<uint64_t>(r.sweeps);
   tally->sweeps += sw;
   tally->cell_visits += sw * (dense_cells_ + gene_nnz_[static_cast<size_t>(gene)]);
+  tally->sparse_visits += sw * gene_nnz_[static_cast<size_t>(gene)];
   tally->slot_cycles += static_cast<uint64_t>(r.cycles);
   tally->first_ns = std::min<int64_t>(tally->first_ns, r.start_ns);
   tally->wait_ns += r.wait_ns;
@@ -547,6 +549,7 @@ void DeviceFitter::add_tally(const Tally& t) {
   requests_ += t.requests;
   sweeps_ += t.sweeps;
   cell_visits_ += t.cell_visits;
+  sparse_visits_ += t.sparse_visits;
   slot_cycles_ += t.slot_cycles;
   h2d_bytes_ += t.h2d;
   d2h_bytes_ += t.d2h;
@@ -1003,7 +1006,7 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
     f.slots.clear();
     f.tickets.clear();
     f.anchor = -1;
-    const bool inner_warm = warm && v < G;
+    const bool inner_warm = warm && v < G && ss.opt.cold_inner == 0;
     const int wb = wstep[g] & 1;
     const bool can_read = inner_warm && wvalid[g][1 - wb];
     for (const auto& point : t.search->ask()) {
@@ -1369,6 +1372,7 @@ void fit_session(Session& ss, nb_fit* out, nb_stats* stats) {
     stats->requests = fitter.requests();
     stats->sweeps = fitter.sweeps();
     stats->cell_visits = fitter.cell_visits();
+    stats->sparse_visits = fitter.sparse_visits();
     stats->fit_slots = static_cast<uint64_t>(fitter.queue_grid(cluster));
     stats->slot_cycles = fitter.slot_cycles();
     stats->cluster = static_cast<uint64_t>(cluster);

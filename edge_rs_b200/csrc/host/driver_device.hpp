@@ -57,7 +57,7 @@ class DeviceFitter {
   // kernel and reports a timed-out wait as NB_ERR_GPU.
   static constexpr int kMaxPosters = 8;
   struct Tally {
-    uint64_t requests = 0, sweeps = 0, cell_visits = 0, slot_cycles = 0, h2d = 0, d2h = 0;
+    uint64_t requests = 0, sweeps = 0, cell_visits = 0, sparse_visits = 0, slot_cycles = 0, h2d = 0, d2h = 0;
     int64_t first_ns = INT64_MAX, last_ns = INT64_MIN;  // earliest fit start, latest fit end
     int64_t wait_ns = 0;  // the clusters' waits for their tickets' requests
   };
@@ -102,6 +102,7 @@ class DeviceFitter {
   uint64_t requests() const { return requests_; }
   uint64_t sweeps() const { return sweeps_; }
   uint64_t cell_visits() const { return cell_visits_; }
+  uint64_t sparse_visits() const { return sparse_visits_; }
   uint64_t slot_cycles() const { return slot_cycles_; }
   // Zero-count groups the sweeps look up (0: every cell is swept).
   size_t tabled_groups() const { return tabled_groups_; }
@@ -161,7 +162,7 @@ class DeviceFitter {
   double* d_scratch_ = nullptr;
   int pgrid_ = 0;
   double device_ms_ = 0.0;
-  uint64_t launches_ = 0, requests_ = 0, sweeps_ = 0, cell_visits_ = 0, slot_cycles_ = 0;
+  uint64_t launches_ = 0, requests_ = 0, sweeps_ = 0, cell_visits_ = 0, sparse_visits_ = 0, slot_cycles_ = 0;
   int64_t first_ns_ = INT64_MAX, last_ns_ = INT64_MIN;
   int64_t wait_ns_ = 0;
   uint64_t h2d_bytes_ = 0, d2h_bytes_ = 0;

@@ -135,6 +135,11 @@ typedef struct nb_options {
                             zero-count tables (src/sc/zeros.rs) apply; 0 = use
                             them for categorical designs, as the reference's
                             CPU path does */
+  int32_t cold_inner;    /* warm start only: 1 = every inner fit starts its
+                            Newton loop cold, from (beta_start, 0), as the
+                            plain method's do; with warm_radius 1 and
+                            audit_percent 0 a warm search then differs from
+                            the plain one only in its start */
 } nb_options;
 
 /* Counters of one call (timings in milliseconds of host wall clock, device
@@ -163,6 +168,7 @@ typedef struct nb_stats {
   double ms_ticket_wait;    /* summed over the fits of stages two and three:
                                device time a cluster waited for its ticket's
                                request to be posted and read */
+  uint64_t sparse_visits;   /* the positive entries among cell_visits */
 } nb_stats;
 
 void nb_params_default(nb_params* params);
