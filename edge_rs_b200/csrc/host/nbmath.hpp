@@ -74,6 +74,14 @@ NB_HD double nb_from_bits(uint64_t u) {
 #endif
 }
 
+NB_HD double nb_abs(double x) {
+#ifdef __CUDA_ARCH__
+  return fabs(x);
+#else
+  return std::fabs(x);
+#endif
+}
+
 // 2^k for -1022 <= k <= 1023
 NB_HD double nb_pow2(int k) { return nb_from_bits(static_cast<uint64_t>(k + 1023) << 52); }
 
@@ -171,8 +179,8 @@ struct alignas(16) NbPair {
 };
 struct NbTableData {
   NbPair exp2_frac[256];   // {hi, lo} of 2^(j/256)
-  NbPair log_inv_hi[256];  // {inv_j, hi of -ln inv_j}
-  double log_lo[256];      // lo of -ln inv_j
+  NbPair log_inv_hi[257];  // {inv_j, hi of -ln inv_j}
+  double log_lo[257];      // lo of -ln inv_j
 };
 constexpr int kNbTableDoubles = static_cast<int>(sizeof(NbTableData) / sizeof(double));
 
@@ -186,12 +194,15 @@ NB_HD double nb_exp_tab(double x, const NbTableData* t) {
   const double inv_l = 0x1.71547652b82fep+8;    // 256 / ln 2
   const double l_hi = 0x1.62e42fef80000p-9;     // ln 2 / 256, 34 bits
   const double l_lo = 0x1.1cf79abc9e3b4p-44;
-  if (x > -707.0 && x < 707.0) {
+  if (nb_abs(x) < 707.0) {
     // The common range (NaN fails the test): the same steps as below with
-    // the special cases left out. n = rint(x * inv_l) is read from the
-    // shifter's low word instead of a conversion, (n - n mod 256) / 256 is an
-    // arithmetic shift, and 2^m stays normal (|m| <= 1020).
-    const double shifted = x * inv_l + 6755399441055744.0;  // 1.5 * 2^52
+    // the special cases left out. n = rint(x * inv_l), rounded once by the
+    // fused shifter, is read from the shifter's low word instead of a
+    // conversion, (n - n mod 256) / 256 is an arithmetic shift, and 2^m
+    // stays normal (|m| <= 1020), so the scaling adds m to er's exponent
+    // field (er is in [1/2, 2), the result normal: the same double as
+    // er * 2^m).
+    const double shifted = nb_fma(x, inv_l, 6755399441055744.0);  // 1.5 * 2^52
     const double n = shifted - 6755399441055744.0;
     double r = nb_fma(-n, l_hi, x);
     r = nb_fma(-n, l_lo, r);
@@ -202,7 +213,7 @@ NB_HD double nb_exp_tab(double x, const NbTableData* t) {
     const int ni = static_cast<int>(static_cast<uint32_t>(nb_bits(shifted)));
     const NbPair s = t->exp2_frac[ni & 255];
     const double er = s.a + nb_fma(s.a, q, s.b);
-    return er * nb_pow2(ni >> 8);
+    return nb_from_bits(nb_bits(er) + (static_cast<uint64_t>(static_cast<int64_t>(ni >> 8)) << 52));
   }
   if (!(x == x)) return x;                      // NaN
   if (x > 709.782712893384) return 1.0 / 0.0;  // overflow
@@ -232,15 +243,11 @@ NB_HD double nb_log_tab(double x, const NbTableData* t) {
     // same steps as below with the special cases left out, and e converted
     // to a double through the shifter.
     const uint64_t u = nb_bits(x);
-    int e = static_cast<int>(u >> 52) - 1023;
+    const int e = static_cast<int>(u >> 52) - 1023;
     const uint64_t f = u & 0x000fffffffffffffULL;
-    double m = nb_from_bits(f | 0x3ff0000000000000ULL);  // [1, 2)
-    int j = static_cast<int>((f + (1ULL << 43)) >> 44);
-    if (j == 256) {
-      j = 0;
-      e += 1;
-      m *= 0.5;
-    }
+    const double m = nb_from_bits(f | 0x3ff0000000000000ULL);  // [1, 2)
+    // j = 256 (m just below 2) has its own entry, inv = 1/2
+    const int j = static_cast<int>((f + (1ULL << 43)) >> 44);
     const NbPair c = t->log_inv_hi[j];
     const double r = nb_fma(m, c.a, -1.0);
     double p = nb_fma(r, 1.0 / 7.0, -1.0 / 6.0);
@@ -267,13 +274,8 @@ NB_HD double nb_log_tab(double x, const NbTableData* t) {
   const uint64_t u = nb_bits(x);
   e += static_cast<int>((u >> 52) & 0x7ff) - 1023;
   const uint64_t f = u & 0x000fffffffffffffULL;
-  double m = nb_from_bits(f | 0x3ff0000000000000ULL);  // [1, 2)
-  int j = static_cast<int>((f + (1ULL << 43)) >> 44);
-  if (j == 256) {
-    j = 0;
-    e += 1;
-    m *= 0.5;
-  }
+  const double m = nb_from_bits(f | 0x3ff0000000000000ULL);  // [1, 2)
+  const int j = static_cast<int>((f + (1ULL << 43)) >> 44);  // 0 .. 256
   const NbPair c = t->log_inv_hi[j];
   const double r = nb_fma(m, c.a, -1.0);
   double p = nb_fma(r, 1.0 / 7.0, -1.0 / 6.0);

@@ -14,7 +14,7 @@ def pytest_configure(config):
 
 
 def _build(target_dir):
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, target_dir)], check=True)
+    subprocess.run(["make", "-s", f"-j{os.cpu_count() or 1}", "-C", os.path.join(ROOT, target_dir)], check=True)
 
 
 @pytest.fixture(scope="session", autouse=True)

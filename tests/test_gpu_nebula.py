@@ -86,6 +86,20 @@ def test_synthetic_configs_match_the_oracle(name, genes, cells, k):
     assert dev.stats["requests"] > 0 and dev.stats["gpu_launches"] > 0
 
 
+@pytest.mark.parametrize("name,genes", [("c1", 6), ("c2", 10), ("c3", 5), ("c4", 6)])
+def test_configs_at_full_size_match_the_oracle(name, genes):
+    """A few genes of each benchmark configuration at its stated cell and
+    subject counts: c1 100,000 cells x 20 subjects (4 columns), c2 50,000 x 64
+    of 100-5,000 cells (8 columns, five varying within subjects, nnz over
+    three decades), c3 200,000 x 40 (8 columns), c4 100,000 x 100 (4 columns)."""
+    w = workloads.make(name, seed=21, n_genes=genes)
+    assert w.n_cells == workloads.CONFIGS[name]["n_cells"]
+    params = NebulaParams(method="HL")
+    dev = nebula_sparse_cuda(w.csr, w.subject, w.design, w.n_coef, w.offset, params)
+    ref, _ = of.nebula_sparse(w.csr, w.subject, w.design, w.n_coef, w.offset, params, threads=8)
+    compare_to_oracle(dev, ref, name)
+
+
 def test_results_are_reproducible_run_to_run():
     w = workloads.make("c1", seed=5, n_genes=8, n_cells=10000, n_subjects=12)
     params = NebulaParams(method="HL")

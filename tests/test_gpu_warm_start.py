@@ -6,7 +6,7 @@ workloads use seeds 100 and up).
   one's start does: the gain the learned part brings.
 - With every gene audited, the warm searches' objectives match the cold
   ones' (at most a few genes keep the cold result), and the fits agree with
-  the plain method's within the search's tolerance.
+  the plain method's as closely as plain runs from starts 1e-9 to 1e-3 apart.
 - The warm form does less device work than the plain one (fewer sweeps).
 """
 import numpy as np
@@ -21,41 +21,78 @@ pytestmark = pytest.mark.gpu
 
 @pytest.fixture(scope="module")
 def case():
-    w = workloads.make("c1", seed=77, n_genes=96, n_cells=20000, n_subjects=20)
+    w = workloads.make("c1", seed=77, n_genes=160, n_cells=20000, n_subjects=20)
     params = NebulaParams(method="HL")
     s = Session(w.csr, w.subject, w.design, w.n_coef, w.offset, params)
     plain = s.fit()
     feats, targets = examples(s, plain)
+    stage_one = s.features()[1]
     s.close()
-    return w, params, plain, feats, targets
+    # the search's reproducibility floor: the plain method (NLopt's radius,
+    # cold inner fits) from stage one's start moved by 1e-9, 1e-6 and 1e-3
+    # relative
+    floors = []
+    for delta in (1e-9, 1e-6, 1e-3):
+        points = np.zeros((w.n_genes, 2))
+        points[plain.gene_index, 0] = stage_one[:, 0] * (1.0 + delta)
+        points[plain.gene_index, 1] = stage_one[:, 1] * (1.0 - delta)
+        floors.append(nebula_sparse_cuda(w.csr, w.subject, w.design, w.n_coef, w.offset, params, warm_start=2,
+                                         warm_points=points, warm_radius=1.0, audit_percent=0, cold_inner=True))
+    return w, params, plain, feats, targets, floors
 
 
 GATE = 0.07  # the library drops predicted log-corrections smaller than this
+KEYS = ("coefficients", "subject_overdispersion", "cell_overdispersion")
 
 
-def assert_fits_agree(warm, plain):
-    """Warm and plain fits of the same genes agree within the search's
-    tolerance: the same genes kept; the same convergence codes, but for a
-    few genes whose final fit sits on the edge of the backtracking limit
-    and flips between success (1) and critical point (-10) with the last
-    digits of sigma and phi (the plain method at full radius flips the same
-    genes from a different start); and the coefficients, sigma^2 and phi
-    close (the two searches take different paths to the same optimum, so
-    they are not bitwise equal)."""
+def rel_err(a, b):
+    """|a - b| / max(|a|, |b|), entries within 1e-9 counting as zero."""
+    diff = np.abs(a - b)
+    scale = np.maximum(np.abs(a), np.abs(b))
+    return np.where(diff <= 1e-9, 0.0, diff / np.where(scale > 0, scale, 1.0))
+
+
+def gene_errors(fit, plain):
+    """Per gene, the largest relative error over beta, sigma^2 and phi."""
+    return np.max(np.column_stack([rel_err(getattr(fit, k), getattr(plain, k)).reshape(len(plain.gene_index), -1)
+                                   .max(axis=1) for k in KEYS]), axis=1)
+
+
+def assert_fits_agree(warm, plain, floors):
+    """Warm and plain fits of the same genes agree about as closely as plain
+    runs agree with each other: the plain method from a start moved by as
+    little as 1e-9 (`floors`) lands up to ~1e-4 away on beta, sigma^2 and phi
+    and flips a few convergence codes, since BOBYQA stops at a relative
+    resolution of ~1e-6 on an objective that jitters at that level. The warm
+    searches' inner fits start from the previous iterate, so their objective
+    jitters differently, and on a gene whose phi is barely identified the
+    warm optimum can sit a few times further out than the floor runs' worst.
+    Measured on this draw: 95th percentiles of ~2e-6 for the floor runs and
+    ~1.5e-5 for the warm fits, largest errors of ~1.5e-4 and ~6e-4. Bars, per
+    quantity (beta, sigma^2, phi): the 95th percentile of the warm errors
+    within three times the floor runs' largest 95th percentile, or 2e-5 (the
+    reference holds two implementations of this search to 1e-5 on sigma^2
+    and phi, src/sc/nebula.rs TOL_SUBJECT, TOL_CELL); the largest error
+    within ten times the floor runs' largest; the median below 1e-5; no more
+    genes off by over 1e-6 than twice the floor runs' most, plus two;
+    convergence codes that differ only between success (1) and critical
+    point (-10), on no more genes than twice the floor runs' most, plus two."""
     assert np.array_equal(warm.gene_index, plain.gene_index)
     differ = np.flatnonzero(warm.convergence != plain.convergence)
     flips = np.isin(warm.convergence[differ], (1, -10)) & np.isin(plain.convergence[differ], (1, -10))
     assert flips.all(), (differ, warm.convergence[differ], plain.convergence[differ])
-    assert differ.size <= max(1, len(plain.convergence) // 20), differ
-    rel = lambda a, b: np.abs(a - b) / np.maximum(np.abs(b), 1e-12)
-    coef = rel(warm.coefficients, plain.coefficients)
-    assert np.median(coef) < 1e-5 and np.quantile(coef, 0.99) < 1e-2, (np.median(coef), coef.max())
-    assert np.all(np.abs(warm.coefficients - plain.coefficients) < 1e-2 * (1.0 + np.abs(plain.coefficients)))
-    ok = ~plain.sigma_at_bound & (plain.subject_overdispersion > 1e-3)
-    assert np.median(rel(warm.subject_overdispersion[ok], plain.subject_overdispersion[ok])) < 1e-4
-    assert np.quantile(rel(warm.subject_overdispersion[ok], plain.subject_overdispersion[ok]), 0.95) < 1e-2
-    assert np.median(rel(warm.cell_overdispersion, plain.cell_overdispersion)) < 1e-4
-    assert np.quantile(rel(warm.cell_overdispersion, plain.cell_overdispersion), 0.95) < 1e-2
+    floor_flips = max(int(np.sum(f.convergence != plain.convergence)) for f in floors)
+    assert differ.size <= 2 * floor_flips + 2, (differ.size, floor_flips)
+    for key in KEYS:
+        e = rel_err(getattr(warm, key), getattr(plain, key))
+        f = [rel_err(getattr(fl, key), getattr(plain, key)) for fl in floors]
+        q95 = max(np.quantile(x, 0.95) for x in f)
+        assert np.quantile(e, 0.95) <= max(3.0 * q95, 2e-5), (key, np.quantile(e, 0.95), q95)
+        assert e.max() <= max(10.0 * max(x.max() for x in f), 1e-6), (key, e.max(), [x.max() for x in f])
+        assert np.median(e) < 1e-5, (key, np.median(e))
+    off = int(np.sum(gene_errors(warm, plain) > 1e-6))
+    floor_off = max(int(np.sum(gene_errors(fl, plain) > 1e-6)) for fl in floors)
+    assert off <= 2 * floor_off + 2, (off, floor_off)
 
 
 def start_errors(feats, targets):
@@ -92,7 +129,7 @@ def test_learned_start_costs_no_extra_evaluations(case):
     within about 1%: the learned start (warm_start 1) takes no more search
     evaluations than stage one's start with the same warm inner fits
     (warm_start 3)."""
-    w, params, _, _, _ = case
+    w, params, _, _, _, _ = case
     runs = {m: nebula_sparse_cuda(w.csr, w.subject, w.design, w.n_coef, w.offset, params, warm_start=m,
                                   audit_percent=0) for m in (1, 3)}
     assert runs[1].evaluations.sum() <= 1.03 * runs[3].evaluations.sum(), \
@@ -100,33 +137,33 @@ def test_learned_start_costs_no_extra_evaluations(case):
 
 
 def test_audited_warm_fits_match_the_plain_method(case):
-    w, params, plain, _, _ = case
+    w, params, plain, _, _, floors = case
     warm = nebula_sparse_cuda(w.csr, w.subject, w.design, w.n_coef, w.offset, params, warm_start=1,
                               audit_percent=100)
     searched = int((plain.evaluations > 0).sum())
     assert warm.stats["audited"] == searched
     assert warm.stats["refit_cold"] <= max(2, searched // 20), warm.stats["refit_cold"]
-    assert_fits_agree(warm, plain)
+    assert_fits_agree(warm, plain, floors)
 
 
 def test_default_audit_sample_fits_agree(case):
     """The default 5% audit: audited genes finish after both of their
     searches, in any order, and every gene's final fit is its own."""
-    w, params, plain, _, _ = case
+    w, params, plain, _, _, floors = case
     warm = nebula_sparse_cuda(w.csr, w.subject, w.design, w.n_coef, w.offset, params, warm_start=1)
     assert warm.stats["audited"] > 0
-    assert_fits_agree(warm, plain)
+    assert_fits_agree(warm, plain, floors)
 
 
 def test_warm_start_does_less_device_work(case):
-    w, params, plain, _, _ = case
+    w, params, plain, _, _, _ = case
     warm = nebula_sparse_cuda(w.csr, w.subject, w.design, w.n_coef, w.offset, params, warm_start=1)
     assert warm.stats["sweeps"] < 0.85 * plain.stats["sweeps"], (warm.stats["sweeps"], plain.stats["sweeps"])
     assert warm.stats["audited"] > 0
 
 
 def test_caller_supplied_starts(case):
-    w, params, plain, _, _ = case
+    w, params, plain, _, _, _ = case
     points = np.ones((w.n_genes, 2))
     points[plain.gene_index, 0] = plain.subject_overdispersion
     points[plain.gene_index, 1] = 1.0 / plain.cell_overdispersion
@@ -143,7 +180,7 @@ def test_narrow_initial_radius_saves_evaluations(case):
     radius (nb_options.warm_radius): markedly fewer evaluations than the same
     warm search at the full radius, with every gene audited and the fits
     still matching the plain method within the search's tolerance."""
-    w, params, plain, _, _ = case
+    w, params, plain, _, _, floors = case
     full = nebula_sparse_cuda(w.csr, w.subject, w.design, w.n_coef, w.offset, params, warm_start=1,
                               audit_percent=0, warm_radius=1.0)
     narrow = nebula_sparse_cuda(w.csr, w.subject, w.design, w.n_coef, w.offset, params, warm_start=1,
@@ -152,5 +189,16 @@ def test_narrow_initial_radius_saves_evaluations(case):
         (narrow.evaluations.sum(), full.evaluations.sum())
     searched = int((plain.evaluations > 0).sum())
     assert narrow.stats["refit_cold"] <= max(2, searched // 20), narrow.stats["refit_cold"]
-    assert_fits_agree(narrow, plain)
-    assert_fits_agree(full, plain)
+    assert_fits_agree(narrow, plain, floors)
+    assert_fits_agree(full, plain, floors)
+
+
+def test_stage_one_start_with_cold_inner_fits_is_the_plain_method(case):
+    """warm_start 3 (stage one's start), NLopt's radius, cold inner fits and
+    no audit is the plain method exactly: the floor arm above differs from
+    plain only in its start."""
+    w, params, plain, _, _, _ = case
+    same = nebula_sparse_cuda(w.csr, w.subject, w.design, w.n_coef, w.offset, params, warm_start=3,
+                              warm_radius=1.0, audit_percent=0, cold_inner=True)
+    for key in ("coefficients", "covariance", "subject_overdispersion", "cell_overdispersion", "convergence"):
+        assert np.array_equal(getattr(same, key), getattr(plain, key)), key
