@@ -99,6 +99,13 @@ PRODUCT_SIGNATURES = {
     "nb_glm_sc_test": (ctypes.c_int32, [c_double_p, c_double_p, ctypes.c_uint64, ctypes.c_uint64,
                                         c_double_p, c_double_p, c_double_p, c_double_p, c_double_p,
                                         c_double_p, c_double_p, ctypes.c_char_p, ctypes.c_size_t]),
+    "nb_glm_sc_test_cuda": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
+                                             c_double_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_char_p, ctypes.c_size_t]),
+    "nb_contract_krx_cuda": (ctypes.c_int32, [ctypes.c_int32, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32,
+                                              ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, c_double_p,
+                                              ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
     "nb_bobyqa_new": (ctypes.c_void_p, [c_double_p, c_double_p, c_double_p, ctypes.c_uint32,
                                         ctypes.c_double, ctypes.c_uint32]),
     "nb_bobyqa_new_scaled": (ctypes.c_void_p, [c_double_p, c_double_p, c_double_p, ctypes.c_uint32,

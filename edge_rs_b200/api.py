@@ -203,6 +203,61 @@ def glm_sc_test(coefficients, covariance, coef=None, contrast=None):
     return ScTestResult(*outs)
 
 
+def glm_sc_test_cuda(coefficients, covariance, coef=None, contrast=None):
+    """glm_sc_test on the device for fits held in HBM: `coefficients`
+    (n_genes x n_coef) and the packed `covariance` are CUDA float64 tensors;
+    returns an ScTestResult of CUDA tensors (nb_glm_sc_test_cuda)."""
+    import torch
+    lib = _ffi.product_library()
+    beta = coefficients.contiguous()
+    cov = covariance.contiguous()
+    if not (beta.is_cuda and cov.is_cuda) or beta.dtype != torch.float64 or cov.dtype != torch.float64:
+        raise NebulaError(2, "coefficients and covariance must be CUDA float64 tensors")
+    n_genes, n_coef = beta.shape
+    if contrast is None:
+        if coef is None or not 0 <= coef < n_coef:
+            raise NebulaError(13, f"coefficient {coef} is out of range for {n_coef}")
+        contrast = np.zeros(n_coef)
+        contrast[coef] = 1.0
+    c = np.ascontiguousarray(contrast, dtype=np.float64)
+    outs = [torch.empty(n_genes, dtype=torch.float64, device=beta.device) for _ in range(6)]
+    err = ctypes.create_string_buffer(256)
+    stream = torch.cuda.current_stream(beta.device).cuda_stream
+    rc = lib.nb_glm_sc_test_cuda(beta.data_ptr(), cov.data_ptr(), n_genes, n_coef, _ffi.ptr(c, ctypes.c_double),
+                                 *[o.data_ptr() for o in outs], ctypes.c_void_p(stream), err, len(err))
+    if rc != 0:
+        raise NebulaError(rc, err.value.decode(errors="replace"))
+    return ScTestResult(*outs)
+
+
+CONTRACT_VARIANTS = {0: "fp64_cuda_cores", 1: "fp32_cuda_cores", 2: "tf32_tensor_cores", 3: "split_bf16_tensor_cores"}
+
+
+def contract_krx_cuda(variant, design, weights):
+    """S[r] = sum_c weights[r, c] x_c x_c' packed (b (b + 1) / 2 + a for
+    a <= b) for CUDA float64 tensors design (n_cells x p, p <= 8) and
+    weights (R x n_cells, R <= 128), in one of CONTRACT_VARIANTS
+    (nb_contract_krx_cuda). Returns (S as a CUDA tensor, contraction ms,
+    ms with the operand conversions)."""
+    import torch
+    lib = _ffi.product_library()
+    x = design.contiguous()
+    w = weights.contiguous()
+    if not (x.is_cuda and w.is_cuda) or x.dtype != torch.float64 or w.dtype != torch.float64:
+        raise NebulaError(2, "design and weights must be CUDA float64 tensors")
+    n_cells, p = x.shape
+    r = w.shape[0]
+    out = torch.empty((r, p * (p + 1) // 2), dtype=torch.float64, device=x.device)
+    ms = np.zeros(2)
+    err = ctypes.create_string_buffer(256)
+    stream = torch.cuda.current_stream(x.device).cuda_stream
+    rc = lib.nb_contract_krx_cuda(int(variant), x.data_ptr(), n_cells, p, w.data_ptr(), r, out.data_ptr(),
+                                  _ffi.ptr(ms, ctypes.c_double), ctypes.c_void_p(stream), err, len(err))
+    if rc != 0:
+        raise NebulaError(rc, err.value.decode(errors="replace"))
+    return out, float(ms[0]), float(ms[1])
+
+
 class Session:
     """nb_session_create / nb_session_fit: inputs validated, stage one run and
     the data made resident on the device once; `fit()` runs stages two and

@@ -299,6 +299,41 @@ int32_t nb_glm_sc_test(const double* coefficients, const double* covariance,
                        double* log_p_value, double* fdr, char* err,
                        size_t err_len);
 
+/* nb_glm_sc_test on the device (src/sc/test.rs:96-200), for fits kept in
+ * HBM: coefficients (n_genes x n_coef, n_coef <= 8), the packed covariance
+ * and every output are DEVICE pointers (any output may be NULL); contrast is
+ * a host array of n_coef. Same arithmetic in the same order as
+ * nb_glm_sc_test; erfc and log are CUDA's, so p-values agree with the host's
+ * to a few ulps. The BH FDR sorts on the device (its scratch comes from the
+ * device's stream-ordered memory pool). Runs on the current device and
+ * `stream` (NULL: the default stream) and returns once the outputs are
+ * written. */
+int32_t nb_glm_sc_test_cuda(const double* coefficients,
+                            const double* covariance, uint64_t n_genes,
+                            uint64_t n_coef, const double* contrast,
+                            double* log_fc, double* se, double* z,
+                            double* p_value, double* log_p_value, double* fdr,
+                            void* stream, char* err, size_t err_len);
+
+/* The inner fit's Hessian contraction S_r = sum_c w_rc x_c x_c' for a batch
+ * of requests (the dense product of their cell weights with the Khatri-Rao
+ * square of the design; the reference's fused curvature assembly,
+ * src/gpu/pml_kernel.rs:350-515), in one of four arithmetics: 0 FP64 and
+ * 1 FP32 on CUDA cores, 2 TF32 and 3 split BF16 (hi.hi + hi.lo + lo.hi,
+ * FP32 accumulation) on the tensor cores (tcgen05.mma). design: device
+ * n_cells x n_coef FP64 (n_coef <= 8); weights: device n_requests x n_cells
+ * FP64 (n_requests <= 128); out: device n_requests x n_coef (n_coef + 1) / 2,
+ * entry b (b + 1) / 2 + a = sum_c w_rc x_ca x_cb for a <= b. ms_out (host,
+ * 2 doubles, may be NULL): device ms of the contraction kernel, and with the
+ * operand conversions. Scratch comes from the device's stream-ordered pool;
+ * returns once `out` is written. A precision study: the fits themselves
+ * keep this sum in FP64. */
+int32_t nb_contract_krx_cuda(int32_t variant, const double* design,
+                             uint64_t n_cells, uint32_t n_coef,
+                             const double* weights, uint32_t n_requests,
+                             double* out, double* ms_out, void* stream,
+                             char* err, size_t err_len);
+
 /* Reverse-communication BOBYQA as NLopt 2.7.1 runs it
  * (src/numeric/bobyqa.rs:141-560 BobyqaStepper::{new, ask, tell, result}). */
 typedef struct nb_bobyqa nb_bobyqa;
