@@ -97,6 +97,9 @@ def parse():
     ap.add_argument("--fit-batch", type=int, default=0,
                     help="instead of the bench: time launches of the fit kernel in batch mode, this many inner fits "
                          "of the workload's first gene per launch (the profiling workload)")
+    ap.add_argument("--contraction", action="store_true",
+                    help="instead of the bench: the Hessian contraction of config 3's final fits in FP64, FP32, "
+                         "TF32 and split BF16 (tensor cores), with the errors it carries into se and log p")
     ap.add_argument("--zero-tables", action="store_true",
                     help="instead of the bench: the plain method on a categorical design (intercept and a "
                          "subject-level binary) of the default size, with the zero-count tables and with every "
@@ -469,6 +472,125 @@ def zero_tables(args):
                       "tables_vs_dense": compare_fits(a, b)}), flush=True)
 
 
+def contraction_study(args):
+    """The inner fit's Hessian contraction at the workload's shape (default
+    config 3: 200,000 cells, 40 subjects, 8 columns) in four arithmetics
+    (nb_contract_krx_cuda): FP64 / FP32 on CUDA cores, TF32 / split BF16 on
+    the tensor cores. The weights are those of each gene's final fit: the
+    plain method fits up to 128 genes, the subjects' log w are solved at the
+    fitted beta, sigma and phi, and w_c = (gamma + y_c) e_c / (e_c + gamma)^2.
+    For each variant: the contraction's error against the FP64 one, the
+    information matrix it gives (gamma S minus the subjects' Schur terms,
+    those in FP64), and the errors that carries into the standard errors and
+    the Wald log p-values; its device time and rate. Prints one JSON line."""
+    import torch
+    from edge_rs_b200 import glm_sc_test
+    from edge_rs_b200.api import CONTRACT_VARIANTS, Session, contract_krx_cuda
+    cfg = args.config if args.config != "c1" else "c3"
+    n_genes = min(args.genes or 128, 128)
+    work = workloads.make(cfg, seed=1000, n_genes=n_genes)
+    s = Session(work.csr, work.subject, work.design, work.n_coef, work.offset, NebulaParams(method="HL"))
+    fit = s.fit()
+    s.close()
+    dev = torch.device("cuda")
+    kept = fit.gene_index
+    R, N, p = len(kept), work.n_cells, work.n_coef
+    X = torch.from_numpy(work.design).to(dev)
+    subj = torch.from_numpy(work.subject.astype(np.int64)).to(dev)
+    K = int(work.subject.max()) + 1
+    Y = torch.zeros((R, N), dtype=torch.float64, device=dev)
+    for r, g in enumerate(kept):
+        lo, hi = int(work.indptr[g]), int(work.indptr[g + 1])
+        Y[r, torch.from_numpy(work.indices[lo:hi].astype(np.int64)).to(dev)] = torch.from_numpy(work.data[lo:hi]).to(dev)
+    beta = torch.from_numpy(fit.coefficients).to(dev)
+    eta0 = beta @ X.T + torch.log(torch.from_numpy(work.offset).to(dev))[None, :]
+    sig2 = torch.from_numpy(fit.subject_overdispersion).to(dev)[:, None]
+    gam = (1.0 / torch.from_numpy(fit.cell_overdispersion).to(dev))[:, None]
+    exps = 1.0 + sig2
+    alpha, lam = 1.0 / (exps - 1.0), 1.0 / (torch.sqrt(exps) * (exps - 1.0))
+
+    def seg(v):  # per-subject sums of an R x N array
+        return torch.zeros((R, K), dtype=torch.float64, device=dev).index_add_(1, subj, v)
+
+    lw = torch.zeros((R, K), dtype=torch.float64, device=dev)
+    for _ in range(100):  # each subject's log w at the fitted beta (Newton on the penalised likelihood)
+        e = torch.exp(eta0 + lw[:, subj])
+        t = e + gam
+        score = seg(Y - (Y + gam) * e / t) + alpha - lam * torch.exp(lw)
+        curv = gam * seg((gam + Y) * e / (t * t)) + lam * torch.exp(lw)
+        step = score / curv
+        lw = lw + step
+        if float(step.abs().max()) < 1e-14:
+            break
+    e = torch.exp(eta0 + lw[:, subj])
+    t = e + gam
+    W = (gam + Y) * e / (t * t)
+    bounds = np.concatenate([[0], np.cumsum(work.truth["sizes"])])
+    vwb = torch.stack([gam * (W[:, a:b] @ X[a:b]) for a, b in zip(bounds[:-1], bounds[1:])], dim=1)  # R x K x p
+    vw = gam * seg(W) + lam * torch.exp(lw)
+    schur = torch.einsum("rka,rkb->rab", vwb / vw[:, :, None], vwb)
+    pairs = [(a, b) for b in range(p) for a in range(b + 1)]
+
+    def information(S):
+        full = torch.zeros((R, p, p), dtype=torch.float64, device=dev)
+        for j, (a, b) in enumerate(pairs):
+            full[:, a, b] = S[:, j]
+            full[:, b, a] = S[:, j]
+        return gam[:, :, None] * full - schur
+
+    def wald(info):
+        cov = torch.linalg.inv(info).cpu().numpy()
+        packed = np.stack([cov[:, a, b] for a, b in pairs], axis=1)
+        se = np.sqrt(np.stack([cov[:, j, j] for j in range(p)], axis=1))
+        logp = np.stack([glm_sc_test(fit.coefficients, packed, coef=c).log_p_value for c in range(1, p)], axis=1)
+        return packed, se, logp
+
+    out = {}
+    base = None
+    ref_dgemm = None
+    for v, name in CONTRACT_VARIANTS.items():
+        ms = []
+        for _ in range(args.warmup + args.steps):
+            S, m_kernel, m_total = contract_krx_cuda(v, X, W)
+            ms.append((m_kernel, m_total))
+        m_kernel = float(np.median([a for a, _ in ms[args.warmup:]]))
+        m_total = float(np.median([b for _, b in ms[args.warmup:]]))
+        packed, se, logp = wald(information(S))
+        se = se[:, 1:]  # the slopes: the intercept's se depends on the design's centring
+        flop = 2.0 * R * N * len(pairs) * (3 if v == 3 else 1)
+        entry = {"ms_kernel": m_kernel, "ms_with_conversions": m_total,
+                 "tflops": flop / (m_kernel * 1e-3) / 1e12}
+        if base is None:
+            base = (S, se, logp)
+            # sanity: FP64 against a cuBLAS DGEMM of the same product, and the
+            # recomputed covariance against the fit's own
+            kr = torch.stack([X[:, a] * X[:, b] for a, b in pairs], dim=1)
+            ref_dgemm = W @ kr
+            entry["vs_dgemm_max_rel"] = float(((S - ref_dgemm).abs() / ref_dgemm.abs().amax(1, keepdim=True)).max())
+            # the slopes' variances (the fit reports the intercept's in centred
+            # coordinates, these are in the design's own)
+            diag = [b * (b + 1) // 2 + b for b in range(1, p)]
+            entry["slope_variance_vs_fit"] = rel_errors(packed[:, diag], fit.covariance[:, diag], 0.0)
+        else:
+            S0, se0, logp0 = base
+            entry["contraction_max_rel"] = float(((S - S0).abs() / S0.abs().amax(1, keepdim=True)).max())
+            entry["se_slopes"] = rel_errors(se, se0, 0.0)
+            entry["log_p"] = rel_errors(logp, logp0, 1e-6)
+        out[name] = entry
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            peaks = json.load(fh)
+    except Exception:
+        pass
+    print(json.dumps({"mode": "contraction", "config": {"workload": f"{cfg}: {R} genes' final fits x {N} cells, "
+                                                                    f"{K} subjects, {p} columns ({len(pairs)} "
+                                                                    "Khatri-Rao columns)"},
+                      "variants": out, "measured_peaks": peaks,
+                      "beta_sigma2_phi": "unchanged at the fit's fixed point: the contraction steers Newton "
+                                         "only; the value, gradient and log-determinant stay FP64"}), flush=True)
+
+
 def fit_batch(args):
     """R inner fits of one c1-shaped gene per launch through nb_opt_pml_cuda:
     the per-fit code of the persistent launch (fit_one) in the batch kernel,
@@ -508,6 +630,9 @@ def main():
         return
     if args.zero_tables:
         zero_tables(args)
+        return
+    if args.contraction:
+        contraction_study(args)
         return
     if args.impl == "reference":  # rank 0 alone times the CPU path; other ranks exit
         reference_arm(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), None)

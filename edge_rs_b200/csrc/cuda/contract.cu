@@ -126,11 +126,25 @@ __device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity) {
   return false;
 }
 
+constexpr int kStages = 4;  // operand tiles in flight per CTA
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // One CTA: requests 0..kM-1 against the Khatri-Rao rows 0..kN-1 over the
-// K tiles [tile0, tile1) of kRowBytes per row; FP32 partial sums into
+// K tiles [t0, t1) of kRowBytes per row; FP32 partial sums into
 // partial[blockIdx.x][kM][kN]. Operands are row-major in global memory,
 // `row_bytes` apart: A (requests) a_hi / a_lo, B (pairs) b_hi / b_lo (the
-// lo halves unused for TF32). *status = 1 if a wait ran out.
+// lo halves unused for TF32). kStages tiles are in flight: the threads copy
+// tile i + kStages - 1 (cp.async) while the tensor cores multiply tile i;
+// a stage is refilled once the MMAs that read it have completed (its
+// mbarrier). *status = 1 if a wait ran out.
 template <bool TF32>
 __global__ void __launch_bounds__(kThreads, 1)
     contract_tc(const char* __restrict__ a_hi, const char* __restrict__ a_lo, const char* __restrict__ b_hi,
@@ -139,15 +153,17 @@ __global__ void __launch_bounds__(kThreads, 1)
   extern __shared__ __align__(1024) unsigned char smem[];
   constexpr uint32_t kLboA = (kM / 8) * 128, kLboB = (kN / 8) * 128;
   constexpr uint32_t kABytes = kM * kRowBytes, kBBytes = kN * kRowBytes;
-  unsigned char* sa_hi = smem;
-  unsigned char* sa_lo = smem + kABytes;
-  unsigned char* sb_hi = smem + 2 * kABytes;
-  unsigned char* sb_lo = smem + 2 * kABytes + kBBytes;
-  __shared__ __align__(8) unsigned long long mbar;
+  constexpr uint32_t kStageBytes = (TF32 ? 1 : 2) * (kABytes + kBBytes);
+  __shared__ __align__(8) unsigned long long mbar[kStages];
   __shared__ uint32_t tmem_base;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint64_t t0 = blockIdx.x * tiles_per_cta;
   const uint64_t t1 = t0 + tiles_per_cta < tiles ? t0 + tiles_per_cta : tiles;
+  const uint64_t n_tiles = t1 > t0 ? t1 - t0 : 0;
+  const uint32_t base = smem_u32(smem);
+  // stage s: A hi, B hi, then (split BF16) A lo, B lo
+  auto a_at = [&](int st, int lo) { return base + st * kStageBytes + (lo ? kABytes + kBBytes : 0); };
+  auto b_at = [&](int st, int lo) { return base + st * kStageBytes + kABytes + (lo ? kABytes + kBBytes : 0); };
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
                  "r"(kTmemCols)
@@ -155,7 +171,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)) : "memory");
+    for (int st = 0; st < kStages; ++st)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[st])) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -163,32 +180,44 @@ __global__ void __launch_bounds__(kThreads, 1)
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base;
   const uint32_t idesc = instr_desc<TF32>();
-  const uint32_t bar = smem_u32(&mbar);
-  uint32_t phase = 0;
-  bool ok = true, pending = false;  // pending: MMAs committed and not yet waited for
-  for (uint64_t t = t0; t < t1; ++t) {
-    if (pending) {  // the previous tile's MMAs still read shared memory
-      ok = __syncthreads_and(mbar_wait(bar, phase)) != 0;  // every thread takes the same branch
+  // copies tile t0 + i into stage i % kStages (16-byte chunk c of a row's
+  // tile is K chunk c: row group (row / 8) at 128-byte steps, K chunks kLbo apart)
+  auto load = [&](uint64_t i) {
+    if (i < n_tiles) {
+      const int st = static_cast<int>(i % kStages);
+      const uint64_t k_off = (t0 + i) * kRowBytes;
+      for (int c = tid; c < kM * 8; c += kThreads) {
+        const int m = c >> 3, kc = c & 7;
+        const uint32_t dst = static_cast<uint32_t>(kc) * kLboA + static_cast<uint32_t>(m >> 3) * 128 + (m & 7) * 16;
+        const uint64_t src = static_cast<uint64_t>(m) * row_bytes + k_off + kc * 16;
+        cp_async16(a_at(st, 0) + dst, a_hi + src);
+        if (!TF32) cp_async16(a_at(st, 1) + dst, a_lo + src);
+      }
+      for (int c = tid; c < kN * 8; c += kThreads) {
+        const int n = c >> 3, kc = c & 7;
+        const uint32_t dst = static_cast<uint32_t>(kc) * kLboB + static_cast<uint32_t>(n >> 3) * 128 + (n & 7) * 16;
+        const uint64_t src = static_cast<uint64_t>(n) * row_bytes + k_off + kc * 16;
+        cp_async16(b_at(st, 0) + dst, b_hi + src);
+        if (!TF32) cp_async16(b_at(st, 1) + dst, b_lo + src);
+      }
+    }
+    cp_async_commit();  // one group per tile, empty past the end
+  };
+  for (int i = 0; i < kStages - 1; ++i) load(static_cast<uint64_t>(i));
+  uint32_t uses[kStages] = {};  // completed MMA groups per stage: the parity to wait for
+  bool ok = true;
+  uint64_t issued = 0;  // tiles whose MMAs have been issued
+  for (uint64_t i = 0; i < n_tiles; ++i) {
+    const int st = static_cast<int>(i % kStages);
+    // the stage that tile i + kStages - 1 refills last held tile i - 1
+    if (i > 0) {
+      const int prev = static_cast<int>((i - 1) % kStages);
+      ok = __syncthreads_and(mbar_wait(smem_u32(&mbar[prev]), uses[prev] & 1u)) != 0;
       if (!ok) break;
-      phase ^= 1u;
-      pending = false;
+      ++uses[prev];
     }
-    // stage: 16-byte chunk i of the tile is row i / 8, K chunk i % 8
-    const uint64_t k_off = t * kRowBytes;
-    for (int i = tid; i < kM * 8; i += kThreads) {
-      const int m = i >> 3, kc = i & 7;
-      const uint32_t dst = static_cast<uint32_t>(kc) * kLboA + static_cast<uint32_t>(m >> 3) * 128 + (m & 7) * 16;
-      const uint64_t src = static_cast<uint64_t>(m) * row_bytes + k_off + kc * 16;
-      *reinterpret_cast<int4*>(sa_hi + dst) = __ldg(reinterpret_cast<const int4*>(a_hi + src));
-      if (!TF32) *reinterpret_cast<int4*>(sa_lo + dst) = __ldg(reinterpret_cast<const int4*>(a_lo + src));
-    }
-    for (int i = tid; i < kN * 8; i += kThreads) {
-      const int n = i >> 3, kc = i & 7;
-      const uint32_t dst = static_cast<uint32_t>(kc) * kLboB + static_cast<uint32_t>(n >> 3) * 128 + (n & 7) * 16;
-      const uint64_t src = static_cast<uint64_t>(n) * row_bytes + k_off + kc * 16;
-      *reinterpret_cast<int4*>(sb_hi + dst) = __ldg(reinterpret_cast<const int4*>(b_hi + src));
-      if (!TF32) *reinterpret_cast<int4*>(sb_lo + dst) = __ldg(reinterpret_cast<const int4*>(b_lo + src));
-    }
+    load(i + kStages - 1);
+    cp_async_wait<kStages - 1>();  // this thread's copies of tile i have landed
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (tid == 0) {
@@ -196,31 +225,37 @@ __global__ void __launch_bounds__(kThreads, 1)
       // four MMA K steps of two 16-byte chunks each (16 BF16 or 8 TF32 values)
 #pragma unroll
       for (int step = 0; step < 4; ++step) {
-        const uint32_t first = (t == t0 && step == 0) ? 0u : 1u;
-        const uint64_t da_hi = smem_desc(smem_u32(sa_hi) + 2 * step * kLboA, kLboA, 128);
-        const uint64_t db_hi = smem_desc(smem_u32(sb_hi) + 2 * step * kLboB, kLboB, 128);
-        mma<TF32>(tmem, da_hi, db_hi, idesc, first);
+        const uint32_t acc = (i == 0 && step == 0) ? 0u : 1u;
+        const uint64_t da_hi = smem_desc(a_at(st, 0) + 2 * step * kLboA, kLboA, 128);
+        const uint64_t db_hi = smem_desc(b_at(st, 0) + 2 * step * kLboB, kLboB, 128);
+        mma<TF32>(tmem, da_hi, db_hi, idesc, acc);
         if (!TF32) {
-          const uint64_t da_lo = smem_desc(smem_u32(sa_lo) + 2 * step * kLboA, kLboA, 128);
-          const uint64_t db_lo = smem_desc(smem_u32(sb_lo) + 2 * step * kLboB, kLboB, 128);
+          const uint64_t da_lo = smem_desc(a_at(st, 1) + 2 * step * kLboA, kLboA, 128);
+          const uint64_t db_lo = smem_desc(b_at(st, 1) + 2 * step * kLboB, kLboB, 128);
           mma<TF32>(tmem, da_hi, db_lo, idesc, 1u);
           mma<TF32>(tmem, da_lo, db_hi, idesc, 1u);
         }
       }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(&mbar[st]))
                    : "memory");
     }
-    pending = true;
+    issued = i + 1;
   }
-  if (pending && ok) ok = __syncthreads_and(mbar_wait(bar, phase)) != 0;
-  if (!ok) mbar_wait(bar, phase);  // once more, bounded, for the MMAs in flight before freeing their memory
+  cp_async_wait<0>();
+  // the last tile's MMAs (or, after a failed wait, the ones in flight: once more, bounded)
+  if (issued > 0) {
+    const int last = static_cast<int>((issued - 1) % kStages);
+    const bool done = mbar_wait(smem_u32(&mbar[last]), uses[last] & 1u);
+    ok = __syncthreads_and(ok && done) != 0;
+  }
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   __syncthreads();
   float* out = partial + static_cast<uint64_t>(blockIdx.x) * kM * kN;
   const int row = warp * 32 + lane;
   if (!ok) {
     if (tid == 0) atomicExch(status, 1);
-  } else if (t0 >= t1) {
+  } else if (n_tiles == 0) {
     for (int c = 0; c < kN; ++c) out[row * kN + c] = 0.0f;
   } else {
     // each warp reads its 32 lanes (rows) of the accumulator, 16 columns at a time
@@ -388,7 +423,7 @@ NB_API int32_t nb_contract_krx_cuda(int32_t variant, const double* design, uint6
   if (tc) {
     const uint64_t tiles = n_pad / kt;
     const uint64_t per = (tiles + ctas - 1) / ctas;
-    const size_t smem = 2 * (static_cast<size_t>(kM) + kN) * kRowBytes;
+    const size_t smem = static_cast<size_t>(kStages) * (tf32 ? 1 : 2) * (kM + kN) * kRowBytes;
     const char* ah = tf32 ? reinterpret_cast<const char*>(a32) : reinterpret_cast<const char*>(a_hi);
     const char* al = tf32 ? nullptr : reinterpret_cast<const char*>(a_lo);
     const char* bh = tf32 ? reinterpret_cast<const char*>(b32) : reinterpret_cast<const char*>(b_hi);
