@@ -77,7 +77,8 @@ __global__ void __launch_bounds__(kMlpThreads) mlp_predict_kernel(const float* _
   extern __shared__ float sh[];
   float* w = sh;
   float* rows = sh + kParams;
-  for (int p = threadIdx.x; p < kParams; p += blockDim.x) w[p] = params[p];
+  // the weights as BF16 values (mlp_layout.hpp), FP32 accumulation
+  for (int p = threadIdx.x; p < kParams; p += blockDim.x) w[p] = is_weight(p) ? bf16_round(params[p]) : params[p];
   __syncthreads();
   for (int base = blockIdx.x * kTile; base < n; base += gridDim.x * kTile) {
     const int s = base + static_cast<int>(threadIdx.x);

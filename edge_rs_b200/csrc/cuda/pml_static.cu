@@ -28,8 +28,11 @@
 //
 // Set-up: the first call on a device (the calling thread's current device)
 // looks up the array's device address with cudaGetSymbolAddress and the SM
-// count, and caches both for that device; make that first call before any
-// stream capture begins.
+// count, and caches both for that device for the life of the process; calls
+// after a cudaDeviceReset of that device are not supported (the module's
+// array may then sit elsewhere). Every call is blocking (it reads a status
+// word back and synchronises its stream before returning), so no call can be
+// made while a stream is being captured.
 #include <cuda_runtime.h>
 
 #include <algorithm>

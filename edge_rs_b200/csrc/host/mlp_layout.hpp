@@ -14,6 +14,9 @@
 // number of samples, with w = (1, 1, 0.25).
 #pragma once
 
+#include <cstdint>
+#include <cstring>
+
 namespace nebula {
 namespace mlp {
 
@@ -35,6 +38,38 @@ constexpr int kTrained = kInMean;        // parameters the optimiser updates
 __host__ __device__
 #endif
 constexpr float loss_weight(int o) { return o == kOut - 1 ? 0.25f : 1.0f; }
+
+// Inference takes the weight matrices W1, W2, W3 as BF16 values (8-bit
+// significand, rounded to nearest even from the FP32 parameters); biases and
+// the input normalisation stay FP32, and every sum accumulates in FP32.
+// Training updates FP32 parameters.
+#ifdef __CUDACC__
+__host__ __device__
+#endif
+inline bool is_weight(int p) {
+  return (p >= kW1 && p < kB1) || (p >= kW2 && p < kB2) || (p >= kW3 && p < kB3);
+}
+
+#ifdef __CUDACC__
+__host__ __device__
+#endif
+inline float bf16_round(float v) {
+  uint32_t u;
+#ifdef __CUDA_ARCH__
+  u = __float_as_uint(v);
+#else
+  std::memcpy(&u, &v, 4);
+#endif
+  u += 0x7FFFu + ((u >> 16) & 1u);  // finite inputs: round to nearest, ties to even
+  u &= 0xFFFF0000u;
+#ifdef __CUDA_ARCH__
+  return __uint_as_float(u);
+#else
+  float r;
+  std::memcpy(&r, &u, 4);
+  return r;
+#endif
+}
 
 }  // namespace mlp
 }  // namespace nebula

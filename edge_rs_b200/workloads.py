@@ -85,8 +85,12 @@ def subject_sizes(rng, n_cells, n_subjects, kind):
 
 
 def make(name="c1", seed=0, n_genes: Optional[int] = None, n_cells: Optional[int] = None,
-         n_subjects: Optional[int] = None, sigma_log_sd=0.5, phi_log_sd=0.5, chunk=64):
-    """Draws one workload; the named configuration may be shrunk for tests."""
+         n_subjects: Optional[int] = None, sigma_log_sd=0.5, phi_log_sd=0.5, chunk=64,
+         gene_seed: Optional[int] = None):
+    """Draws one workload; the named configuration may be shrunk for tests.
+    gene_seed: draw the genes from their own stream (the cells, subjects and
+    design still from `seed`), so that workloads drawn with one seed and
+    different gene seeds share their cells and can be concatenated."""
     cfg = dict(CONFIGS[name])
     G = n_genes or cfg["n_genes"]
     N = n_cells or cfg["n_cells"]
@@ -108,6 +112,8 @@ def make(name="c1", seed=0, n_genes: Optional[int] = None, n_cells: Optional[int
     design = np.column_stack(cols)
     p = design.shape[1]
     lib = np.exp(rng.normal(np.log(2000.0), 0.3, N))
+    if gene_seed is not None:
+        rng = np.random.default_rng([seed, gene_seed])
     kind, a, b = cfg["intercept"]
     intercept = rng.normal(a, b, G) if kind == "normal" else rng.uniform(a, b, G)
     beta = np.zeros((G, p))

@@ -236,8 +236,10 @@ int32_t nb_opt_pml_cuda(const double* design, const double* offset,
  * nothing. Limits: at most 2048 requests and 8192 subjects per call, else
  * NB_ERR_INVALID_ARGUMENT before any launch. Runs on the calling thread's
  * current device and `stream` (NULL: the default stream), and returns once
- * the outputs are written. The first call on a device looks up the array's
- * address; make it before any stream capture. All calls on a device share
+ * the outputs are written: it is blocking and cannot be made during stream
+ * capture. The first call on a device looks up the array's address and keeps
+ * it for the process; calls after cudaDeviceReset on that device are not
+ * supported. All calls on a device share
  * the array: calls whose GPU work overlaps race, so issue them one at a
  * time. */
 int32_t nb_opt_pml_cuda_noalloc(const double* design, const double* offset,
@@ -268,7 +270,10 @@ int32_t nb_opt_pml_cuda_noalloc(const double* design, const double* offset,
 void nb_mlp_init(uint64_t seed, float* params);
 /* The built-in network warm_start = 1 uses when mlp_weights is NULL. */
 void nb_mlp_builtin(float* params);
-/* out: n x NB_MLP_OUTPUTS predictions for n x NB_MLP_FEATURES features. */
+/* out: n x NB_MLP_OUTPUTS predictions for n x NB_MLP_FEATURES features.
+ * Inference takes the weight matrices as BF16 values (rounded to nearest
+ * even from `params`), biases and normalisation in FP32, FP32 accumulation;
+ * training (below) updates FP32 parameters. */
 int32_t nb_mlp_predict_cuda(const float* params, const float* features,
                             uint64_t n, float* out, char* err, size_t err_len);
 /* The loss over n samples (targets n x NB_MLP_OUTPUTS) and its gradient

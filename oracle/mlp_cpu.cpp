@@ -46,10 +46,14 @@ void forward(const float* w, const float* x, Pass* p) {
 
 }  // namespace
 
+// Inference, as nb_mlp_predict_cuda runs it: the weight matrices as BF16
+// values (mlp_layout.hpp).
 ORACLE_API void oracle_mlp_predict(const float* params, const float* features, uint64_t n, double* out) {
+  float q[kParams];
+  for (int i = 0; i < kParams; ++i) q[i] = is_weight(i) ? bf16_round(params[i]) : params[i];
   for (uint64_t s = 0; s < n; ++s) {
     Pass p;
-    forward(params, features + s * kIn, &p);
+    forward(q, features + s * kIn, &p);
     for (int o = 0; o < kOut; ++o) out[s * kOut + o] = p.y[o];
   }
 }
