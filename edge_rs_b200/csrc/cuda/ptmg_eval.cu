@@ -29,9 +29,9 @@ int launch_ptmg_queue(const GeneData& d, const PtmgQueue& queue, double* scratch
   return o.launch(d, queue, scratch, grid, static_cast<cudaStream_t>(stream));
 }
 
-int ptmg_blocks_per_sm(int n_subjects, int n_coef, int n_varying) {
+int ptmg_resident_ctas(int n_subjects, int n_coef, int n_varying) {
   const PtmgOps o = ops(n_coef, n_varying);
-  return o.blocks ? o.blocks(n_subjects) : 0;
+  return o.resident ? o.resident(n_subjects) : 0;
 }
 
 size_t ptmg_scratch_doubles(int n_subjects, int n_coef, int n_varying) {

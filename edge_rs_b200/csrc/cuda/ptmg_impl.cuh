@@ -32,6 +32,7 @@
 // sums live in a per-CTA global scratch region (L2-resident).
 #pragma once
 
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -44,6 +45,8 @@
 namespace nebula {
 namespace device {
 namespace {
+
+namespace cg = cooperative_groups;
 
 // The full per-subject row of pass two (stage_one.hpp).
 template <int NB>
@@ -64,7 +67,13 @@ struct RDims {
   static constexpr int W = kBq + T;
 };
 
-constexpr int ptmg_threads(int nb, int nv) { return ptmg_warps(nb, nv) * 32; }
+// A request's W warp ranges are served by a thread-block cluster of W / 4
+// CTAs of four warps each (ptmg_cluster), spread over as many SMs: CTA rank r
+// takes ranges [4 r, 4 r + 4). The tree, and so every sum, is the same as
+// one CTA of W warps would take.
+constexpr int kPtmgCtaWarps = 4;
+constexpr int kPtmgCtaThreads = kPtmgCtaWarps * 32;
+constexpr int ptmg_cluster(int nb, int nv) { return ptmg_warps(nb, nv) / kPtmgCtaWarps; }
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -194,21 +203,29 @@ struct PtmgCta {
   uint32_t* fid;     // K + 1
   uint32_t* wcells;  // ptmg_warps + 1
   int32_t* vpos;     // kMaxCoef: each column's index among the varying ones, or -1
-  double* slots;     // this CTA's scratch: warp and subject pieces
-  double* reduced;   // this CTA's scratch: K reduced pass-two rows
+  double* slots;     // the cluster's scratch: warp and subject pieces
+  double* reduced;   // the cluster's scratch: K reduced pass-two rows
+  int rank, size;    // this CTA's place in its cluster
 };
 
+__device__ __forceinline__ void cluster_sync(const PtmgCta& c) {
+  if (c.size > 1) cg::this_cluster().sync();  // barrier.cluster: release / acquire at cluster scope
+  else __syncthreads();
+}
+
 // One pass through the tree: dense pieces into slots[(s + warp) * stride],
-// sparse pieces into slots[(K + W + s) * stride] (W = ptmg_warps), then per subject
-// out[s * out_stride + v] = 0 + dense pieces (warp order) + sparse piece.
-// Lanes take two cells (r, r + 32) or entries per iteration; each lane's
-// partials still take them in its sequential order.
+// sparse pieces into slots[(K + W + s) * stride] (W = ptmg_warps; warp is the
+// range's index over the cluster), then per subject
+// out[s * out_stride + v] = 0 + dense pieces (warp order) + sparse piece,
+// by every CTA of the cluster (`all_combine`) or by rank 0 alone. Lanes take
+// two cells (r, r + 32) or entries per iteration; each lane's partials still
+// take them in its sequential order.
 template <int NB, int NV, int PASS, int N>
 __device__ void tree_pass(const GeneData& d, const PtmgCta& c, int gene, const double* beta, double gamma,
-                          const int* vc, int stride, double* out, int out_stride) {
+                          const int* vc, int stride, double* out, int out_stride, bool all_combine) {
   const int K = d.n_subjects;
   constexpr int W = ptmg_warps(NB, NV);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int warp = c.rank * kPtmgCtaWarps + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   constexpr int NX = NV > 0 ? NV : 1;
   const int c_begin = static_cast<int>(c.wcells[warp]), c_end = static_cast<int>(c.wcells[warp + 1]);
   if (c_begin < c_end) {
@@ -268,18 +285,20 @@ __device__ void tree_pass(const GeneData& d, const PtmgCta& c, int gene, const d
     }
     reduce_to<N>(acc, c.slots + (K + W + s) * stride, lane);
   }
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < K * N; idx += blockDim.x) {
-    const int s = idx / N, v = idx - s * N;
-    const uint32_t a0 = c.fid[s], a1 = c.fid[s + 1];
-    double total = 0.0;
+  cluster_sync(c);  // every CTA's pieces are in the scratch (read past L1)
+  if (all_combine || c.rank == 0) {
+    for (int idx = threadIdx.x; idx < K * N; idx += blockDim.x) {
+      const int s = idx / N, v = idx - s * N;
+      const uint32_t a0 = c.fid[s], a1 = c.fid[s + 1];
+      double total = 0.0;
 #pragma unroll
-    for (int w = 0; w < W; ++w)
-      if (c.wcells[w] < a1 && c.wcells[w + 1] > a0) total += c.slots[(s + w) * stride + v];
-    total += c.slots[(K + W + s) * stride + v];
-    out[s * out_stride + v] = total;
+      for (int w = 0; w < W; ++w)
+        if (c.wcells[w] < a1 && c.wcells[w + 1] > a0) total += __ldcg(c.slots + (s + w) * stride + v);
+      total += __ldcg(c.slots + (K + W + s) * stride + v);
+      out[s * out_stride + v] = total;
+    }
   }
-  __syncthreads();
+  cluster_sync(c);  // no CTA refills the pieces before every combine has read them
 }
 
 // Subject s's full pass-two row (PDims<NB>) from its reduced one, element x.
@@ -327,8 +346,10 @@ __device__ PtmgCta ptmg_setup(const GeneData& d, double* smem, double* scratch) 
       if (d.varying[j] == static_cast<int>(threadIdx.x)) pos = j;
     c.vpos[threadIdx.x] = pos;
   }
+  c.size = ptmg_cluster(NB, NV);
+  c.rank = c.size > 1 ? static_cast<int>(cg::this_cluster().block_rank()) : 0;
   const size_t per_cta = static_cast<size_t>(2 * K + W) * RDims<NV>::W + static_cast<size_t>(K) * RDims<NV>::W;
-  c.slots = scratch + static_cast<size_t>(blockIdx.x) * per_cta;
+  c.slots = scratch + static_cast<size_t>(blockIdx.x / c.size) * per_cta;
   c.reduced = c.slots + static_cast<size_t>(2 * K + W) * RDims<NV>::W;
   return c;
 }
@@ -362,15 +383,18 @@ __device__ void ptmg_one(const GeneData& d, const PtmgCta& c, const PtmgRequest&
     beta[j] = beta_sm[vc[j]];
   }
   __syncthreads();
-  tree_pass<NB, NV, 1, 2>(d, c, req.gene, beta, req.gamma, vc, D::W, c.p1, 2);
+  tree_pass<NB, NV, 1, 2>(d, c, req.gene, beta, req.gamma, vc, D::W, c.p1, 2, true);
   const double* tot = d.totals + static_cast<size_t>(req.gene) * K;
   for (int s = tid; s < K; s += blockDim.x) {
     c.ym[s] = (__ldg(tot + s) + req.alpha) / (c.p1[2 * s] + req.lambda);
-    out[s] = c.p1[2 * s];          // cumsumxtb
-    out[K + s] = c.p1[2 * s + 1];  // ylin
+    if (c.rank == 0) {
+      out[s] = c.p1[2 * s];          // cumsumxtb
+      out[K + s] = c.p1[2 * s + 1];  // ylin
+    }
   }
   __syncthreads();
-  tree_pass<NB, NV, 2, D::W>(d, c, req.gene, beta, req.gamma, vc, D::W, c.reduced, D::W);
+  tree_pass<NB, NV, 2, D::W>(d, c, req.gene, beta, req.gamma, vc, D::W, c.reduced, D::W, false);
+  if (c.rank != 0) return;  // rank 0 writes the result
   // every subject's full row, the constant columns' sums from the scalars
   for (int idx = tid; idx < K * F::W; idx += blockDim.x) {
     const int s = idx / F::W, x = idx - s * F::W;
@@ -384,9 +408,11 @@ __device__ void ptmg_one(const GeneData& d, const PtmgCta& c, const PtmgRequest&
 }
 
 // Streaming mode: one persistent launch for stage one, the request-ring
-// protocol of FitQueue (pml_device.cuh) with one CTA per request.
+// protocol of FitQueue (pml_device.cuh) with one cluster per request: rank
+// 0's first warp takes the ticket and hands it and the request to the other
+// CTAs, every CTA sweeps its ranges, rank 0 writes the result.
 template <int NB, int NV>
-__global__ void __launch_bounds__(ptmg_threads(NB, NV), 1)
+__global__ void __launch_bounds__(kPtmgCtaThreads, ptmg_cluster(NB, NV))
     ptmg_queue_kernel(GeneData d, PtmgQueue qu, double* scratch) {
   extern __shared__ __align__(16) double smem[];
   const PtmgCta c = ptmg_setup<NB, NV>(d, smem, scratch);
@@ -394,22 +420,50 @@ __global__ void __launch_bounds__(ptmg_threads(NB, NV), 1)
   __shared__ PtmgRequest next_req;
   __shared__ double beta_sm[kMaxCoef];
   for (;;) {
-    __syncthreads();
-    if (threadIdx.x < 32) {  // the first warp takes a ticket and waits for its request
+    cluster_sync(c);  // nobody still reads the previous ticket and request
+    if (c.rank == 0 && threadIdx.x < 32) {
       const long long got = ring_next(qu.ring, &next_req, nullptr);
       if (threadIdx.x == 0) next_ticket = got;
+      if (c.size > 1) {
+        cg::cluster_group cluster = cg::this_cluster();
+        constexpr int kWords = static_cast<int>(sizeof(PtmgRequest) / 8);
+        const unsigned long long* mine = reinterpret_cast<const unsigned long long*>(&next_req);
+        for (int r = 1; r < c.size; ++r) {
+          if (threadIdx.x == 0) *cluster.map_shared_rank(&next_ticket, r) = got;
+          if (static_cast<int>(threadIdx.x) < kWords && got >= 0)
+            cluster.map_shared_rank(reinterpret_cast<unsigned long long*>(&next_req), r)[threadIdx.x] =
+                mine[threadIdx.x];
+        }
+      }
     }
-    __syncthreads();
+    cluster_sync(c);
     const long long t = next_ticket;
     if (t < 0) break;
     const PtmgRequest req = next_req;
     ptmg_one<NB, NV>(d, c, req, beta_sm, qu.results + (t & qu.ring.mask) * qu.result_stride);
-    ring_publish(qu.done + (t & qu.ring.mask), t);
+    if (c.rank == 0) ring_publish(qu.done + (t & qu.ring.mask), t);
   }
+  cluster_sync(c);  // no CTA leaves while another may still write its shared memory
 }
 
 inline size_t smem_bytes(int K) {
   return static_cast<size_t>(4 * K) * 8 + (K + 1 + kMaxPtmgWarps + 1 + kMaxCoef) * 4 + 16;
+}
+
+template <int NB, int NV>
+cudaLaunchConfig_t ptmg_config(int grid, size_t smem, cudaStream_t stream, cudaLaunchAttribute* attr) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid, 1, 1);
+  cfg.blockDim = dim3(kPtmgCtaThreads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = ptmg_cluster(NB, NV);
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cfg;
 }
 
 template <int NB, int NV>
@@ -418,21 +472,24 @@ int launch_queue_nb(const GeneData& d, const PtmgQueue& qu, double* scratch, int
   cudaError_t e = cudaFuncSetAttribute(ptmg_queue_kernel<NB, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;
-  ptmg_queue_kernel<NB, NV><<<grid, ptmg_threads(NB, NV), smem, stream>>>(d, qu, scratch);
-  return cudaGetLastError();
+  if (grid % ptmg_cluster(NB, NV) != 0) return cudaErrorInvalidValue;
+  cudaLaunchAttribute attr[1];
+  cudaLaunchConfig_t cfg = ptmg_config<NB, NV>(grid, smem, stream, attr);
+  return cudaLaunchKernelEx(&cfg, ptmg_queue_kernel<NB, NV>, d, qu, scratch);
 }
 
+// CTAs the kernel keeps resident at once: whole clusters.
 template <int NB, int NV>
-int blocks_nb(int K) {
+int resident_nb(int K) {
   const size_t smem = smem_bytes(K);
   if (cudaFuncSetAttribute(ptmg_queue_kernel<NB, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            static_cast<int>(smem)) != cudaSuccess)
     return 0;
-  int blocks = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, ptmg_queue_kernel<NB, NV>, ptmg_threads(NB, NV), smem) !=
-      cudaSuccess)
-    return 0;
-  return blocks;
+  cudaLaunchAttribute attr[1];
+  cudaLaunchConfig_t cfg = ptmg_config<NB, NV>(ptmg_cluster(NB, NV), smem, nullptr, attr);
+  int clusters = 0;
+  if (cudaOccupancyMaxActiveClusters(&clusters, ptmg_queue_kernel<NB, NV>, &cfg) != cudaSuccess) return 0;
+  return clusters * ptmg_cluster(NB, NV);
 }
 
 template <int NB, int NV>
@@ -445,7 +502,7 @@ PtmgOps ptmg_ops_for(int n_varying) {
   if constexpr (NV > NB) {
     return PtmgOps{};
   } else {
-    if (n_varying == NV) return PtmgOps{&launch_queue_nb<NB, NV>, &blocks_nb<NB, NV>, &scratch_nb<NB, NV>};
+    if (n_varying == NV) return PtmgOps{&launch_queue_nb<NB, NV>, &resident_nb<NB, NV>, &scratch_nb<NB, NV>};
     return ptmg_ops_for<NB, NV + 1>(n_varying);
   }
 }

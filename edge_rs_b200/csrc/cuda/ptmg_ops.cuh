@@ -14,7 +14,7 @@ namespace device {
 
 struct PtmgOps {
   int (*launch)(const GeneData& d, const PtmgQueue& qu, double* scratch, int grid, cudaStream_t stream);
-  int (*blocks)(int K);
+  int (*resident)(int K);  // CTAs resident at once (whole clusters)
   size_t (*scratch)(int K);
 };
 

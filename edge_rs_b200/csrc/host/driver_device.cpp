@@ -330,13 +330,9 @@ double DeviceFitter::end_step() {
 void DeviceFitter::ensure_ptmg_scratch() {
   if (d_scratch_) return;
   const int K = data_.n_subjects;
-  int sms = 0, dev = 0;
-  cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
-  cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute");
-  const int per_sm = device::ptmg_blocks_per_sm(K, data_.n_coef, data_.n_varying);
-  if (per_sm <= 0)
+  pgrid_ = device::ptmg_resident_ctas(K, data_.n_coef, data_.n_varying);
+  if (pgrid_ <= 0)
     fail(NB_ERR_UNSUPPORTED, "the stage-one kernel cannot be resident with " + std::to_string(K) + " subjects");
-  pgrid_ = per_sm * sms;
   d_scratch_ = pool_alloc<double>(
       static_cast<size_t>(pgrid_) * device::ptmg_scratch_doubles(K, data_.n_coef, data_.n_varying), stream_,
       &pooled_);
