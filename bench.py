@@ -299,7 +299,10 @@ def ours_arm(args, world, rank, local, dist):
     import torch
     from edge_rs_b200.api import measure_fp64_tflops, nebula_sparse_cuda
     torch.cuda.set_device(local)
-    work = workloads.make(args.config, seed=1000 + rank, n_genes=args.genes)
+    if (args.genes or workloads.CONFIGS[args.config]["n_genes"]) > 4000:  # c4: gene blocks drawn in parallel
+        work = workloads.make_blocks(args.config, seed=1000 + rank, n_genes=args.genes)
+    else:
+        work = workloads.make(args.config, seed=1000 + rank, n_genes=args.genes)
     params = NebulaParams(method="HL")
     flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > 126 MB L2
     # the plain method (the reference's algorithm, bit-identical to the oracle)

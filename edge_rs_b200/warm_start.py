@@ -48,9 +48,7 @@ def examples(session, fit):
     return feats[ok], t[ok].astype(np.float32)
 
 
-def _draw(spec):
-    """workloads.make(**spec) in a worker process (numpy only, no GPU)."""
-    return workloads.make(**spec)
+_draw = workloads._draw
 
 
 def _fits(specs, procs):
@@ -83,23 +81,6 @@ def training_set(n_workloads=28, genes=600, seed=100, c2_genes=200000, c2_per_wo
         specs.append(dict(name="c1", seed=seed + i, n_genes=genes, n_cells=n_cells, n_subjects=n_subj,
                           sigma_log_sd=sd, phi_log_sd=sd))
     return _fits(specs, procs)
-
-
-def concat(parts):
-    """One workload from parts that share their cells (drawn with one seed
-    and different gene seeds): their genes stacked."""
-    ptr = [np.asarray(parts[0].indptr, np.uint64)]
-    for w in parts[1:]:
-        ptr.append(np.asarray(w.indptr[1:], np.uint64) + ptr[-1][-1])
-    indptr = np.concatenate(ptr)
-    if indptr[-1] >= 2 ** 32:
-        raise ValueError("more stored counts than a uint32 CSR can index")
-    first = parts[0]
-    return workloads.Workload(name=first.name, indptr=indptr.astype(np.uint32),
-                              indices=np.concatenate([w.indices for w in parts]),
-                              data=np.concatenate([w.data for w in parts]), n_genes=sum(w.n_genes for w in parts),
-                              n_cells=first.n_cells, subject=first.subject, design=first.design, offset=first.offset,
-                              truth=dict(sizes=first.truth["sizes"]))
 
 
 def train(features, targets, epochs=300, batch=512, lr=1e-3, seed=0):
@@ -173,12 +154,9 @@ def compare(params, name="c1", seed=1000, genes=500, n_cells=None, n_subjects=No
 def config4(params, procs, parts=5, seed=4000):
     """Config 4's evaluation workload (20,000 genes x 100,000 cells, 100
     subjects, 4 columns) drawn in `parts` gene blocks in parallel."""
-    import multiprocessing as mp
-    per = workloads.CONFIGS["c4"]["n_genes"] // parts
-    specs = [dict(name="c4", seed=seed, n_genes=per, gene_seed=i) for i in range(parts)]
-    with mp.get_context("spawn").Pool(min(procs, parts)) as pool:
-        blocks = pool.map(_draw, specs)
-    return compare(params, work=concat(blocks), steps=2, warmup=2)
+    work = workloads.make_blocks("c4", seed, block=workloads.CONFIGS["c4"]["n_genes"] // parts,
+                                 procs=min(procs, parts))
+    return compare(params, work=work, steps=2, warmup=2)
 
 
 def main():

@@ -148,3 +148,41 @@ def make(name="c1", seed=0, n_genes: Optional[int] = None, n_cells: Optional[int
     return Workload(name=name, indptr=indptr.astype(np.uint32), indices=indices, data=data, n_genes=G,
                     n_cells=N, subject=subject.astype(np.uint64), design=np.ascontiguousarray(design),
                     offset=lib, truth=dict(beta=beta, sigma2=sigma2, phi=phi, sizes=sizes))
+
+
+def _draw(spec):
+    """make(**spec) in a worker process."""
+    return make(**spec)
+
+
+def concat(parts):
+    """One workload from parts that share their cells (drawn with one seed and
+    different gene seeds): their genes stacked."""
+    ptr = [np.asarray(parts[0].indptr, np.uint64)]
+    for w in parts[1:]:
+        ptr.append(np.asarray(w.indptr[1:], np.uint64) + ptr[-1][-1])
+    indptr = np.concatenate(ptr)
+    if indptr[-1] >= 2 ** 32:
+        raise ValueError("more stored counts than a uint32 CSR can index")
+    first = parts[0]
+    return Workload(name=first.name, indptr=indptr.astype(np.uint32),
+                    indices=np.concatenate([w.indices for w in parts]),
+                    data=np.concatenate([w.data for w in parts]), n_genes=sum(w.n_genes for w in parts),
+                    n_cells=first.n_cells, subject=first.subject, design=first.design, offset=first.offset,
+                    truth=dict(sizes=first.truth["sizes"], sigma2=np.concatenate([w.truth["sigma2"] for w in parts]),
+                               phi=np.concatenate([w.truth["phi"] for w in parts])))
+
+
+def make_blocks(name, seed, n_genes=None, block=4000, procs=None):
+    """A workload of the named configuration drawn in gene blocks of `block`
+    in spawned worker processes (every block shares the cells, subjects and
+    design of `seed`; block i draws its genes from gene seed i). For the
+    largest configurations, where one process would take minutes."""
+    import multiprocessing as mp
+    import os
+    G = n_genes or CONFIGS[name]["n_genes"]
+    specs = [dict(name=name, seed=seed, n_genes=min(block, G - at), gene_seed=i)
+             for i, at in enumerate(range(0, G, block))]
+    procs = procs or max(1, min(16, os.cpu_count() or 1, len(specs)))
+    with mp.get_context("spawn").Pool(procs) as pool:
+        return concat(pool.map(_draw, specs))
