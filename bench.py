@@ -21,8 +21,10 @@ and warm inner fits, 5% of the genes audited cold
   on a bounded gene sample of the same workload, all host threads.
 
 `--impl reference` times that CPU path alone on the same workload and metric.
-Multi-GPU (torchrun): genes shard across ranks with no collective on the data
-path (weak scaling); each rank fits its own 500-gene workload.
+Multi-GPU (torchrun): weak scaling through the product's sharding: one
+workload of N x 500 genes cut into blocks of equal estimated work
+(edge_rs_b200/shard.py); each rank times its block, and the e2e leg calls
+fit_sharded, whose only collective is the gather of the results.
 """
 import argparse
 import json
@@ -171,6 +173,16 @@ def barrier_max(dist, value):
     return float(t.item())
 
 
+def all_sum(dist, value):
+    """Sum of a float over ranks (one all-reduce), or the value itself."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def cpu_sample(work, n_genes):
     """The first n_genes genes of a workload as their own CSR."""
     n = min(n_genes, work.n_genes)
@@ -299,16 +311,30 @@ def ours_arm(args, world, rank, local, dist):
     import torch
     from edge_rs_b200.api import measure_fp64_tflops, nebula_sparse_cuda
     torch.cuda.set_device(local)
-    if (args.genes or workloads.CONFIGS[args.config]["n_genes"]) > 4000:  # c4: gene blocks drawn in parallel
-        work = workloads.make_blocks(args.config, seed=1000 + rank, n_genes=args.genes)
+    per_rank = args.genes or workloads.CONFIGS[args.config]["n_genes"]
+    if per_rank * world > 4000:  # c4, or several ranks: gene blocks drawn in parallel
+        full = workloads.make_blocks(args.config, seed=1000, n_genes=per_rank * world)
     else:
-        work = workloads.make(args.config, seed=1000 + rank, n_genes=args.genes)
+        full = workloads.make(args.config, seed=1000, n_genes=per_rank * world)
+    work = full
+    if world > 1:
+        # weak scaling through the product's sharding: one workload of world x
+        # the per-rank genes (the same draw on every rank), each rank fitting
+        # the block shard_bounds gives it; the e2e leg calls fit_sharded
+        from edge_rs_b200.shard import shard_bounds, slice_genes
+        bounds = shard_bounds(full.indptr, full.n_cells, world)
+        lo, hi = int(bounds[rank]), int(bounds[rank + 1])
+        ptr, ind, dat, _ = slice_genes(full.csr, lo, hi)
+        work = workloads.Workload(name=full.name, indptr=ptr, indices=ind, data=dat, n_genes=hi - lo,
+                                  n_cells=full.n_cells, subject=full.subject, design=full.design,
+                                  offset=full.offset, truth=full.truth)
     params = NebulaParams(method="HL")
     flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > 126 MB L2
     # the plain method (the reference's algorithm, bit-identical to the oracle)
     plain_ms, plain_stats, plain_fit, _, stage_one = timed_session(args, work, params, flush, dist, 0,
                                                                    want_stage_one=True)
-    plain_value = world * len(plain_fit.gene_index) * args.steps / (barrier_max(dist, float(np.sum(plain_ms))) / 1000.0)
+    plain_value = (all_sum(dist, len(plain_fit.gene_index)) * args.steps
+                   / (barrier_max(dist, float(np.sum(plain_ms))) / 1000.0))
     # the headline: warm-started (learned search start, narrowed initial trust
     # radius, warm inner fits) and batched
     sampler = ClockSampler(local)
@@ -317,7 +343,7 @@ def ours_arm(args, world, rank, local, dist):
     clocks = sampler.stop()
     genes = len(fit.gene_index)
     total_ms = barrier_max(dist, float(np.sum(step_ms)))
-    value = world * genes * args.steps / (total_ms / 1000.0)
+    value = all_sum(dist, genes) * args.steps / (total_ms / 1000.0)
     launches = int(np.sum([s["gpu_launches"] for s in stats]))
     visits = float(np.sum([s["cell_visits"] for s in stats]))
     sparse_visits = float(np.sum([s["sparse_visits"] for s in stats]))
@@ -346,11 +372,16 @@ def ours_arm(args, world, rank, local, dist):
             dist.barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        f2 = nebula_sparse_cuda(work.csr, work.subject, work.design, work.n_coef, work.offset, params,
-                                cluster=args.cluster, warm_start=args.warm)
+        if world > 1:  # every rank returns the whole job's merged fit
+            from edge_rs_b200.shard import fit_sharded
+            f2 = fit_sharded(full.csr, full.subject, full.design, full.n_coef, full.offset, params,
+                             cluster=args.cluster, warm_start=args.warm)
+        else:
+            f2 = nebula_sparse_cuda(work.csr, work.subject, work.design, work.n_coef, work.offset, params,
+                                    cluster=args.cluster, warm_start=args.warm)
         torch.cuda.synchronize()
         el = barrier_max(dist, time.perf_counter() - t0)
-        e2e_vals.append(world * len(f2.gene_index) / el)
+        e2e_vals.append(len(f2.gene_index) / el)
         h2d = f2.stats["h2d_bytes"]
         d2h = f2.stats["d2h_bytes"]
         e2e_all.append(f2.stats)

@@ -4,10 +4,13 @@ Genes are independent (the reference fits them in a rayon par_iter and its
 device path in independent searches), so the path shards by gene with no
 exchange on the data path: every rank holds the design, offsets and subject
 boundaries and fits a contiguous block of genes chosen so the blocks carry
-about equal work, estimated per gene as n_cells + nnz (every sweep visits all
-cells plus the gene's positive counts). The only collective is the gather of
-the per-gene results at the end (`torch.distributed.all_gather_object`, over
-NCCL or gloo).
+about equal work, estimated per gene as (n_cells + nnz) x the evaluations its
+search is expected to take: every sweep visits all cells plus the gene's
+positive counts, and the search asks for about as many fits as evaluations.
+Expected evaluations come from the caller (a previous fit's `evaluations`,
+or the warm-start network's third output); without them every gene counts
+the same. The only collective is the gather of the per-gene results at the
+end (`torch.distributed.all_gather_object`, over NCCL or gloo).
 """
 from typing import Callable, Optional
 
@@ -16,12 +19,18 @@ import numpy as np
 from .api import NebulaError, NebulaFit
 
 
-def shard_bounds(indptr, n_cells, world):
+def shard_bounds(indptr, n_cells, world, evaluations=None):
     """Gene boundaries [b_0 = 0, ..., b_world = n_genes] of `world` contiguous
-    blocks of about equal estimated work."""
+    blocks of about equal estimated work: (n_cells + nnz) per gene, times its
+    expected `evaluations` when given (one per gene, positive)."""
     indptr = np.asarray(indptr, np.int64)
     n_genes = indptr.size - 1
-    work = (indptr[1:] - indptr[:-1]) + int(n_cells)
+    work = ((indptr[1:] - indptr[:-1]) + int(n_cells)).astype(np.float64)
+    if evaluations is not None:
+        ev = np.asarray(evaluations, np.float64)
+        if ev.shape != (n_genes,):
+            raise NebulaError(11, f"evaluations has {ev.size} entries, expected {n_genes}")
+        work = work * np.where(np.isfinite(ev) & (ev > 0), ev, 1.0)
     cum = np.concatenate([[0], np.cumsum(work)])
     targets = cum[-1] * np.arange(world + 1) / world
     bounds = np.searchsorted(cum, targets, side="left")
@@ -54,17 +63,18 @@ def merge_fits(parts, offsets, n_coef):
 
 
 def fit_sharded(counts, subject_id, design, n_coef, offset=None, params=None, fit: Optional[Callable] = None,
-                group=None, **kwargs):
+                group=None, evaluations=None, **kwargs):
     """nebula_sparse_cuda over the ranks of torch.distributed's default (or
     given) group: each rank fits its block of genes on its own GPU (or with
     `fit`, any function of nebula_sparse_cuda's signature) and every rank
-    returns the merged NebulaFit of all genes."""
+    returns the merged NebulaFit of all genes. evaluations: expected search
+    evaluations per input gene, weighting the blocks (shard_bounds)."""
     import torch.distributed as dist
     if fit is None:
         from .api import nebula_sparse_cuda as fit
     world = dist.get_world_size(group) if dist.is_initialized() else 1
     rank = dist.get_rank(group) if dist.is_initialized() else 0
-    bounds = shard_bounds(counts[0], counts[3][1], world)
+    bounds = shard_bounds(counts[0], counts[3][1], world, evaluations)
     lo, hi = int(bounds[rank]), int(bounds[rank + 1])
     mine = None
     if hi > lo:

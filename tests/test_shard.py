@@ -26,6 +26,21 @@ def test_shard_bounds_cover_all_genes_and_balance_the_work():
         assert work.max() <= work.mean() * 1.02 + 7000
 
 
+def test_shard_bounds_weight_by_expected_evaluations():
+    """(n_cells + nnz) x expected evaluations per gene: a block of genes whose
+    searches take four times the evaluations gets a quarter of the genes."""
+    from edge_rs_b200.shard import shard_bounds
+    indptr = np.arange(0, 1001 * 100, 100)  # 1000 genes of 100 entries
+    ev = np.ones(1000)
+    ev[:500] = 4.0
+    b = shard_bounds(indptr, 1000, 2, evaluations=ev)
+    cost = 1100.0 * ev
+    halves = [cost[b[0]:b[1]].sum(), cost[b[1]:b[2]].sum()]
+    assert abs(halves[0] - halves[1]) <= cost.max()
+    assert b[1] < 500  # the expensive genes are split off early
+    assert np.array_equal(shard_bounds(indptr, 1000, 2), shard_bounds(indptr, 1000, 2, evaluations=np.ones(1000)))
+
+
 def test_slice_genes_keeps_rows():
     from edge_rs_b200.shard import slice_genes
     indptr = np.array([0, 2, 2, 5], np.uint32)
