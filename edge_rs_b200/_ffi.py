@@ -115,7 +115,17 @@ PRODUCT_SIGNATURES = {
     "nb_bobyqa_result": (ctypes.c_int32, [ctypes.c_void_p, c_double_p, c_double_p,
                                           ctypes.POINTER(ctypes.c_uint32)]),
     "nb_bobyqa_free": (None, [ctypes.c_void_p]),
-    "nb_measure_fp64_tflops": (ctypes.c_double, [ctypes.c_int]),
+    "nb_search_new": (ctypes.c_void_p, [c_double_p, c_double_p, c_double_p, ctypes.c_uint32, ctypes.c_uint32,
+                                        ctypes.c_double]),
+    "nb_search_ask": (ctypes.c_uint32, [ctypes.c_void_p, c_double_p, ctypes.c_uint32]),
+    "nb_search_tell": (ctypes.c_int32, [ctypes.c_void_p, c_double_p, ctypes.c_uint32]),
+    "nb_search_order": (ctypes.c_uint32, [ctypes.c_void_p]),
+    "nb_search_result": (ctypes.c_int32, [ctypes.c_void_p, c_double_p, ctypes.POINTER(ctypes.c_int32),
+                                          ctypes.POINTER(ctypes.c_uint32)]),
+    "nb_search_free": (None, [ctypes.c_void_p]),
+    "nb_ring_check_cuda": (ctypes.c_int32, [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                            ctypes.POINTER(ctypes.c_uint64), ctypes.c_char_p, ctypes.c_size_t]),
+    "nb_measure_fp64_tflops":(ctypes.c_double, [ctypes.c_int]),
     "nb_mlp_init": (None, [ctypes.c_uint64, c_float_p]),
     "nb_mlp_builtin": (None, [c_float_p]),
     "nb_mlp_predict_cuda": (ctypes.c_int32, [c_float_p, c_float_p, ctypes.c_uint64, c_float_p, ctypes.c_char_p,

@@ -168,6 +168,21 @@ struct FitQueue {
 int launch_fit_queue(const GeneData& data, const FitControl& ctl, const FitQueue& queue, int grid, int cluster,
                      void* stream);
 
+// The ring's self-check (ring_check.cu): one-warp CTAs serve tickets with
+// the same ring_next / ring_publish as the persistent kernels and answer
+// each EchoRequest with its EchoResult.
+struct EchoRequest {
+  unsigned long long tag, a, b, c;
+};
+struct EchoResult {
+  unsigned long long tag, mixed, folded, ticket;
+};
+__host__ __device__ inline EchoResult echo_of(const EchoRequest& q, long long ticket) {
+  const unsigned long long t = static_cast<unsigned long long>(ticket);
+  return EchoResult{q.tag, q.a * 0x9E3779B97F4A7C15ull + q.b, q.c ^ (t * 0xD1B54A32D192ED03ull), t};
+}
+int launch_ring_echo(const RingView& ring, EchoResult* results, long long* done, int ctas, void* stream);
+
 // Clusters of `cluster` CTAs the streaming kernel can keep resident at once.
 int fit_queue_max_clusters(int n_subjects, int n_coef, int n_varying, int cluster);
 

@@ -480,19 +480,22 @@ const device::FitResult* DeviceFitter::collect(int lane_index) {
 // Streaming mode.
 
 int DeviceFitter::cluster_for(size_t requests) const {
-  // Spread each fit over more CTAs while (a) the fits in flight times the
-  // cluster stay within about four times the resident CTA slots, so the
-  // searches that finish last still find the SMs busy, and (b) each CTA keeps
-  // at least ~40,000 cells per sweep, so a sweep's fixed costs (the cluster
-  // barrier, the combine, the Newton step every CTA repeats) stay small. The
-  // count is the design's cells even under zero-count tables, whose sweeps
-  // visit far fewer: their steps are bound by the chains of evaluations, and
-  // a fit spread wider ends sooner (500 genes x 100,000 cells, categorical:
-  // 77 ms a step at 4 CTAs per fit, 92 at 2, 119 at 1).
+  // Spread each fit over more CTAs while each CTA keeps at least 25,000 cells
+  // per sweep, so a sweep's fixed costs (the cluster barrier, the combine, the
+  // Newton step every CTA repeats) stay small; beyond two CTAs only while the
+  // requests times the cluster stay within eight times the resident CTA
+  // slots, where the searches that finish last would otherwise run on a few
+  // SMs. The count is the design's cells even under zero-count tables, whose
+  // sweeps visit far fewer: their steps are bound by the chains of
+  // evaluations, and a fit spread wider ends sooner (500 genes x 100,000
+  // cells, categorical: 77 ms a step at 4 CTAs per fit, 92 at 2, 119 at 1).
+  // The sessions' tuning picked 4, 2, 2 and 2 CTAs for 500 x 100,000 (p = 4),
+  // 4,000 x 50,000 (p = 8), 2,000 x 200,000 (p = 8) and 20,000 x 100,000
+  // (p = 4), which this rule gives.
   int cluster = 1;
   while (cluster < device::kMaxCluster && queue_clusters_[cluster * 2] > 0 &&
-         requests * static_cast<size_t>(cluster) * 2 <= 4 * static_cast<size_t>(grid_) &&
-         n_cells_ >= static_cast<size_t>(cluster) * 2 * 40000)
+         n_cells_ >= static_cast<size_t>(cluster) * 2 * 25000 &&
+         (cluster < 2 || requests * static_cast<size_t>(cluster) * 2 <= 8 * static_cast<size_t>(grid_)))
     cluster *= 2;
   return cluster;
 }

@@ -70,7 +70,11 @@ void* mapped_alloc(size_t bytes) {
 }  // namespace
 
 RequestQueue::RequestQueue(size_t request_bytes, size_t result_bytes, size_t capacity)
-    : request_bytes_(request_bytes), result_bytes_(result_bytes), capacity_(capacity) {}
+    : request_bytes_(request_bytes), result_bytes_(result_bytes), capacity_(capacity), idle_ns_(kIdleNs) {}
+
+static std::string idle_text(long long ns) {
+  return ns % 1000000000LL == 0 ? std::to_string(ns / 1000000000LL) + " s" : std::to_string(ns / 1000000LL) + " ms";
+}
 
 RequestQueue::~RequestQueue() {
   abort();
@@ -144,7 +148,7 @@ void RequestQueue::launch(cudaStream_t stream, const std::function<cudaError_t(c
   v.ring.ring = d_ring_;
   v.ring.words = d_words_;
   v.ring.mask = static_cast<long long>(capacity_ - 1);
-  v.ring.idle_ns = kIdleNs;
+  v.ring.idle_ns = idle_ns_;
   v.ring.request_bytes = static_cast<int>(request_bytes_);
   v.results = device_view(h_results_);
   v.done = device_view(h_done_);
@@ -238,7 +242,7 @@ void RequestQueue::stop_impl(bool check_status) {
   float ms = 0.0f;
   check(cudaEventElapsedTime(&ms, ev0_, ev1_), "event time");
   device_ms_ += ms;
-  if (status != 0) fail(NB_ERR_GPU, "a queue cluster waited more than 5 s for work");
+  if (status != 0) fail(NB_ERR_GPU, "a queue cluster waited more than " + idle_text(idle_ns_) + " for work");
 }
 
 void RequestQueue::stop() { stop_impl(true); }
@@ -259,7 +263,8 @@ void RequestQueue::failure(const char* what) {
       taken = std::to_string(n);
   }
   fail(NB_ERR_GPU, std::string("the queue kernel ") + what + " (tickets posted " + std::to_string(next_.load()) +
-                       ", taken " + taken + (status == 1 ? ", a cluster waited more than 5 s for work)" : ")"));
+                       ", taken " + taken +
+                       (status == 1 ? ", a cluster waited more than " + idle_text(idle_ns_) + " for work)" : ")"));
 }
 
 }  // namespace nebula

@@ -70,6 +70,9 @@ class RequestQueue {
   [[noreturn]] void failure(const char* what);
   double device_ms() const { return device_ms_; }
   size_t capacity() const { return capacity_; }
+  // How long a cluster waits for its ticket's request before it sets the
+  // status word and exits (default 5 s); takes effect at the next launch.
+  void set_idle_ns(long long ns) { idle_ns_ = ns; }
 
  private:
   enum State : int { kIdle = 0, kPrepared = 1, kLaunched = 2 };
@@ -92,6 +95,7 @@ class RequestQueue {
   std::atomic<int> state_{kIdle};
   int device_ = -1;
   double device_ms_ = 0.0;
+  long long idle_ns_;
 };
 
 }  // namespace nebula

@@ -360,6 +360,48 @@ int32_t nb_bobyqa_result(const nb_bobyqa* h, double* x, double* f,
                          uint32_t* evaluations);
 void nb_bobyqa_free(nb_bobyqa* h);
 
+/* The stage-two search the device driver steps for every gene, in reverse
+ * communication (src/sc/nebula.rs:1568-1951 StageTwoSearch::{new, ask,
+ * tell, order, result}): n = 2 runs BOBYQA over (sigma, gamma), n = 1 the
+ * clamped start, a bounded Nelder-Mead and the polish stencils. A
+ * non-finite value told at Laplace order ord > 1 restarts the pass at order
+ * one; at order one it abandons the search. radius_scale (0, 1] narrows the
+ * first BOBYQA pass's initial trust region (1: NLopt's). NULL on invalid
+ * arguments. */
+typedef struct nb_search nb_search;
+nb_search* nb_search_new(const double* start, const double* lower,
+                         const double* upper, uint32_t n, uint32_t ord,
+                         double radius_scale);
+/* How many points are pending (0 once the search is done); copies up to
+ * max_points of them, n doubles each, into points (may be NULL). */
+uint32_t nb_search_ask(const nb_search* h, double* points, uint32_t max_points);
+/* One value per pending point; NB_ERR_LENGTH_MISMATCH otherwise. */
+int32_t nb_search_tell(nb_search* h, const double* values, uint32_t n_values);
+uint32_t nb_search_order(const nb_search* h); /* the Laplace order under test */
+/* 1: done with a minimiser in x (n doubles) and *failed = 1 where BOBYQA
+ * ended roundoff-limited (the gene's convergence -50); 0: done, abandoned
+ * (no finite pass: the gene keeps stage one's estimates, convergence -50);
+ * -1: still running. *evaluations: values told so far. */
+int32_t nb_search_result(const nb_search* h, double* x, int32_t* failed,
+                         uint32_t* evaluations);
+void nb_search_free(nb_search* h);
+
+/* Self-check of the request ring that feeds the persistent kernels (no
+ * counterpart in the reference, whose rounds are host-driven launches,
+ * src/gpu/stage_two.rs:362-580 search_all). On the current device, `ctas` one-warp CTAs
+ * serve n_requests tickets through a ring of `capacity` slots (a power of
+ * two; fewer slots than requests exercises slot reuse) with the same device
+ * protocol as the fit and stage-one kernels, answering each request with a
+ * fixed function of it; *mismatches counts results that differ from it.
+ * idle_ms: how long a CTA waits for its ticket's request before it sets the
+ * ring's status word and returns (0 = the library's 5 s). With n_requests 0
+ * nothing is posted and no stop is requested, so every CTA's wait runs out:
+ * the call then returns NB_ERR_GPU ("... waited more than idle_ms for
+ * work") without a device fault, and the device stays usable. */
+int32_t nb_ring_check_cuda(uint64_t n_requests, uint32_t capacity,
+                           uint32_t ctas, uint32_t idle_ms,
+                           uint64_t* mismatches, char* err, size_t err_len);
+
 /* Measured FP64 FMA throughput of the current device in TFLOP/s (best of
  * `repeats` launches), the peak the fit kernel's roofline is taken against. */
 double nb_measure_fp64_tflops(int repeats);
