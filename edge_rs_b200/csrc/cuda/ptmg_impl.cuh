@@ -38,6 +38,7 @@
 #include <cstdint>
 
 #include "../host/nbmath.hpp"
+#include "nbmath_device.cuh"
 #include "ptmg_device.cuh"
 #include "ptmg_ops.cuh"
 #include "ring_device.cuh"
@@ -118,11 +119,12 @@ __device__ __forceinline__ double eta_from(const double* x, const double* beta, 
 
 // Pass two's dense (count zero) contribution of one cell.
 template <int NV>
-__device__ __forceinline__ void dense_two(double* acc, const double* x, double e, double ym, double gamma) {
+__device__ __forceinline__ void dense_two(double* acc, const double* x, double e, double ym, double gamma,
+                                          const NbTableData* tab) {
   using D = RDims<NV>;
   const double we = ym * e;
   const double w = we + gamma;
-  const double lw = nb_log(w);
+  const double lw = nb_log_tab(w, tab);
   const double iw = nb_recip(w);
   const double gg = gamma * iw;
   const double gt = gg * iw;
@@ -162,10 +164,10 @@ __device__ __forceinline__ void dense_two(double* acc, const double* x, double e
 // What a positive count y adds to a cell's pass-two contribution.
 template <int NV>
 __device__ __forceinline__ void sparse_two(double* acc, const double* x, double e, double y, double ym,
-                                           double gamma) {
+                                           double gamma, const NbTableData* tab) {
   using D = RDims<NV>;
   const double w = ym * e + gamma;
-  const double lw = nb_log(w);
+  const double lw = nb_log_tab(w, tab);
   const double iw = nb_recip(w);
   const double gg = y * iw;
   const double gt = gg * iw;
@@ -197,6 +199,7 @@ __device__ __forceinline__ void sparse_two(double* acc, const double* x, double 
 
 // Shared-memory and scratch views of one stage-one CTA.
 struct PtmgCta {
+  const NbTableData* tab;  // exp/log tables (nbmath.hpp), shared memory
   double* ym;        // K
   double* p1;        // K x 2: cumsumxtb, ylin
   double* cs;        // K: the constant columns' share of eta for this request
@@ -237,21 +240,41 @@ __device__ void tree_pass(const GeneData& d, const PtmgCta& c, int gene, const d
       for (int v = 0; v < N; ++v) acc[v] = 0.0;
       const double yms = PASS == 2 ? c.ym[s] : 0.0;
       const double cs = c.cs[s];
-      for (int r = c0 + lane; r < s_end; r += 64) {
-        const bool has_b = r + 32 < s_end;
-        const int rb = has_b ? r + 32 : r;
-        double xa[NX], xb[NX];
+      // each lane's next two rows and offsets are loaded one iteration
+      // ahead, so their latency overlaps the current cells' arithmetic
+      int r = c0 + lane;
+      double xa[NX], xb[NX], oa = 0.0, ob = 0.0;
+      if (r < s_end) {
+        const int rb = r + 32 < s_end ? r + 32 : r;
         varying_row<NB, NV>(d.design, vc, r, xa);
         varying_row<NB, NV>(d.design, vc, rb, xb);
-        const double ea = nb_exp(eta_from<NV>(xa, beta, __ldg(d.log_offset + r) + cs));
-        const double eb = nb_exp(eta_from<NV>(xb, beta, __ldg(d.log_offset + rb) + cs));
+        oa = __ldg(d.log_offset + r);
+        ob = __ldg(d.log_offset + rb);
+      }
+      for (; r < s_end; r += 64) {
+        const bool has_b = r + 32 < s_end;
+        const int rn = r + 64 < s_end ? r + 64 : r;
+        const int rnb = rn + 32 < s_end ? rn + 32 : rn;
+        double xna[NX], xnb[NX];
+        varying_row<NB, NV>(d.design, vc, rn, xna);
+        varying_row<NB, NV>(d.design, vc, rnb, xnb);
+        const double ona = __ldg(d.log_offset + rn), onb = __ldg(d.log_offset + rnb);
+        const double ea = nb_exp_tab(eta_from<NV>(xa, beta, oa + cs), c.tab);
+        const double eb = nb_exp_tab(eta_from<NV>(xb, beta, ob + cs), c.tab);
         if constexpr (PASS == 1) {
           acc[0] += ea;
           if (has_b) acc[0] += eb;
         } else {
-          dense_two<NV>(acc, xa, ea, yms, gamma);
-          if (has_b) dense_two<NV>(acc, xb, eb, yms, gamma);
+          dense_two<NV>(acc, xa, ea, yms, gamma, c.tab);
+          if (has_b) dense_two<NV>(acc, xb, eb, yms, gamma, c.tab);
         }
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
+          xa[j] = xna[j];
+          xb[j] = xnb[j];
+        }
+        oa = ona;
+        ob = onb;
       }
       reduce_to<N>(acc, c.slots + (s + warp) * stride, lane);
       c0 = s_end;
@@ -279,8 +302,8 @@ __device__ void tree_pass(const GeneData& d, const PtmgCta& c, int gene, const d
         acc[1] = nb_fma(eta_a, ya, acc[1]);
         if (has_b) acc[1] = nb_fma(eta_b, yb, acc[1]);
       } else {
-        sparse_two<NV>(acc, xa, nb_exp(eta_a), ya, yms, gamma);
-        if (has_b) sparse_two<NV>(acc, xb, nb_exp(eta_b), yb, yms, gamma);
+        sparse_two<NV>(acc, xa, nb_exp_tab(eta_a, c.tab), ya, yms, gamma, c.tab);
+        if (has_b) sparse_two<NV>(acc, xb, nb_exp_tab(eta_b, c.tab), yb, yms, gamma, c.tab);
       }
     }
     reduce_to<N>(acc, c.slots + (K + W + s) * stride, lane);
@@ -332,7 +355,10 @@ __device__ PtmgCta ptmg_setup(const GeneData& d, double* smem, double* scratch) 
   const int K = d.n_subjects;
   constexpr int W = ptmg_warps(NB, NV);
   PtmgCta c;
-  c.ym = smem;
+  NbTableData* tab = reinterpret_cast<NbTableData*>(smem);
+  nb_load_tables(tab);  // first used after the request loop's opening cluster barrier
+  c.tab = tab;
+  c.ym = smem + kNbTableDoubles;
   c.p1 = c.ym + K;
   c.cs = c.p1 + 2 * K;
   c.fid = reinterpret_cast<uint32_t*>(c.cs + K);
@@ -447,7 +473,7 @@ __global__ void __launch_bounds__(kPtmgCtaThreads, ptmg_cluster(NB, NV))
 }
 
 inline size_t smem_bytes(int K) {
-  return static_cast<size_t>(4 * K) * 8 + (K + 1 + kMaxPtmgWarps + 1 + kMaxCoef) * 4 + 16;
+  return static_cast<size_t>(kNbTableDoubles + 4 * K) * 8 + (K + 1 + kMaxPtmgWarps + 1 + kMaxCoef) * 4 + 16;
 }
 
 template <int NB, int NV>

@@ -17,9 +17,12 @@
 namespace oracle {
 namespace {
 
-using nebula::nb_exp;
 using nebula::nb_fma;
-using nebula::nb_log;
+
+// the table-driven exp and log the kernel calls (its shared-memory copy of
+// the same tables)
+double cell_exp(double x) { return nebula::nb_exp_tab(x, &nebula::kNbTables); }
+double cell_log(double x) { return nebula::nb_log_tab(x, &nebula::kNbTables); }
 
 
 }  // namespace
@@ -55,7 +58,7 @@ nebula::PtmgSums ptmg_sums(const PmlData& d, const double* beta, double alpha, d
   // pass one: sum e over every cell, sum y eta over the positive ones
   auto dense1 = [&](double* acc, size_t r, int s) {
     double x[kMaxRow];
-    acc[0] += nb_exp(eta_at(r, s, x));
+    acc[0] += cell_exp(eta_at(r, s, x));
   };
   auto sparse1 = [&](double* acc, size_t i, int s) {
     double x[kMaxRow];
@@ -73,11 +76,11 @@ nebula::PtmgSums ptmg_sums(const PmlData& d, const double* beta, double alpha, d
   // pass two
   auto dense2 = [&](double* acc, size_t r, int s) {
     double x[kMaxRow];
-    const double e = nb_exp(eta_at(r, s, x));
+    const double e = cell_exp(eta_at(r, s, x));
     const double yms = ym[s];
     const double we = yms * e;
     const double w = we + gamma;
-    const double lw = nb_log(w);
+    const double lw = cell_log(w);
     const double iw = 1.0 / w;
     const double gg = gamma * iw;
     const double gt = gg * iw;
@@ -114,10 +117,10 @@ nebula::PtmgSums ptmg_sums(const PmlData& d, const double* beta, double alpha, d
   auto sparse2 = [&](double* acc, size_t i, int s) {
     double x[kMaxRow];
     const double y = d.counts[i];
-    const double e = nb_exp(eta_at(d.cells[i], s, x));
+    const double e = cell_exp(eta_at(d.cells[i], s, x));
     const double yms = ym[s];
     const double w = yms * e + gamma;
-    const double lw = nb_log(w);
+    const double lw = cell_log(w);
     const double iw = 1.0 / w;
     const double gg = y * iw;
     const double gt = gg * iw;
