@@ -29,7 +29,7 @@
 // serves the whole stage: each CTA claims the next ticket of the request
 // ring (host memory mapped into the device), waits (bounded) for the host to
 // post it, and writes its result to host-mapped memory; the warp slots and the subjects' reduced
-// sums live in a per-CTA global scratch region (L2-resident).
+// sums live in a per-cluster global scratch region (L2-resident).
 #pragma once
 
 #include <cooperative_groups.h>
@@ -216,25 +216,36 @@ __device__ __forceinline__ void cluster_sync(const PtmgCta& c) {
   else __syncthreads();
 }
 
-// One pass through the tree: dense pieces into slots[(s + warp) * stride],
-// sparse pieces into slots[(K + W + s) * stride] (W = ptmg_warps; warp is the
-// range's index over the cluster), then per subject
-// out[s * out_stride + v] = 0 + dense pieces (warp order) + sparse piece,
-// by every CTA of the cluster (`all_combine`) or by rank 0 alone. Lanes take
-// two cells (r, r + 32) or entries per iteration; each lane's partials still
-// take them in its sequential order.
+// One pass through the segment tree: warp w of the request sums its cell
+// range [wcells[w], wcells[w + 1]) one subject segment at a time, first the
+// segment's cells (dense, at a count of zero) and then, into the same
+// partials, the positive entries whose cells fall in the segment (sparse),
+// into slots[(s + w) * stride]; then per subject
+// out[s * out_stride + v] = 0 + the pieces of the warps that meet it, in warp
+// order, by every CTA of the cluster (`all_combine`) or by rank 0 alone.
+// Lanes take two cells (r, r + 32) or entries per iteration; each lane's
+// partials still take them in its sequential order. The warp ranges are
+// every (64 / W)-th of the fit's 64 cell ranges, so their first positive
+// entries are the gene's range_pos there.
 template <int NB, int NV, int PASS, int N>
 __device__ void tree_pass(const GeneData& d, const PtmgCta& c, int gene, const double* beta, double gamma,
                           const int* vc, int stride, double* out, int out_stride, bool all_combine) {
   const int K = d.n_subjects;
   constexpr int W = ptmg_warps(NB, NV);
+  static_assert(kRanges % W == 0, "warp ranges are unions of the fit's cell ranges");
+  constexpr int kStep = kRanges / W;
   const int warp = c.rank * kPtmgCtaWarps + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   constexpr int NX = NV > 0 ? NV : 1;
   const int c_begin = static_cast<int>(c.wcells[warp]), c_end = static_cast<int>(c.wcells[warp + 1]);
   if (c_begin < c_end) {
+    const uint64_t* runs = d.runs + static_cast<size_t>(gene) * (K + 1);
+    const uint64_t* rpos = d.range_pos + static_cast<size_t>(gene) * (kRanges + 1);
+    uint64_t pa = rpos[warp * kStep];
+    const uint64_t p_last = rpos[(warp + 1) * kStep];
     int s = subject_of(c.fid, K, c_begin);
     for (int c0 = c_begin; c0 < c_end; ++s) {
       const int s_end = min(c_end, static_cast<int>(c.fid[s + 1]));
+      const uint64_t p_end = s_end == c_end ? p_last : runs[s + 1];
       double acc[N];
 #pragma unroll
       for (int v = 0; v < N; ++v) acc[v] = 0.0;
@@ -276,37 +287,29 @@ __device__ void tree_pass(const GeneData& d, const PtmgCta& c, int gene, const d
         oa = ona;
         ob = onb;
       }
+      // the segment's positive entries, continuing the same partials
+      for (uint64_t p = pa + lane; p < p_end; p += 64) {
+        const bool has_b = p + 32 < p_end;
+        const uint64_t pb = has_b ? p + 32 : p;
+        const int ca = static_cast<int>(__ldg(d.cells + p)), cb = static_cast<int>(__ldg(d.cells + pb));
+        const double ya = __ldg(d.counts + p), yb = __ldg(d.counts + pb);
+        double xca[NX], xcb[NX];
+        varying_row<NB, NV>(d.design, vc, ca, xca);
+        varying_row<NB, NV>(d.design, vc, cb, xcb);
+        const double eta_a = eta_from<NV>(xca, beta, __ldg(d.log_offset + ca) + cs);
+        const double eta_b = eta_from<NV>(xcb, beta, __ldg(d.log_offset + cb) + cs);
+        if constexpr (PASS == 1) {
+          acc[1] = nb_fma(eta_a, ya, acc[1]);
+          if (has_b) acc[1] = nb_fma(eta_b, yb, acc[1]);
+        } else {
+          sparse_two<NV>(acc, xca, nb_exp_tab(eta_a, c.tab), ya, yms, gamma, c.tab);
+          if (has_b) sparse_two<NV>(acc, xcb, nb_exp_tab(eta_b, c.tab), yb, yms, gamma, c.tab);
+        }
+      }
       reduce_to<N>(acc, c.slots + (s + warp) * stride, lane);
+      pa = p_end;
       c0 = s_end;
     }
-  }
-  const uint64_t* runs = d.runs + static_cast<size_t>(gene) * (K + 1);
-  for (int s = warp; s < K; s += W) {
-    const uint64_t p0 = runs[s], p1 = runs[s + 1];
-    double acc[N];
-#pragma unroll
-    for (int v = 0; v < N; ++v) acc[v] = 0.0;
-    const double yms = PASS == 2 ? c.ym[s] : 0.0;
-    const double cs = c.cs[s];
-    for (uint64_t p = p0 + lane; p < p1; p += 64) {
-      const bool has_b = p + 32 < p1;
-      const uint64_t pb = has_b ? p + 32 : p;
-      const int ca = static_cast<int>(__ldg(d.cells + p)), cb = static_cast<int>(__ldg(d.cells + pb));
-      const double ya = __ldg(d.counts + p), yb = __ldg(d.counts + pb);
-      double xa[NX], xb[NX];
-      varying_row<NB, NV>(d.design, vc, ca, xa);
-      varying_row<NB, NV>(d.design, vc, cb, xb);
-      const double eta_a = eta_from<NV>(xa, beta, __ldg(d.log_offset + ca) + cs);
-      const double eta_b = eta_from<NV>(xb, beta, __ldg(d.log_offset + cb) + cs);
-      if constexpr (PASS == 1) {
-        acc[1] = nb_fma(eta_a, ya, acc[1]);
-        if (has_b) acc[1] = nb_fma(eta_b, yb, acc[1]);
-      } else {
-        sparse_two<NV>(acc, xa, nb_exp_tab(eta_a, c.tab), ya, yms, gamma, c.tab);
-        if (has_b) sparse_two<NV>(acc, xb, nb_exp_tab(eta_b, c.tab), yb, yms, gamma, c.tab);
-      }
-    }
-    reduce_to<N>(acc, c.slots + (K + W + s) * stride, lane);
   }
   cluster_sync(c);  // every CTA's pieces are in the scratch (read past L1)
   if (all_combine || c.rank == 0) {
@@ -317,7 +320,6 @@ __device__ void tree_pass(const GeneData& d, const PtmgCta& c, int gene, const d
 #pragma unroll
       for (int w = 0; w < W; ++w)
         if (c.wcells[w] < a1 && c.wcells[w + 1] > a0) total += __ldcg(c.slots + (s + w) * stride + v);
-      total += __ldcg(c.slots + (K + W + s) * stride + v);
       out[s * out_stride + v] = total;
     }
   }
@@ -374,9 +376,10 @@ __device__ PtmgCta ptmg_setup(const GeneData& d, double* smem, double* scratch) 
   }
   c.size = ptmg_cluster(NB, NV);
   c.rank = c.size > 1 ? static_cast<int>(cg::this_cluster().block_rank()) : 0;
-  const size_t per_cta = static_cast<size_t>(2 * K + W) * RDims<NV>::W + static_cast<size_t>(K) * RDims<NV>::W;
+  // per cluster: the K + W segment pieces, then the K reduced rows
+  const size_t per_cta = static_cast<size_t>(2 * K + W) * RDims<NV>::W;
   c.slots = scratch + static_cast<size_t>(blockIdx.x / c.size) * per_cta;
-  c.reduced = c.slots + static_cast<size_t>(2 * K + W) * RDims<NV>::W;
+  c.reduced = c.slots + static_cast<size_t>(K + W) * RDims<NV>::W;
   return c;
 }
 
@@ -520,7 +523,7 @@ int resident_nb(int K) {
 
 template <int NB, int NV>
 size_t scratch_nb(int K) {
-  return static_cast<size_t>(3 * K + ptmg_warps(NB, NV)) * RDims<NV>::W;
+  return static_cast<size_t>(2 * K + ptmg_warps(NB, NV)) * RDims<NV>::W;
 }
 
 template <int NB, int NV = 0>

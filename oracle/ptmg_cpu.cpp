@@ -53,7 +53,6 @@ nebula::PtmgSums ptmg_sums(const PmlData& d, const double* beta, double alpha, d
     for (int j = 0; j < nv; ++j) eta = nb_fma(x[j], bv[j], eta);
     return eta;
   };
-  const std::vector<size_t> run = positive_runs(d);
   nebula::PtmgSums out;
   // pass one: sum e over every cell, sum y eta over the positive ones
   auto dense1 = [&](double* acc, size_t r, int s) {
@@ -64,7 +63,7 @@ nebula::PtmgSums ptmg_sums(const PmlData& d, const double* beta, double alpha, d
     double x[kMaxRow];
     acc[1] = nb_fma(eta_at(d.cells[i], s, x), d.counts[i], acc[1]);
   };
-  std::vector<double> p1 = tree_sums(d, run, 2, warps, dense1, sparse1);
+  std::vector<double> p1 = tree_sums(d, 2, warps, dense1, sparse1);
   out.cumsumxtb.resize(k);
   out.ylin.resize(k);
   std::vector<double> ym(k);
@@ -147,7 +146,7 @@ nebula::PtmgSums ptmg_sums(const PmlData& d, const double* beta, double alpha, d
       }
     }
   };
-  const std::vector<double> red = tree_sums(d, run, RW, warps, dense2, sparse2);
+  const std::vector<double> red = tree_sums(d, RW, warps, dense2, sparse2);
   // every subject's full row: a constant column's sums are its value times a
   // scalar sum (sum x_a e = x_a sum e, sum x_a gg e = x_a acc[6], ...)
   out.sums.assign(static_cast<size_t>(k) * W, 0.0);
