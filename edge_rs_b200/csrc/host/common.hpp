@@ -70,17 +70,57 @@ struct Prepared {
 Prepared prepare(const nb_csr* counts, const uint64_t* subject_id, const double* design,
                  uint32_t n_coef, const double* offset, const nb_params* params);
 
-// One gene's positive counts (positive_indices, ptmg.rs:1681-1728).
+// A read-only view of n contiguous values (the CUDA translation units that
+// include this header compile as C++17, without std::span).
+template <typename T>
+struct View {
+  const T* ptr = nullptr;
+  size_t n = 0;
+  View() = default;
+  View(const T* p, size_t count) : ptr(p), n(count) {}
+  View(const std::vector<T>& v) : ptr(v.data()), n(v.size()) {}  // NOLINT: views a vector in place
+  const T* data() const { return ptr; }
+  size_t size() const { return n; }
+  bool empty() const { return n == 0; }
+  const T* begin() const { return ptr; }
+  const T* end() const { return ptr + n; }
+  const T& operator[](size_t i) const { return ptr[i]; }
+};
+
+// One gene's positive counts (positive_indices, ptmg.rs:1681-1728). `cells`
+// and `counts` view either the caller's CSR row itself (borrowed: every
+// stored value of the row is positive) or the gene's own compacted copy; a
+// move keeps the views valid, a copy is not allowed.
 struct GeneCounts {
-  std::vector<uint32_t> cells;
-  std::vector<double> counts;
+  View<uint32_t> cells;
+  View<double> counts;
   double mean_count = 0.0;
   size_t n_one = 0, n_two = 0;
   // distinct counts other than one and two, increasing, with multiplicities:
   // the gamma-function terms take one lgamma per distinct value
   std::vector<double> big_values, big_mult;
+
+  GeneCounts() = default;
+  GeneCounts(GeneCounts&&) = default;
+  GeneCounts& operator=(GeneCounts&&) = default;
+  GeneCounts(const GeneCounts&) = delete;
+  GeneCounts& operator=(const GeneCounts&) = delete;
+  // Takes its own copy of n entries and views it.
+  void own(const uint32_t* c, const double* y, size_t n) {
+    own_cells_.assign(c, c + n);
+    own_counts_.assign(y, y + n);
+    cells = own_cells_;
+    counts = own_counts_;
+  }
+
+ private:
+  friend GeneCounts positive_indices(const CsrView& csr, size_t gene, bool borrow);
+  std::vector<uint32_t> own_cells_;
+  std::vector<double> own_counts_;
 };
-GeneCounts positive_indices(const CsrView& csr, size_t gene);
+// borrow: view the caller's row where every stored value is positive (the
+// caller keeps `csr` alive while the result is used); otherwise copy.
+GeneCounts positive_indices(const CsrView& csr, size_t gene, bool borrow = false);
 
 // Stage one's decision for one gene (nebula.rs:745-773).
 enum class Refit { None, Both, SubjectOnly };

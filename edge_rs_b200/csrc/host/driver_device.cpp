@@ -659,9 +659,12 @@ void record_cluster(Session& ss, int cluster, double ms) {
   }
 }
 
+// borrow_counts: the genes view the caller's CSR rows instead of copying
+// them (a one-shot call, whose caller keeps its arrays for the call); a
+// session kept across calls holds its own copy.
 std::unique_ptr<Session> create_session(const nb_csr* counts, const uint64_t* subject_id, const double* design,
                                         uint32_t n_coef, const double* offset, const nb_params* params,
-                                        const nb_options* options) {
+                                        const nb_options* options, bool borrow_counts) {
   auto t0 = Clock::now();
   auto ss = std::make_unique<Session>();
   ss->opt.device = -1;
@@ -674,7 +677,7 @@ std::unique_ptr<Session> create_session(const nb_csr* counts, const uint64_t* su
   const size_t G = ss->prep.kept.size();
   ss->genes.resize(G);
   parallel_for(G, ss->opt.host_threads,
-               [&](size_t g) { ss->genes[g] = positive_indices(ss->prep.counts, ss->prep.kept[g]); });
+               [&](size_t g) { ss->genes[g] = positive_indices(ss->prep.counts, ss->prep.kept[g], borrow_counts); });
   ss->ms_prepare = ms_since(t0);
   auto t2 = Clock::now();
   ss->fitter = std::make_unique<DeviceFitter>(ss->prep, ss->genes, ss->opt.device, 1, ss->opt.dense_sweep == 0);
@@ -1400,7 +1403,7 @@ int32_t run_nebula_device(const nb_csr* counts, const uint64_t* subject_id, cons
   const auto t_start = Clock::now();
   try {
     if (!out) fail(NB_ERR_INVALID_ARGUMENT, "out is null");
-    std::unique_ptr<Session> ss = create_session(counts, subject_id, design, n_coef, offset, params, options);
+    std::unique_ptr<Session> ss = create_session(counts, subject_id, design, n_coef, offset, params, options, true);
     const uint64_t upload = ss->fitter->h2d_bytes();
     if (stats) *stats = nb_stats{};
     fit_session(*ss, out, stats);
@@ -1427,7 +1430,8 @@ NB_API int32_t nb_session_create(const nb_csr* counts, const uint64_t* subject_i
   try {
     if (!out) nebula::fail(NB_ERR_INVALID_ARGUMENT, "out is null");
     auto s = std::make_unique<nb_session>();
-    s->impl = nebula::create_session(counts, subject_id, design, n_coef, offset_or_null, params_or_null, options);
+    s->impl = nebula::create_session(counts, subject_id, design, n_coef, offset_or_null, params_or_null, options,
+                                     false);
     *out = s.release();
     return NB_OK;
   } catch (const nebula::NbError& e) {
@@ -1548,8 +1552,7 @@ NB_API int32_t nb_opt_pml_cuda(const double* design, const double* offset, uint6
     prep.totals.assign(subject_total, subject_total + k);
     prep.kept = {0};
     std::vector<GeneCounts> genes(1);
-    genes[0].cells.assign(cells, cells + n_pos);
-    genes[0].counts.assign(counts, counts + n_pos);
+    genes[0].own(cells, counts, n_pos);
     DeviceFitter fitter(prep, genes, -1);
     std::vector<device::FitRequest> reqs(n_requests);
     for (uint32_t q = 0; q < n_requests; ++q) {

@@ -269,14 +269,18 @@ Prepared prepare(const nb_csr* counts, const uint64_t* subject_id, const double*
   return out;
 }
 
-GeneCounts positive_indices(const CsrView& csr, size_t gene) {
+GeneCounts positive_indices(const CsrView& csr, size_t gene, bool borrow) {
   GeneCounts out;
-  out.cells.reserve(csr.indptr[gene + 1] - csr.indptr[gene]);
-  out.counts.reserve(csr.indptr[gene + 1] - csr.indptr[gene]);
+  const uint32_t e0 = csr.indptr[gene], e1 = csr.indptr[gene + 1];
+  // distinct counts other than one and two: small whole counts tallied by
+  // index, anything else in a map, then merged in increasing order
+  constexpr int kDirect = 1024;
+  std::vector<double> direct(kDirect, 0.0);
+  std::unordered_map<double, double> other;
   double sum = 0.0;
   uint32_t prev = 0;
-  bool have_prev = false;
-  for (uint32_t e = csr.indptr[gene]; e < csr.indptr[gene + 1]; ++e) {
+  bool have_prev = false, all_positive = true;
+  for (uint32_t e = e0; e < e1; ++e) {
     double v = csr.data[e];
     if (v > 0.0) {
       uint32_t c = csr.indices[e];
@@ -285,24 +289,31 @@ GeneCounts positive_indices(const CsrView& csr, size_t gene) {
         fail(NB_ERR_INVALID_ARGUMENT, "Cell indices must be strictly increasing.");
       prev = c;
       have_prev = true;
-      out.cells.push_back(c);
-      out.counts.push_back(v);
       sum += v;
       if (v == 1.0) ++out.n_one;
       else if (v == 2.0) ++out.n_two;
+      else if (v < kDirect && v == std::floor(v)) direct[static_cast<int>(v)] += 1.0;
+      else other[v] += 1.0;
+    } else {
+      all_positive = false;
     }
   }
-  out.mean_count = sum / static_cast<double>(csr.n_cells);
-  // distinct counts other than one and two: small whole counts tallied by
-  // index, anything else in a map, then merged in increasing order
-  constexpr int kDirect = 1024;
-  std::vector<double> direct(kDirect, 0.0);
-  std::unordered_map<double, double> other;
-  for (double y : out.counts) {
-    if (y == 1.0 || y == 2.0) continue;
-    if (y < kDirect && y == std::floor(y)) direct[static_cast<int>(y)] += 1.0;
-    else other[y] += 1.0;
+  if (all_positive && borrow) {
+    out.cells = View<uint32_t>(csr.indices + e0, e1 - e0);
+    out.counts = View<double>(csr.data + e0, e1 - e0);
+  } else {  // the stored zeros left out
+    out.own_cells_.reserve(e1 - e0);
+    out.own_counts_.reserve(e1 - e0);
+    for (uint32_t e = e0; e < e1; ++e) {
+      if (csr.data[e] > 0.0) {
+        out.own_cells_.push_back(csr.indices[e]);
+        out.own_counts_.push_back(csr.data[e]);
+      }
+    }
+    out.cells = out.own_cells_;
+    out.counts = out.own_counts_;
   }
+  out.mean_count = sum / static_cast<double>(csr.n_cells);
   std::vector<std::pair<double, double>> rest(other.begin(), other.end());
   std::sort(rest.begin(), rest.end());
   size_t r = 0;

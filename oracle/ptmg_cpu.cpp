@@ -218,8 +218,7 @@ ORACLE_API double oracle_ptmg_eval(const double* design, const double* log_offse
   sh.n_coef = static_cast<int>(n_coef);
   sh.n_subjects = static_cast<int>(k);
   nebula::GeneCounts gc;
-  gc.counts.assign(counts, counts + n_pos);
-  gc.cells.assign(cells, cells + n_pos);
+  gc.own(cells, counts, n_pos);
   for (double y : gc.counts) {  // the tallies positive_indices keeps (ptmg.rs:1708-1719)
     if (y == 1.0) {
       ++gc.n_one;
