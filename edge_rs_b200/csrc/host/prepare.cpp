@@ -74,7 +74,10 @@ void Params::validate() const {
 
 namespace {
 
-void validate_csr(const nb_csr* c) {
+// Checks the CSR structure; returns whether every stored value is a
+// non-negative finite number (found in the same pass as the index check and
+// reported by the caller after the checks that come before it).
+bool validate_csr(const nb_csr* c) {
   if (!c) fail(NB_ERR_INVALID_ARGUMENT, "counts is null");
   if (c->format != NB_CSR)
     fail(NB_ERR_MALFORMED_SPARSE, "nebula_sparse needs gene-major counts in CSR form.");
@@ -90,12 +93,19 @@ void validate_csr(const nb_csr* c) {
     if (c->indptr[g + 1] < c->indptr[g]) fail(NB_ERR_MALFORMED_SPARSE, "indptr is not non-decreasing");
   if (c->indptr[c->n_genes] != c->nnz)
     fail(NB_ERR_MALFORMED_SPARSE, "indptr does not end at the number of stored values");
+  std::atomic<bool> finite{true};
   const bool in_range = all_blocks(c->nnz, c->nnz >= (size_t{1} << 20), [&](size_t a, size_t b) {
-    for (size_t i = a; i < b; ++i)
-      if (c->indices[i] >= c->n_cells) return false;
-    return true;
+    bool ok = true, fin = true;
+    for (size_t i = a; i < b; ++i) {
+      ok &= c->indices[i] < c->n_cells;
+      const double v = c->data[i];
+      fin &= std::isfinite(v) && v >= 0.0;
+    }
+    if (!fin) finite.store(false);
+    return ok;
   });
   if (!in_range) fail(NB_ERR_MALFORMED_SPARSE, "cell index out of range");
+  return finite.load();
 }
 
 }  // namespace
@@ -104,18 +114,11 @@ Prepared prepare(const nb_csr* counts, const uint64_t* subject_id, const double*
                  uint32_t n_coef, const double* offset, const nb_params* params_in) {
   Params params = Params::from(params_in);
   params.validate();
-  validate_csr(counts);
+  const bool finite = validate_csr(counts);
   const size_t n_cells = counts->n_cells;
   const size_t n_genes = counts->n_genes;
   if (n_cells < 2) fail(NB_ERR_INVALID_ARGUMENT, "NEBULA needs more than one cell in the count matrix.");
   if (n_coef == 0) fail(NB_ERR_MUST_BE_POSITIVE, "n_coef must be positive");
-  const bool finite = all_blocks(counts->nnz, counts->nnz >= (size_t{1} << 20), [&](size_t a, size_t b) {
-    for (size_t i = a; i < b; ++i) {
-      const double v = counts->data[i];
-      if (!(std::isfinite(v) && v >= 0.0)) return false;
-    }
-    return true;
-  });
   if (!finite) fail(NB_ERR_INVALID_ARGUMENT, "The counts hold a value that is not a non-negative finite number.");
   if (!design) fail(NB_ERR_SHAPE_MISMATCH, "design is null");
   if (!subject_id) fail(NB_ERR_LENGTH_MISMATCH, "subject_id is null");
