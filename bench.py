@@ -356,8 +356,11 @@ def ours_arm(args, world, rank, local, dist):
     flop = ((visits - sparse_visits) * flops_per_visit(n_varying)
             + sparse_visits * flops_per_visit(n_varying, sparse=True))
     achieved = flop / (float(np.sum(step_ms)) / 1000.0) / 1e12
+    # DRAM bytes of one launch, measured by ncu on the c1 workload of 500
+    # genes (one pass over the whole persistent launch); no figure for other
+    # workloads
     traffic = None
-    if os.path.exists(PROFILE_SUMMARY):
+    if os.path.exists(PROFILE_SUMMARY) and args.config == "c1" and genes == 500 and world == 1:
         try:
             with open(PROFILE_SUMMARY) as fh:
                 traffic = json.load(fh).get("dram_bytes_per_launch")
