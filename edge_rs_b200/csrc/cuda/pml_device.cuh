@@ -183,6 +183,9 @@ __host__ __device__ inline EchoResult echo_of(const EchoRequest& q, long long ti
 }
 int launch_ring_echo(const RingView& ring, EchoResult* results, long long* done, int ctas, void* stream);
 
+// dst[i] = src[i] for n counts uploaded as floats (upload.cu).
+int widen_counts(const float* src, double* dst, size_t n, void* stream);
+
 // Clusters of `cluster` CTAs the streaming kernel can keep resident at once.
 int fit_queue_max_clusters(int n_subjects, int n_coef, int n_varying, int cluster);
 

@@ -96,6 +96,8 @@ struct GeneCounts {
   View<double> counts;
   double mean_count = 0.0;
   size_t n_one = 0, n_two = 0;
+  // every count is a whole number below 2^24, so a float holds it exactly
+  bool small_whole = true;
   // distinct counts other than one and two, increasing, with multiplicities:
   // the gamma-function terms take one lgamma per distinct value
   std::vector<double> big_values, big_mult;
@@ -111,6 +113,9 @@ struct GeneCounts {
     own_counts_.assign(y, y + n);
     cells = own_cells_;
     counts = own_counts_;
+    small_whole = true;
+    for (size_t i = 0; i < n; ++i)
+      small_whole = small_whole && y[i] >= 0.0 && y[i] < 16777216.0 && y[i] == static_cast<double>(static_cast<int32_t>(y[i]));
   }
 
  private:

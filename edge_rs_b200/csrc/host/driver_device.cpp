@@ -17,6 +17,7 @@
 #include <cmath>
 #include <chrono>
 #include <cstring>
+#include <exception>
 #include <limits>
 #include <memory>
 #include <mutex>
@@ -167,6 +168,11 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
   const size_t nd = sh.design.size(), no = sh.log_offset.size();
   PinnedStage stage((nz + nd + no) * sizeof(double) + nz * sizeof(uint32_t));
   double* const counts_h = reinterpret_cast<double*>(stage.data());
+  // whole counts below 2^24 travel as floats (exact), half the bytes, and
+  // are widened to doubles on the device
+  bool small_whole = true;
+  for (const GeneCounts& gc : genes) small_whole = small_whole && gc.small_whole;
+  float* const countsf_h = reinterpret_cast<float*>(counts_h);
   double* const design_h = counts_h + nz;
   double* const offset_h = design_h + nd;
   uint32_t* const cells_h = reinterpret_cast<uint32_t*>(offset_h + no);
@@ -178,6 +184,27 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
   std::vector<uint32_t> rcells(R + 1);
   for (int v = 0; v <= R; ++v) rcells[v] = static_cast<uint32_t>(sh.n_cells * static_cast<size_t>(v) / R);
   std::vector<uint64_t> rpos(G * (R + 1));
+  // zero-count tables (the reference's ZeroCells, nebula.rs:641), built once
+  // for the call when enough cells share their subject's design rows, on
+  // their own thread while the others fill the staging; whether the run is
+  // tabled decides stage one's descent (L-BFGS-B), so it is found even when
+  // the sweeps are asked to visit every cell
+  zero::Tables zt;
+  bool tabled = false;
+  std::exception_ptr tables_err;
+  std::thread tables_thread([&] {
+    try {
+      tabled = zero::build_tables(sh.design.data(), sh.log_offset.data(), sh.fid.data(), K, sh.n_coef, &zt);
+    } catch (...) {
+      tables_err = std::current_exception();
+    }
+  });
+  struct JoinAtExit {
+    std::thread& t;
+    ~JoinAtExit() {
+      if (t.joinable()) t.join();
+    }
+  } join_tables{tables_thread};
   parallel_for(G + 1, 0, [&](size_t g) {
     if (g == G) {
       std::copy(sh.design.begin(), sh.design.end(), design_h);
@@ -186,7 +213,12 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
     }
     const GeneCounts& gc = genes[g];
     std::copy(gc.cells.begin(), gc.cells.end(), cells_h + gene_ptr[g]);
-    std::copy(gc.counts.begin(), gc.counts.end(), counts_h + gene_ptr[g]);
+    if (small_whole) {
+      float* dst = countsf_h + gene_ptr[g];
+      for (size_t i = 0; i < gc.counts.size(); ++i) dst[i] = static_cast<float>(gc.counts[i]);
+    } else {
+      std::copy(gc.counts.begin(), gc.counts.end(), counts_h + gene_ptr[g]);
+    }
     std::copy(prep.totals.begin() + prep.kept[g] * K, prep.totals.begin() + (prep.kept[g] + 1) * K,
               totals.begin() + g * K);
     // positive_runs (pml.rs:1155-1160) as absolute positions
@@ -225,17 +257,22 @@ DeviceFitter::DeviceFitter(const Prepared& prep, const std::vector<GeneCounts>& 
   data_.design = device_copy(design_h, nd, stream_, &pooled_);
   data_.log_offset = device_copy(offset_h, no, stream_, &pooled_);
   data_.cells = device_copy(cells_h, nnz, stream_, &pooled_);
-  data_.counts = device_copy(counts_h, nnz, stream_, &pooled_);
-  h2d_bytes_ = (sh.design.size() + sh.log_offset.size() + nnz + totals.size()) * sizeof(double) +
+  if (small_whole && nnz > 0) {
+    const float* countsf_d = device_copy(countsf_h, nnz, stream_, &pooled_);
+    double* counts_d = pool_alloc<double>(nnz, stream_, &pooled_);
+    cuda_check(static_cast<cudaError_t>(device::widen_counts(countsf_d, counts_d, nnz, stream_)), "widen counts");
+    data_.counts = counts_d;
+  } else {
+    data_.counts = device_copy(counts_h, nnz, stream_, &pooled_);
+  }
+  h2d_bytes_ = (sh.design.size() + sh.log_offset.size() + (small_whole ? 0 : nnz) + totals.size()) * sizeof(double) +
+               (small_whole ? nnz : 0) * sizeof(float) +
                (fid.size() + nnz + wcells.size() + rcells.size()) * sizeof(uint32_t) +
                (gene_ptr.size() + runs.size() + rpos.size()) * sizeof(uint64_t);
-  // zero-count tables (the reference's ZeroCells, nebula.rs:641): built once
-  // for the call when enough cells share their subject's design rows
+  tables_thread.join();
+  if (tables_err) std::rethrow_exception(tables_err);
+  design_tabled_ = tabled;
   {
-    // whether the run is tabled decides stage one's descent (L-BFGS-B), so
-    // it is found even when the sweeps are asked to visit every cell
-    zero::Tables zt;
-    design_tabled_ = zero::build_tables(sh.design.data(), sh.log_offset.data(), sh.fid.data(), K, sh.n_coef, &zt);
     if (tables && design_tabled_) {
       std::vector<uint64_t> lpos(R + 1);
       for (int v = 0; v <= R; ++v)

@@ -296,7 +296,10 @@ GeneCounts positive_indices(const CsrView& csr, size_t gene, bool borrow) {
       if (v == 1.0) ++out.n_one;
       else if (v == 2.0) ++out.n_two;
       else if (v < kDirect && v == std::floor(v)) direct[static_cast<int>(v)] += 1.0;
-      else other[v] += 1.0;
+      else {
+        other[v] += 1.0;
+        if (!(v < 16777216.0 && v == std::floor(v))) out.small_whole = false;
+      }
     } else {
       all_positive = false;
     }
