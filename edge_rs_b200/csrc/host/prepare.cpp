@@ -176,31 +176,51 @@ Prepared prepare(const nb_csr* counts, const uint64_t* subject_id, const double*
   sh.log_mean_offset = std::log(mean_offset);
   sh.cv2 = cv * cv;
 
-  // centre_design (ptmg.rs:1748-1797)
+  // centre_design (ptmg.rs:1748-1797), in row-major passes over the design;
+  // each column's sums still take its cells in order
   const int nc = sh.n_coef;
-  for (size_t i = 0; i < n_cells * nc; ++i)
-    if (!std::isfinite(design[i])) fail(NB_ERR_INVALID_ARGUMENT, "design holds a non-finite value.");
-  sh.design.assign(n_cells * nc, 0.0);
+  std::vector<double> mean(nc, 0.0), var(nc, 0.0);
+  for (size_t i = 0; i < n_cells; ++i) {
+    const double* row = design + i * nc;
+    for (int j = 0; j < nc; ++j)
+      if (!std::isfinite(row[j])) fail(NB_ERR_INVALID_ARGUMENT, "design holds a non-finite value.");
+  }
+  for (size_t i = 0; i < n_cells; ++i) {
+    const double* row = design + i * nc;
+    for (int j = 0; j < nc; ++j) mean[j] += row[j];
+  }
+  for (int j = 0; j < nc; ++j) mean[j] /= static_cast<double>(n_cells);
+  sh.design.resize(n_cells * nc);
+  for (size_t i = 0; i < n_cells; ++i) {
+    const double* row = design + i * nc;
+    double* out_row = &sh.design[i * nc];
+    for (int j = 0; j < nc; ++j) {
+      const double d = row[j] - mean[j];
+      out_row[j] = d;
+      var[j] += d * d;
+    }
+  }
+  // per column: 0 scaled by its sd, 1 a constant column set to one (the
+  // intercept), 2 a zero vector (refused below)
+  std::vector<int> mode(nc, 0);
   sh.sds.assign(nc, 0.0);
   for (int j = 0; j < nc; ++j) {
-    double mean = 0.0;
-    for (size_t i = 0; i < n_cells; ++i) mean += design[i * nc + j];
-    mean /= static_cast<double>(n_cells);
-    double var = 0.0;
-    for (size_t i = 0; i < n_cells; ++i) {
-      double d = design[i * nc + j] - mean;
-      sh.design[i * nc + j] = d;
-      var += d * d;
-    }
-    double sd = std::sqrt(var / static_cast<double>(n_cells));
+    const double sd = std::sqrt(var[j] / static_cast<double>(n_cells));
     if (sd > 0.0) {
-      for (size_t i = 0; i < n_cells; ++i) sh.design[i * nc + j] /= sd;
       sh.sds[j] = sd;
     } else if (design[j] != 0.0) {
-      for (size_t i = 0; i < n_cells; ++i) sh.design[i * nc + j] = 1.0;
       sh.sds[j] = sd;
+      mode[j] = 1;
     } else {
       sh.sds[j] = -1.0;
+      mode[j] = 2;
+    }
+  }
+  for (size_t i = 0; i < n_cells; ++i) {
+    double* out_row = &sh.design[i * nc];
+    for (int j = 0; j < nc; ++j) {
+      if (mode[j] == 0) out_row[j] /= sh.sds[j];
+      else if (mode[j] == 1) out_row[j] = 1.0;
     }
   }
   for (int j = 0; j < nc; ++j)
@@ -236,13 +256,22 @@ Prepared prepare(const nb_csr* counts, const uint64_t* subject_id, const double*
   for (int s = 0; s < k; ++s)
     for (size_t i = sh.fid[s]; i < sh.fid[s + 1]; ++i) subject_of[i] = s;
   out.totals.assign(n_genes * k, 0.0);
-  // each gene's row on its own, in entry order; blocks of genes run in parallel
+  // each gene's row on its own, in entry order; blocks of genes run in
+  // parallel. Cells come in increasing order (checked later), so the
+  // subject advances with them; a cell before the current subject (an
+  // unsorted row) looks its subject up
   all_blocks(n_genes, counts->nnz >= (size_t{1} << 20), [&](size_t a, size_t b) {
     for (size_t g = a; g < b; ++g) {
       double* row = &out.totals[g * k];
+      int s = 0;
       for (uint32_t e = counts->indptr[g]; e < counts->indptr[g + 1]; ++e) {
         double v = counts->data[e];
-        if (v > 0.0) row[subject_of[counts->indices[e]]] += v;
+        if (v > 0.0) {
+          const uint64_t c = counts->indices[e];
+          if (c < sh.fid[s]) s = subject_of[c];
+          while (c >= sh.fid[s + 1]) ++s;
+          row[s] += v;
+        }
       }
     }
     return true;
