@@ -172,7 +172,10 @@ Prepared prepare(const nb_csr* counts, const uint64_t* subject_id, const double*
     cv = std::sqrt(ss / static_cast<double>(n_cells)) / mean_offset;
   }
   sh.log_offset.resize(n_cells);
-  for (size_t i = 0; i < n_cells; ++i) sh.log_offset[i] = std::log(offset ? offset[i] : 1.0);
+  all_blocks(n_cells, n_cells >= (size_t{1} << 15), [&](size_t a, size_t b) {
+    for (size_t i = a; i < b; ++i) sh.log_offset[i] = std::log(offset ? offset[i] : 1.0);
+    return true;
+  });
   sh.log_mean_offset = std::log(mean_offset);
   sh.cv2 = cv * cv;
 
