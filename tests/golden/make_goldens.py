@@ -13,8 +13,8 @@ their root on the command line or in EDGE_RS_REFERENCE:
    reference keeps inside its unit tests (R's 17-digit prints), transcribed
    here with the file:line each comes from.
 
-The GPU box has no copy of the reference; the tests only read the files this
-script writes.
+The tests read only the files this script writes, so they run where no copy
+of the reference exists.
 """
 import json
 import os
