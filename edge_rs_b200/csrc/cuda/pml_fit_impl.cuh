@@ -61,17 +61,6 @@ struct Dims {
 };
 constexpr int kLaplaceSums = 4;
 
-// Asynchronous 8-byte copy global -> shared (cp.async), and its group fences.
-__device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
-  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
@@ -100,7 +89,6 @@ struct Smem {
   double* pieces[2];     // (K + kRanges) x NP each: one sweep's (subject, range) pieces, by sweep parity
   double* rtot;          // K x NP, per-subject reduced totals after the combine
   double* totals;        // K x NS (Dims<NB>), per-subject totals over every column
-  double* stage;         // kWarps x kStageDoubles: each lane's next two cells' varying columns and offsets
   double* sw[2];         // two sweeps: w K, dw K, vw K, vwb K*NB, db NB, vb NB*NB, ll 1
   double* beta;          // NB
   double* log_w;         // K
@@ -127,11 +115,9 @@ struct Smem {
   int32_t* vhi;          // K: last range meeting each subject
   int32_t* vpos;         // NB: each column's index among the varying columns, or -1
 
-  // two buffers x two cells x (NV varying design values + the offset) x 32 lanes
-  static constexpr int kStageDoubles = 2 * 2 * (NV + 1) * 32;
   __host__ __device__ static size_t sweep_doubles(int K) { return 3 * K + K * NB + NB + NB * NB + 1; }
   __host__ __device__ static size_t doubles(int K) {
-    return (size_t)kNbTableDoubles + (size_t)kWarps * kStageDoubles + (size_t)(3 * K + 2 * kRanges) * NP +
+    return (size_t)kNbTableDoubles + (size_t)(3 * K + 2 * kRanges) * NP +
            (size_t)K * Dims<NB>::NS + 2 * sweep_doubles(K) + 4 * NB + 7 * K + 2 * NB * NB + 16 +
            (size_t)K * NB + 2 * K + (kRanges + 1) + (K + 1);
   }
@@ -144,8 +130,6 @@ struct Smem {
     double* p = base;
     tab = reinterpret_cast<NbTableData*>(p);
     p += kNbTableDoubles;
-    stage = p;
-    p += kWarps * kStageDoubles;
     pieces[0] = p;
     p += (K + kRanges) * NP;
     pieces[1] = p;
@@ -344,10 +328,11 @@ __device__ void sweep_sums(const GeneData& d, Smem<NB, NV>& sm, const double* be
       for (int x = 0; x < NPV; ++x) acc[x] = 0.0;
       // dense: two cells (r and r + 32) per iteration; their exp/log/division
       // chains interleave, and each accumulator still takes cell r before
-      // cell r + 32, the order of the lane's sequential sum. Each lane copies
-      // its next iteration's two cells' varying design values and offsets
-      // into shared memory (cp.async, double-buffered) while it computes the
-      // current ones, and reads only what it copied itself.
+      // cell r + 32, the order of the lane's sequential sum. The cells'
+      // varying design values and offsets are read straight from L2 (the
+      // other resident warps hide the latency): staging the next iteration's
+      // rows in shared memory with cp.async cost more issue slots than it
+      // saved (warm c1 65.1 against 62.8-63.4 ms a step).
       if (d.tabled) {
         // zero-count tables: the dense part visits the segment's loose cells
         // only, two per iteration like the positive entries below
@@ -381,42 +366,16 @@ __device__ void sweep_sums(const GeneData& d, Smem<NB, NV>& sm, const double* be
           }
         }
       } else {
-        double* stg = sm.stage + warp * Smem<NB, NV>::kStageDoubles;
-        auto prefetch = [&](int r, int buf) {
-          double* dst = stg + buf * 2 * (NV + 1) * 32 + lane;
-#pragma unroll
-          for (int k = 0; k < 2; ++k) {
-            const int c = r + 32 * k;
-            if (c < s_end) {
-              const double* row = d.design + static_cast<size_t>(c) * NB;
-#pragma unroll
-              for (int j = 0; j < NV; ++j) cp_async8(dst + (k * (NV + 1) + j) * 32, row + vc[j]);
-              cp_async8(dst + (k * (NV + 1) + NV) * 32, d.log_offset + c);
-            }
-          }
-          cp_async_commit();
-        };
-        int buf = 0;
-        prefetch(c0 + lane, 0);
         for (int r = c0 + lane; r < s_end; r += 64) {
-          prefetch(r + 64, buf ^ 1);
-          cp_async_wait<1>();
           const bool has_b = r + 32 < s_end;
-          const double* src = stg + buf * 2 * (NV + 1) * 32 + lane;
+          const int rb = has_b ? r + 32 : r;
           double xa[NX], xb[NX];
 #pragma unroll
-          for (int j = 0; j < NV; ++j) xa[j] = src[j * 32];
-          const double offa = src[NV * 32];
-          double offb = offa;
-          if (has_b) {
-#pragma unroll
-            for (int j = 0; j < NV; ++j) xb[j] = src[((NV + 1) + j) * 32];
-            offb = src[(2 * NV + 1) * 32];
-          } else {
-#pragma unroll
-            for (int j = 0; j < NV; ++j) xb[j] = xa[j];
+          for (int j = 0; j < NV; ++j) {
+            xa[j] = __ldg(d.design + static_cast<size_t>(r) * NB + vc[j]);
+            xb[j] = __ldg(d.design + static_cast<size_t>(rb) * NB + vc[j]);
           }
-          buf ^= 1;
+          const double offa = __ldg(d.log_offset + r), offb = __ldg(d.log_offset + rb);
           const double ea = nb_exp_tab(linear_eta<NV>(xa, beta, offa + csl), tab);
           const double eb = nb_exp_tab(linear_eta<NV>(xb, beta, offb + csl), tab);
           const double ta = ea + gamma, tb = eb + gamma;
@@ -435,7 +394,6 @@ __device__ void sweep_sums(const GeneData& d, Smem<NB, NV>& sm, const double* be
             if (has_b) laplace_terms(acc, eb, tb, gamma, gamma);
           }
         }
-        cp_async_wait<0>();
       }
       // sparse: the segment's positive entries, into the same partials
       for (uint64_t p = pa + lane; p < p_end; p += 64) {
